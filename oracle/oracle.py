@@ -1,0 +1,224 @@
+"""ctypes bindings for the CPU oracle (oracle/liboracle.so) and the reference
+build (oracle/_ref/libref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker.  The product package never
+imports this module.
+
+All matrices are numpy float64 arrays in column-major (Fortran) order, as the
+reference stores them.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_ORC = None
+_REF = None
+
+_i64 = C.c_int64
+_dp = C.POINTER(C.c_double)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def lib():
+    """The C restatement (built by `make -C oracle`)."""
+    global _ORC
+    if _ORC is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            import subprocess
+            subprocess.check_call(["make", "-s", "-C", _HERE, "liboracle.so"])
+        _ORC = C.CDLL(path)
+        for name in ("orc_chol_residual", "orc_backward_error"):
+            getattr(_ORC, name).restype = C.c_double
+    return _ORC
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(_HERE, "_ref", "libref.so"))
+
+
+def ref():
+    """The reference compiled from its own sources (built by `make -C oracle ref`)."""
+    global _REF
+    if _REF is None:
+        _REF = C.CDLL(os.path.join(_HERE, "_ref", "libref.so"))
+    return _REF
+
+
+def fortran(a) -> np.ndarray:
+    return np.asfortranarray(np.array(a, dtype=np.float64, copy=True))
+
+
+# --------------------------------------------------------------------------
+# seeded inputs with the shapes/distributions of the reference's generators
+# --------------------------------------------------------------------------
+def spd_diag_dominant(n: int, seed: int = 0) -> np.ndarray:
+    """A = (R + R^T)/2 + n I with R ~ U[0,1): the distribution of dgenmat_spd
+    (genmat.c:49-70, symmetric U[0,1) plus n on the diagonal)."""
+    rng = np.random.default_rng(seed)
+    R = rng.random((n, n))
+    return fortran((R + R.T) / 2 + n * np.eye(n))
+
+
+def spd_covariance(n: int, delta: float, seed: int = 0) -> np.ndarray:
+    """A = G G^T / n + delta I with G ~ N(0,1)."""
+    rng = np.random.default_rng(seed)
+    G = rng.standard_normal((n, n))
+    return fortran(G @ G.T / n + delta * np.eye(n))
+
+
+# --------------------------------------------------------------------------
+# oracle wrappers (operate in place, return info / codes like the reference)
+# --------------------------------------------------------------------------
+def chol_rl(A: np.ndarray, b: int) -> int:
+    n = A.shape[0]
+    return lib().orc_dchol_rl(_i64(n), _i64(b), _ptr(A), _i64(A.shape[0]))
+
+
+def chol_ll(A: np.ndarray, b: int) -> int:
+    n = A.shape[0]
+    return lib().orc_dchol_ll(_i64(n), _i64(b), _ptr(A), _i64(A.shape[0]))
+
+
+def schol_rl(A: np.ndarray, b: int) -> int:
+    n = A.shape[0]
+    return lib().orc_schol_rl(_i64(n), _i64(b), _ptr(A), _i64(A.shape[0]))
+
+
+def _tile_table(tiles: np.ndarray):
+    """tiles: (mt, mt, b, b) array, tiles[j, i] is tile (i, j) stored column-major."""
+    mt = tiles.shape[0]
+    arr = (C.c_void_p * (mt * mt))()
+    for j in range(mt):
+        for i in range(mt):
+            arr[j * mt + i] = tiles[j, i].ctypes.data
+    return arr
+
+
+def chol_hrl(tiles: np.ndarray) -> int:
+    mt, b = tiles.shape[0], tiles.shape[2]
+    return lib().orc_dchol_hrl(_i64(mt), _i64(b), _tile_table(tiles))
+
+
+def chol_hll(tiles: np.ndarray) -> int:
+    mt, b = tiles.shape[0], tiles.shape[2]
+    return lib().orc_dchol_hll(_i64(mt), _i64(b), _tile_table(tiles))
+
+
+def ltrsm(uplo: str, trans: str, diag: str, bm: int, alpha: float, A: np.ndarray,
+          B: np.ndarray) -> None:
+    m, n = B.shape
+    lib().orc_dltrsm(C.c_char(uplo.encode()), C.c_char(trans.encode()), C.c_char(diag.encode()),
+                     _i64(bm), _i64(m), _i64(n), C.c_double(alpha), _ptr(A), _i64(A.shape[0]),
+                     _ptr(B), _i64(B.shape[0]))
+
+
+def spdsolv(A: np.ndarray, B: np.ndarray, b: int) -> int:
+    m, nrhs = B.shape
+    return lib().orc_dspdsolv(_i64(m), _i64(nrhs), _i64(b), _ptr(A), _ptr(B))
+
+
+def cg(A: np.ndarray, rhs: np.ndarray, bm: int, tol: float, steps: int):
+    n = A.shape[0]
+    x = np.zeros(n)
+    log = np.zeros(max(steps, 1))
+    rc = lib().orc_dcg(_i64(n), _i64(bm), _ptr(A), _i64(n), _ptr(rhs), _ptr(x),
+                       C.c_double(tol), C.c_int(steps), _ptr(log))
+    return rc, x, log
+
+
+def itref(A: np.ndarray, rhs: np.ndarray, bm: int, prec: float, refit: int, it: int):
+    n = A.shape[0]
+    x = np.zeros(n)
+    norms = np.zeros(max(refit, 1))
+    k = lib().orc_ditref(_i64(n), _i64(bm), _ptr(A), _ptr(rhs), _ptr(x), C.c_double(prec),
+                         C.c_int(refit), C.c_int(it), _ptr(norms))
+    return k, x, norms[:k]
+
+
+def chol_residual(A0: np.ndarray, L: np.ndarray) -> float:
+    n = A0.shape[0]
+    return lib().orc_chol_residual(_i64(n), _ptr(A0), _i64(A0.shape[0]), _ptr(L), _i64(L.shape[0]))
+
+
+def backward_error(A: np.ndarray, X: np.ndarray, B: np.ndarray) -> float:
+    n = A.shape[0]
+    X = fortran(X.reshape(n, -1))
+    B = fortran(B.reshape(n, -1))
+    return lib().orc_backward_error(_i64(n), _i64(X.shape[1]), _ptr(A), _i64(n), _ptr(X), _i64(n),
+                                    _ptr(B), _i64(n))
+
+
+# numpy helpers for big cases (vectorised, same definitions as above)
+def chol_residual_np(A0: np.ndarray, L: np.ndarray) -> float:
+    n = A0.shape[0]
+    Lt = np.tril(L)
+    R = Lt @ Lt.T - A0
+    return float(np.abs(R).sum(axis=1).max() / (np.abs(A0).sum(axis=1).max() * n * np.finfo(float).eps / 2))
+
+
+def backward_error_np(A: np.ndarray, X: np.ndarray, B: np.ndarray) -> float:
+    X = X.reshape(A.shape[0], -1)
+    B = B.reshape(A.shape[0], -1)
+    R = B - A @ X
+    return float(np.abs(R).max() / (np.abs(A).sum(axis=1).max() * np.abs(X).max() + np.abs(B).max()))
+
+
+# --------------------------------------------------------------------------
+# the reference itself (oracle/_ref/libref.so)
+# --------------------------------------------------------------------------
+class _OmpssBlas(C.Union):
+    """ompssblas_t (fpmatr.h:14-17), non-MKL form: .s points at "L"/"R"/"T"/..."""
+    _fields_ = [("e", C.c_int), ("s", C.c_char_p)]
+
+
+_KEEP = {}
+
+
+def ref_opt(ch: str) -> _OmpssBlas:
+    if ch not in _KEEP:
+        _KEEP[ch] = C.c_char_p(ch.encode())
+    u = _OmpssBlas()
+    u.s = _KEEP[ch].value
+    return u
+
+
+def ref_chol(variant: str, A: np.ndarray, b: int) -> int:
+    f = getattr(ref(), "ompss_dchol_" + variant)
+    n = A.shape[0]
+    return f(C.c_int(n), C.c_int(b), C.c_int(b), _ptr(A), C.c_int(A.shape[0]))
+
+
+def ref_chol_h(variant: str, tiles: np.ndarray) -> int:
+    f = getattr(ref(), "ompss_dchol_" + variant)
+    mt, b = tiles.shape[0], tiles.shape[2]
+    return f(C.c_int(mt), C.c_int(b), C.c_int(b), _tile_table(tiles))
+
+
+def ref_spdsolv(A: np.ndarray, B: np.ndarray, b: int) -> int:
+    m, nrhs = B.shape
+    return ref().dspdsolv_main(C.c_int(m), C.c_int(nrhs), C.c_int(b), _ptr(A), _ptr(B))
+
+
+def ref_dtrsm(side, uplo, trans, diag, m, n, b, alpha, A, lda, B, ldb) -> None:
+    f = ref().ompss_dtrsm
+    f.argtypes = [_OmpssBlas] * 4 + [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int,
+                                     C.c_void_p, C.c_int]
+    f(ref_opt(side), ref_opt(uplo), ref_opt(trans), ref_opt(diag), m, n, b, alpha,
+      _ptr(A), lda, _ptr(B), ldb)
+
+
+def ref_cg(A: np.ndarray, rhs: np.ndarray, bm: int, tol: float, steps: int):
+    n = A.shape[0]
+    x = np.zeros(n)
+    rc = ref().lnbref_dcg(C.c_int(n), C.c_int(bm), _ptr(A), _ptr(np.ascontiguousarray(rhs)),
+                          _ptr(x), C.c_double(tol), C.c_int(steps))
+    return rc, x
