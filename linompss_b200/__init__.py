@@ -1,0 +1,245 @@
+"""linompss_b200 -- B200 (sm_100a) tiled SPD solve with the Linompss C interface.
+
+The product is the shared library ``liblinompss_b200.so`` (C host code plus
+sm_100a CUDA kernels) whose C ABI is ``include/linompss_b200.h``.  This module
+is a thin ctypes binding over that ABI, mirroring the reference's entry points
+(same names, argument meaning and return codes) for Python callers and for
+the tests:
+
+  * host (numpy, column-major) forms: ``ompss_dchol_rl``, ``ompss_dchol_ll``,
+    ``ompss_dchol_hrl``, ``ompss_dchol_hll``, ``dspdsolv_main``, ``ompss_dtrsm``,
+    ``task_dpotrf``/``task_dtrsm``/``task_dsyrk``/``task_dgemm``, ``ompss_dcg``,
+    ``ompss_ditref``;
+  * device (torch CUDA tensor) forms: ``dchol_dev``, ``dpotrs_dev``, ``dposv_dev``,
+    ``dtrsm_dev`` and the mixed-precision / batched solvers.
+
+There is no CPU fallback: if the library is missing, importing the binding
+raises, and on a machine without an sm_100 GPU every call returns LNB_ENODEV.
+
+Device matrices are column-major like the reference's: an n x n matrix with
+leading dimension ld is held in a torch tensor ``At`` of shape (n, ld) whose
+row j is column j (i.e. ``At = A.T`` stored contiguously).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblinompss_b200.so")
+
+LNB_OK, LNB_EINVAL, LNB_ENODEV, LNB_ECUDA, LNB_ENOMEM, LNB_ETIMEOUT, LNB_ENOCONV, LNB_ETOOBIG = (
+    0, -1, -2, -3, -4, -5, -6, -7)
+FACTOR_FP64, FACTOR_FP32, FACTOR_TF32X3, FACTOR_BF16 = 0, 1, 2, 3
+
+
+class LinompssError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load the in-tree library; raise loudly if it was not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} not built: run `make -C linompss_b200/csrc` "
+                              "(or __graft_entry__.build())")
+        _lib = C.CDLL(LIB_PATH)
+        _lib.lnb_last_error.restype = C.c_char_p
+        _lib.lnb_version.restype = C.c_char_p
+    return _lib
+
+
+def last_error() -> str:
+    return lib().lnb_last_error().decode()
+
+
+def _chk(rc: int) -> int:
+    """negative return codes are LNB_E* errors"""
+    if rc < 0:
+        raise LinompssError(rc, last_error())
+    return rc
+
+
+def _p(a) -> C.c_void_p:
+    if a is None:
+        return C.c_void_p(0)
+    if isinstance(a, np.ndarray):
+        return C.c_void_p(a.ctypes.data)
+    return C.c_void_p(a.data_ptr())  # torch tensor
+
+
+def _colmajor(A: np.ndarray, dtype=np.float64):
+    if A.dtype != dtype or not A.flags.f_contiguous:
+        raise ValueError("matrix must be a Fortran-ordered (column-major) %s array" % np.dtype(dtype).name)
+    return A
+
+
+# --------------------------------------------------------------------------
+# ompssblas_t (fpmatr.h:14-17), non-MKL form
+# --------------------------------------------------------------------------
+class ompssblas_t(C.Union):
+    _fields_ = [("e", C.c_int), ("s", C.c_char_p)]
+
+
+_OPT_STRINGS = {}
+
+
+def opt(ch: str) -> ompssblas_t:
+    """OMPSSBLAS_* descriptor whose .s starts with `ch` ('L','R','U','N','T')."""
+    if ch not in _OPT_STRINGS:
+        _OPT_STRINGS[ch] = C.create_string_buffer(ch.encode())
+    u = ompssblas_t()
+    u.s = C.cast(_OPT_STRINGS[ch], C.c_char_p)
+    return u
+
+
+# --------------------------------------------------------------------------
+# host entry points (numpy, in place, like the reference)
+# --------------------------------------------------------------------------
+def ompss_dchol_rl(n: int, b: int, t: int, A: np.ndarray, lda: int) -> int:
+    _colmajor(A)
+    return _chk(lib().ompss_dchol_rl(C.c_int(n), C.c_int(b), C.c_int(t), _p(A), C.c_int(lda)))
+
+
+def ompss_dchol_ll(n: int, b: int, t: int, A: np.ndarray, lda: int) -> int:
+    _colmajor(A)
+    return _chk(lib().ompss_dchol_ll(C.c_int(n), C.c_int(b), C.c_int(t), _p(A), C.c_int(lda)))
+
+
+def _tile_table(tiles):
+    mt = tiles.shape[0]
+    arr = (C.c_void_p * (mt * mt))()
+    for j in range(mt):
+        for i in range(mt):
+            arr[j * mt + i] = tiles[j, i].ctypes.data
+    return arr
+
+
+def ompss_dchol_hrl(mt: int, b: int, t: int, tiles: np.ndarray) -> int:
+    """tiles: (mt, mt, b, b) C-ordered array; tiles[j, i] is tile (i, j) column-major."""
+    return _chk(lib().ompss_dchol_hrl(C.c_int(mt), C.c_int(b), C.c_int(t), _tile_table(tiles)))
+
+
+def ompss_dchol_hll(mt: int, b: int, t: int, tiles: np.ndarray) -> int:
+    return _chk(lib().ompss_dchol_hll(C.c_int(mt), C.c_int(b), C.c_int(t), _tile_table(tiles)))
+
+
+def ompss_dchol_nhrl(mt: int, b: int, t: int, tiles: np.ndarray) -> int:
+    return _chk(lib().ompss_dchol_nhrl(C.c_int(mt), C.c_int(b), C.c_int(t), _tile_table(tiles)))
+
+
+def ompss_dchol_nhll(mt: int, b: int, t: int, tiles: np.ndarray) -> int:
+    return _chk(lib().ompss_dchol_nhll(C.c_int(mt), C.c_int(b), C.c_int(t), _tile_table(tiles)))
+
+
+def dspdsolv_main(m: int, n: int, b: int, A: np.ndarray, B: np.ndarray) -> int:
+    _colmajor(A)
+    _colmajor(B)
+    return _chk(lib().dspdsolv_main(C.c_int(m), C.c_int(n), C.c_int(b), _p(A), _p(B)))
+
+
+def ompss_dtrsm(side, uplo, trans, diag, m, n, b, alpha, A, lda, B, ldb) -> int:
+    f = lib().ompss_dtrsm
+    f.argtypes = [ompssblas_t] * 4 + [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int,
+                                      C.c_void_p, C.c_int]
+    return _chk(f(opt(side), opt(uplo), opt(trans), opt(diag), m, n, b, alpha, _p(A), lda, _p(B), ldb))
+
+
+def task_dpotrf(uplo: str, n: int, A: np.ndarray, lda: int, p: int = 0) -> int:
+    f = lib().task_dpotrf
+    f.argtypes = [ompssblas_t, C.c_int, C.c_void_p, C.c_int, C.c_int]
+    return _chk(f(opt(uplo), n, _p(A), lda, p))
+
+
+def task_dtrsm(side, uplo, trans, diag, bm, bn, alpha, A, lda, B, ldb, p=0) -> int:
+    f = lib().task_dtrsm
+    f.argtypes = [ompssblas_t] * 4 + [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_void_p,
+                                      C.c_int, C.c_int]
+    return _chk(f(opt(side), opt(uplo), opt(trans), opt(diag), bm, bn, alpha, _p(A), lda, _p(B), ldb, p))
+
+
+def task_dsyrk(uplo, trans, n, k, alpha, A, lda, beta, Cm, ldc, p=0) -> int:
+    f = lib().task_dsyrk
+    f.argtypes = [ompssblas_t] * 2 + [C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_double,
+                                      C.c_void_p, C.c_int, C.c_int]
+    return _chk(f(opt(uplo), opt(trans), n, k, alpha, _p(A), lda, beta, _p(Cm), ldc, p))
+
+
+def task_dgemm(transa, transb, bm, bn, bk, alpha, A, lda, B, ldb, beta, Cm, ldc, p=0) -> int:
+    f = lib().task_dgemm
+    f.argtypes = [ompssblas_t] * 2 + [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int,
+                                      C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_int]
+    return _chk(f(opt(transa), opt(transb), bm, bn, bk, alpha, _p(A), lda, _p(B), ldb, beta, _p(Cm), ldc, p))
+
+
+def ompss_dcg(n, bm, A, lda, b, x, tol, steps) -> int:
+    """Returns -1 if converged, else the number of steps (itref.c:922-924)."""
+    f = lib().ompss_dcg
+    f.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_int]
+    rc = f(n, bm, _p(A), lda, _p(b), _p(x), tol, steps)
+    if rc < -1:
+        raise LinompssError(rc, last_error())
+    return rc
+
+
+def ompss_ditref(n, bm, A, lda, b, x, prec, refit, it, norms=None) -> int:
+    f = lib().ompss_ditref
+    f.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_int,
+                  C.c_int, C.c_void_p]
+    return _chk(f(n, bm, _p(A), lda, _p(b), _p(x), prec, refit, it, _p(norms)))
+
+
+# --------------------------------------------------------------------------
+# device entry points (torch CUDA tensors, column-major as (ncols, ld))
+# --------------------------------------------------------------------------
+def _stream(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+def _ld(t) -> int:
+    return int(t.stride(0))
+
+
+def dchol_dev(At, n: int, b: int, info=None, stream=None) -> int:
+    return _chk(lib().lnb_dchol_dev(C.c_int(n), C.c_int(b), _p(At), C.c_int(_ld(At)), _p(info), _stream(stream)))
+
+
+def dposv_dev(At, Bt, n: int, nrhs: int, b: int, info=None, stream=None) -> int:
+    return _chk(lib().lnb_dposv_dev(C.c_int(n), C.c_int(nrhs), C.c_int(b), _p(At), C.c_int(_ld(At)), _p(Bt),
+                                    C.c_int(_ld(Bt)), _p(info), _stream(stream)))
+
+
+def dpotrs_dev(Lt, Bt, n: int, nrhs: int, which: str = "B", stream=None) -> int:
+    return _chk(lib().lnb_dpotrs_dev(C.c_int(n), C.c_int(nrhs), _p(Lt), C.c_int(_ld(Lt)), _p(Bt),
+                                     C.c_int(_ld(Bt)), C.c_char(which.encode()), _stream(stream)))
+
+
+def dtrsm_dev(uplo: str, trans: str, diag: str, m: int, n: int, alpha: float, At, Bt, stream=None) -> int:
+    f = lib().lnb_dtrsm_dev
+    f.argtypes = [C.c_char, C.c_char, C.c_char, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int,
+                  C.c_void_p, C.c_int, C.c_void_p]
+    return _chk(f(uplo.encode(), trans.encode(), diag.encode(), m, n, alpha, _p(At), _ld(At), _p(Bt), _ld(Bt),
+                  _stream(stream)))
+
+
+def set_wait_limit_us(us: int) -> None:
+    lib().lnb_set_wait_limit_us(C.c_longlong(us))
+
+
+def release_workspace() -> None:
+    lib().lnb_release_workspace()
+
+
+def version() -> str:
+    return lib().lnb_version().decode()

@@ -1,0 +1,82 @@
+/*
+ * lnb_host.h -- internal declarations shared by the host-side C files.
+ */
+#ifndef LNB_HOST_H
+#define LNB_HOST_H
+
+#include <cuda_runtime_api.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/linompss_b200.h"
+#include "lnb_kern.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* per-device context: streams, events, cached workspace, status words */
+typedef struct {
+    int           ready;
+    int           device;
+    int           sms;
+    cudaStream_t  main;        /* stream of the host-pointer entry points */
+    cudaStream_t  crit;        /* high-priority stream: panel factorization */
+    cudaStream_t  copy;        /* device->host panel copies */
+    cudaEvent_t   ev[8];
+    void         *ws;          /* grow-only device workspace */
+    size_t        ws_size;
+    lnb_status_t *st;          /* device status word */
+    lnb_status_t *st_host;     /* pinned host mirror */
+    cudaEvent_t   t0, t1;      /* timing */
+} lnb_ctx;
+
+/* Returns the current device's context (creating it), or NULL after setting
+ * the error (LNB_ENODEV / LNB_ECUDA). */
+lnb_ctx *lnb_ctx_get(void);
+/* Ensure the cached workspace holds at least `bytes`; NULL on failure. */
+void *lnb_ws(lnb_ctx *c, size_t bytes);
+
+/* workspace carving: bump allocator over one buffer, 256-byte aligned */
+typedef struct { char *base; size_t off, cap; } lnb_arena;
+static inline size_t lnb_align256(size_t x) { return (x + 255) & ~(size_t)255; }
+static inline void *lnb_arena_take(lnb_arena *a, size_t bytes)
+{
+    size_t o = lnb_align256(a->off);
+    if (o + bytes > a->cap) return NULL;
+    a->off = o + bytes;
+    return a->base + o;
+}
+
+int  lnb_set_error(int code, const char *fmt, ...);
+int  lnb_cuda_error(int cuda_err, const char *where);
+long long lnb_wait_ns(void);
+
+/* Read back the status word after the stream work completed; returns info
+ * (>= 0) or LNB_ETIMEOUT.  Synchronizes `s`. */
+int lnb_status_read(lnb_ctx *c, cudaStream_t s);
+
+/* ---- FP64 factorization schedule on device memory (lnb_chol.c) ---------- */
+size_t lnb_chol_f64_ws_bytes(int n, int b);
+/* Factor dA in place on stream s.  `copy_back` (may be NULL): host matrix to
+ * receive each finished panel as soon as it is final (lower part). */
+int lnb_chol_f64_run(lnb_ctx *c, int n, int b, double *dA, int64_t lda, lnb_arena *ar,
+                     cudaStream_t s, double *copy_back, int64_t ldh);
+
+/* ---- FP64 triangular solves on device memory (lnb_solve.c) --------------- */
+size_t lnb_trsm_f64_ws_bytes(int64_t n);
+int lnb_trsm_f64_run(lnb_ctx *c, char uplo, char trans, char diag, int64_t n, int64_t nrhs,
+                     double alpha, const double *dT, int64_t ldt, double *dB, int64_t ldb,
+                     lnb_arena *ar, cudaStream_t s, const double *dinv_given);
+
+/* diagnostics: bracket one launch with events when profiling is on */
+int  lnb_prof_begin(cudaStream_t s);
+void lnb_prof_end(int slot, cudaStream_t s, double flops, double bytes);
+
+/* is this host pointer page-locked (so async copies really are async)? */
+int lnb_host_is_pinned(const void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

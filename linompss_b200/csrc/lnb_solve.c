@@ -1,0 +1,238 @@
+/*
+ * lnb_solve.c -- blocked triangular solves and the SPD solve (host C).
+ *
+ * bblas_dltrsm (bblas_trsm.h:116-202) walks block rows issuing one TRSM task
+ * per diagonal block and one GEMM task per off-diagonal block; spdsolv_main
+ * (spdsolv_main.c:10-20) runs it twice, L Y = B then L^T X = Y.  Here each
+ * solve is one persistent DAG-walking launch (k_trsv.cu) after one launch
+ * that inverts the 64 x 64 diagonal blocks; the forward and the backward
+ * solve share the inverses.
+ */
+#include <string.h>
+
+#include "lnb_host.h"
+
+#define CK(call, where)                                            \
+    do {                                                           \
+        int _e = (int)(call);                                      \
+        if (_e != 0) return lnb_cuda_error(_e, where);             \
+    } while (0)
+
+#define TRSV_H 64
+
+static inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+size_t lnb_trsm_f64_ws_bytes(int64_t n)
+{
+    const int64_t nb = ceil_div(n, TRSV_H);
+    return lnb_align256((size_t)nb * TRSV_H * TRSV_H * sizeof(double)) +
+           lnb_align256((size_t)lnb_trsm_sync_ints(n, TRSV_H) * sizeof(int)) + 512;
+}
+
+/* op(T) X = alpha B with T triangular (uplo as stored), left side */
+int lnb_trsm_f64_run(lnb_ctx *c, char uplo, char trans, char diag, int64_t n, int64_t nrhs,
+                     double alpha, const double *dT, int64_t ldt, double *dB, int64_t ldb,
+                     lnb_arena *ar, cudaStream_t s, const double *dinv_given)
+{
+    if (n <= 0 || nrhs <= 0) return 0;
+    const int64_t nb = ceil_div(n, TRSV_H);
+    double *dinv = (double *)dinv_given;
+    if (!dinv) {
+        dinv = (double *)lnb_arena_take(ar, (size_t)nb * TRSV_H * TRSV_H * sizeof(double));
+        if (!dinv) return lnb_set_error(LNB_ENOMEM, "trsm workspace");
+        CK(lnb_k_trtri_blocks_f64(dT, ldt, n, TRSV_H, uplo, diag == 'U', dinv, s), "trtri");
+    }
+    int *sync = (int *)lnb_arena_take(ar, (size_t)lnb_trsm_sync_ints(n, TRSV_H) * sizeof(int));
+    if (!sync) return lnb_set_error(LNB_ENOMEM, "trsm sync workspace");
+    CK(lnb_k_trsm_left_f64(uplo, trans, n, nrhs, alpha, dT, ldt, dinv, TRSV_H, dB, ldb, sync, c->st,
+                           lnb_wait_ns(), 0, s), "trsm dag");
+    return 0;
+}
+
+int lnb_selftest_wait_timeout(long long wait_us)
+{
+    /* 128 x 128 identity, 1 rhs: two diagonal items and one update item.  The
+     * ticket starts at 1, so diagonal item 0 never runs and both remaining
+     * items wait on a flag that nothing sets. */
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const int64_t n = 128;
+    void *ws = lnb_ws(c, lnb_align256(n * n * 8) + lnb_align256(n * 8) + lnb_trsm_f64_ws_bytes(n));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    double *T = lnb_arena_take(&ar, n * n * 8), *B = lnb_arena_take(&ar, n * 8);
+    double *dinv = lnb_arena_take(&ar, (size_t)ceil_div(n, TRSV_H) * TRSV_H * TRSV_H * 8);
+    int *sync = lnb_arena_take(&ar, (size_t)lnb_trsm_sync_ints(n, TRSV_H) * sizeof(int));
+    cudaStream_t s = c->main;
+    CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
+    CK(cudaMemsetAsync(T, 0, n * n * 8, s), "zero");
+    CK(cudaMemsetAsync(B, 0, n * 8, s), "zero");
+    CK(lnb_k_trtri_blocks_f64(T, n, n, TRSV_H, 'L', 1, dinv, s), "trtri");
+    CK(lnb_k_trsm_left_f64('L', 'N', n, 1, 1.0, T, n, dinv, TRSV_H, B, n, sync, c->st,
+                           (wait_us > 0 ? wait_us : 1000) * 1000LL, 1, s), "trsm dag");
+    return lnb_status_read(c, s);
+}
+
+static int opt_char(ompssblas_t o, const char *allowed, char *out, const char *what)
+{
+    if (!o.s || !o.s[0] || !strchr(allowed, o.s[0]))
+        return lnb_set_error(LNB_EINVAL, "bad %s option", what);
+    *out = o.s[0];
+    return 0;
+}
+
+/* ---- device-pointer entry points ---------------------------------------- */
+int lnb_dtrsm_dev(char uplo, char trans, char diag, int m, int n, double alpha, const double *dA,
+                  int lda, double *dB, int ldb, void *stream)
+{
+    if (m < 0 || n < 0 || lda < (m > 1 ? m : 1) || ldb < (m > 1 ? m : 1))
+        return lnb_set_error(LNB_EINVAL, "dtrsm sizes m=%d n=%d lda=%d ldb=%d", m, n, lda, ldb);
+    if ((uplo != 'L' && uplo != 'U') || (trans != 'N' && trans != 'T') || (diag != 'N' && diag != 'U'))
+        return lnb_set_error(LNB_EINVAL, "dtrsm options");
+    if (m == 0 || n == 0) return 0;
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    void *ws = lnb_ws(c, lnb_trsm_f64_ws_bytes(m));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
+    return lnb_trsm_f64_run(c, uplo, trans, diag, m, n, alpha, dA, lda, dB, ldb, &ar, s, NULL);
+}
+
+int lnb_dpotrs_dev(int n, int nrhs, const double *dL, int lda, double *dB, int ldb, char which,
+                   void *stream)
+{
+    if (n < 0 || nrhs < 0 || lda < (n > 1 ? n : 1) || ldb < (n > 1 ? n : 1))
+        return lnb_set_error(LNB_EINVAL, "potrs sizes");
+    if (which != 'N' && which != 'T' && which != 'B') return lnb_set_error(LNB_EINVAL, "potrs which");
+    if (n == 0 || nrhs == 0) return 0;
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    void *ws = lnb_ws(c, lnb_trsm_f64_ws_bytes(n) + lnb_trsm_f64_ws_bytes(n));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
+    const int64_t nb = ceil_div(n, TRSV_H);
+    double *dinv = (double *)lnb_arena_take(&ar, (size_t)nb * TRSV_H * TRSV_H * sizeof(double));
+    CK(lnb_k_trtri_blocks_f64(dL, lda, n, TRSV_H, 'L', 0, dinv, s), "trtri");
+    int e = 0;
+    if (which == 'N' || which == 'B')
+        e = lnb_trsm_f64_run(c, 'L', 'N', 'N', n, nrhs, 1.0, dL, lda, dB, ldb, &ar, s, dinv);
+    if (!e && (which == 'T' || which == 'B'))
+        e = lnb_trsm_f64_run(c, 'L', 'T', 'N', n, nrhs, 1.0, dL, lda, dB, ldb, &ar, s, dinv);
+    return e;
+}
+
+int lnb_dposv_dev(int n, int nrhs, int b, double *dA, int lda, double *dB, int ldb, int *info_dev,
+                  void *stream)
+{
+    if (n < 0 || nrhs < 0 || b <= 0 || b > 1024 || lda < (n > 1 ? n : 1) || ldb < (n > 1 ? n : 1))
+        return lnb_set_error(LNB_EINVAL, "posv arguments");
+    if (n == 0) return 0;
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const int64_t nb = ceil_div(n, TRSV_H);
+    void *ws = lnb_ws(c, lnb_chol_f64_ws_bytes(n, b) + 2 * lnb_trsm_f64_ws_bytes(n));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    cudaStream_t s = (cudaStream_t)stream;
+    int e = lnb_chol_f64_run(c, n, b, dA, lda, &ar, s, NULL, 0);
+    if (e) return e;
+    if (nrhs > 0) {
+        double *dinv = (double *)lnb_arena_take(&ar, (size_t)nb * TRSV_H * TRSV_H * sizeof(double));
+        CK(lnb_k_trtri_blocks_f64(dA, lda, n, TRSV_H, 'L', 0, dinv, s), "trtri");
+        if ((e = lnb_trsm_f64_run(c, 'L', 'N', 'N', n, nrhs, 1.0, dA, lda, dB, ldb, &ar, s, dinv))) return e;
+        if ((e = lnb_trsm_f64_run(c, 'L', 'T', 'N', n, nrhs, 1.0, dA, lda, dB, ldb, &ar, s, dinv))) return e;
+    }
+    if (info_dev)
+        CK(cudaMemcpyAsync(info_dev, &c->st->info, sizeof(int), cudaMemcpyDeviceToDevice, s), "info");
+    return 0;
+}
+
+/* ---- host entry points ---------------------------------------------------- */
+static inline int64_t ld_dev(int64_t n) { return (n + 7) & ~(int64_t)7; }
+
+int dspdsolv_main(int m, int nrhs, int b, double *A, double *B)
+{
+    if (m < 0 || nrhs < 0 || b <= 0 || b > 1024) return lnb_set_error(LNB_EINVAL, "spdsolv arguments");
+    if (m == 0) return 0;
+    if (!A || (nrhs > 0 && !B)) return lnb_set_error(LNB_EINVAL, "NULL matrix");
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const int64_t ldd = ld_dev(m);
+    const size_t abytes = (size_t)ldd * m * sizeof(double), bbytes = (size_t)ldd * (nrhs ? nrhs : 1) * sizeof(double);
+    void *ws = lnb_ws(c, lnb_align256(abytes) + lnb_align256(bbytes) + lnb_chol_f64_ws_bytes(m, b) +
+                             2 * lnb_trsm_f64_ws_bytes(m));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    double *dA = (double *)lnb_arena_take(&ar, abytes);
+    double *dB = (double *)lnb_arena_take(&ar, bbytes);
+    cudaStream_t s = c->main;
+    /* lower block-columns of A, all of B */
+    for (int64_t c0 = 0; c0 < m; c0 += b) {
+        int64_t w = m - c0 < b ? m - c0 : b;
+        CK(cudaMemcpy2DAsync(dA + c0 + c0 * ldd, ldd * sizeof(double), A + c0 + c0 * (int64_t)m,
+                             (size_t)m * sizeof(double), (size_t)(m - c0) * sizeof(double), w,
+                             cudaMemcpyHostToDevice, s), "A in");
+    }
+    if (nrhs > 0)
+        CK(cudaMemcpy2DAsync(dB, ldd * sizeof(double), B, (size_t)m * sizeof(double),
+                             (size_t)m * sizeof(double), nrhs, cudaMemcpyHostToDevice, s), "B in");
+    const int pinned = lnb_host_is_pinned(A);
+    int e = lnb_chol_f64_run(c, m, b, dA, ldd, &ar, s, pinned ? A : NULL, m);
+    if (e) return e;
+    if (nrhs > 0) {
+        const int64_t nb = ceil_div(m, TRSV_H);
+        double *dinv = (double *)lnb_arena_take(&ar, (size_t)nb * TRSV_H * TRSV_H * sizeof(double));
+        CK(lnb_k_trtri_blocks_f64(dA, ldd, m, TRSV_H, 'L', 0, dinv, s), "trtri");
+        if ((e = lnb_trsm_f64_run(c, 'L', 'N', 'N', m, nrhs, 1.0, dA, ldd, dB, ldd, &ar, s, dinv))) return e;
+        if ((e = lnb_trsm_f64_run(c, 'L', 'T', 'N', m, nrhs, 1.0, dA, ldd, dB, ldd, &ar, s, dinv))) return e;
+        CK(cudaMemcpy2DAsync(B, (size_t)m * sizeof(double), dB, ldd * sizeof(double),
+                             (size_t)m * sizeof(double), nrhs, cudaMemcpyDeviceToHost, s), "X out");
+    }
+    if (!pinned)
+        for (int64_t c0 = 0; c0 < m; c0 += b) {
+            int64_t w = m - c0 < b ? m - c0 : b;
+            CK(cudaMemcpy2DAsync(A + c0 + c0 * (int64_t)m, (size_t)m * sizeof(double), dA + c0 + c0 * ldd,
+                                 ldd * sizeof(double), (size_t)(m - c0) * sizeof(double), w,
+                                 cudaMemcpyDeviceToHost, s), "L out");
+        }
+    return lnb_status_read(c, s);
+}
+
+int ompss_dtrsm(ompssblas_t side, ompssblas_t uplo, ompssblas_t trans, ompssblas_t diag, int m, int n,
+                int b, double alpha, double *A, int lda, double *B, int ldb)
+{
+    char cs = 0, cu = 0, ct = 0, cd = 0;
+    int e;
+    if ((e = opt_char(side, "LR", &cs, "side")) || (e = opt_char(uplo, "LU", &cu, "uplo")) ||
+        (e = opt_char(trans, "NT", &ct, "trans")) || (e = opt_char(diag, "NU", &cd, "diag")))
+        return e;
+    (void)b;
+    if (cs != 'L') return lnb_set_error(LNB_EINVAL, "rtrsm: not implemented (as in trsm_main.c:13)");
+    if (m < 0 || n < 0 || lda < (m > 1 ? m : 1) || ldb < (m > 1 ? m : 1))
+        return lnb_set_error(LNB_EINVAL, "dtrsm sizes");
+    if (m == 0 || n == 0) return 0;
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const int64_t ldd = ld_dev(m);
+    const size_t abytes = (size_t)ldd * m * sizeof(double), bbytes = (size_t)ldd * n * sizeof(double);
+    void *ws = lnb_ws(c, lnb_align256(abytes) + lnb_align256(bbytes) + lnb_trsm_f64_ws_bytes(m));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    double *dA = (double *)lnb_arena_take(&ar, abytes);
+    double *dB = (double *)lnb_arena_take(&ar, bbytes);
+    cudaStream_t s = c->main;
+    CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
+    CK(cudaMemcpy2DAsync(dA, ldd * sizeof(double), A, (size_t)lda * sizeof(double), (size_t)m * sizeof(double),
+                         m, cudaMemcpyHostToDevice, s), "A in");
+    CK(cudaMemcpy2DAsync(dB, ldd * sizeof(double), B, (size_t)ldb * sizeof(double), (size_t)m * sizeof(double),
+                         n, cudaMemcpyHostToDevice, s), "B in");
+    if ((e = lnb_trsm_f64_run(c, cu, ct, cd, m, n, alpha, dA, ldd, dB, ldd, &ar, s, NULL))) return e;
+    CK(cudaMemcpy2DAsync(B, (size_t)ldb * sizeof(double), dB, ldd * sizeof(double), (size_t)m * sizeof(double),
+                         n, cudaMemcpyDeviceToHost, s), "B out");
+    e = lnb_status_read(c, s);
+    return e < 0 ? e : 0;
+}
