@@ -31,9 +31,9 @@ __global__ void __launch_bounds__(256) k_potrf_f64(double *A, int64_t lda, int b
     extern __shared__ double sm[];
     constexpr int LDP = NB + 1;  // panel row stride (odd: spreads banks)
     double *Pn = sm;             // [bs][LDP], row r = tile row j0 + r
-    __shared__ int fail;
+    __shared__ int fail, fail_col;   // fail_col: tile-relative column of the bad pivot
     const int tid = threadIdx.x;
-    if (tid == 0) fail = 0;
+    if (tid == 0) { fail = 0; fail_col = bs; }
 
     for (int j0 = 0; j0 < bs; j0 += NB) {
         const int jb = min(NB, bs - j0);
@@ -51,6 +51,7 @@ __global__ void __launch_bounds__(256) k_potrf_f64(double *A, int64_t lda, int b
                 double d = Pn[c * LDP + c];
                 if (!(d > 0.0)) {
                     fail = 1;
+                    fail_col = j0 + c;
                     atomicCAS(&st->info, 0, (int)(row0 + j0 + c + 1));
                 } else {
                     Pn[c * LDP + c] = sqrt(d);
@@ -76,7 +77,7 @@ __global__ void __launch_bounds__(256) k_potrf_f64(double *A, int64_t lda, int b
             int c = idx / mr, r = idx - c * mr;
             if (r >= c) A[(int64_t)(j0 + r) + (int64_t)(j0 + c) * lda] = Pn[r * LDP + c];
         }
-        if (fail) return;
+        if (fail) break;
         // (e) rank-jb update of the trailing lower triangle of the tile
         const int tr = mr - jb;
         if (tr > 0) {
@@ -119,14 +120,19 @@ __global__ void __launch_bounds__(256) k_potrf_f64(double *A, int64_t lda, int b
         }
     }
     // (d) inverses of the 32x32 diagonal blocks of the factored tile, read
-    // back from global memory (one warp per block, one lane per column)
+    // back from global memory (one warp per block, one lane per column).
+    // After a failed pivot only the columns before it are factored: the
+    // inverses treat the rest as identity, so a panel solve that follows
+    // still produces exact values in those leading columns (as LAPACK's
+    // partial factor does).
     if (dinv != nullptr) {
         __threadfence_block();
         __syncthreads();
         const int lane = tid & 31, warp = tid >> 5;
         const int nq = (bs + 31) / 32;
+        const int lim = fail_col;
         for (int q = warp; q < nq; q += blockDim.x / 32) {
-            const int qn = min(32, bs - q * 32);
+            const int qn = max(0, min(32, lim - q * 32));
             const double *Lq = A + (int64_t)q * 32 * (lda + 1);
             double *D = dinv + (int64_t)q * 1024;
             const int c = lane;
