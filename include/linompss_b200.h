@@ -169,6 +169,12 @@ LNB_EXPORT int lnb_dtrsm_dev(char uplo, char trans, char diag, int m, int n, dou
 #define LNB_FACTOR_FP32    1   /* FP32 storage, SIMT FP32 updates */
 #define LNB_FACTOR_TF32X3  2   /* FP32 storage, 3xTF32 split on tcgen05 */
 #define LNB_FACTOR_BF16    3   /* per-tile-scaled BF16 on tcgen05, FP32 accumulate */
+#define LNB_FACTOR_TF32    4   /* FP32 storage, one TF32 product on tcgen05 */
+
+/* Update path of the FP32 factorizations (ompss_schol_*, lnb_schol_dev):
+ * LNB_FACTOR_FP32, LNB_FACTOR_TF32X3 (default), LNB_FACTOR_TF32 or
+ * LNB_FACTOR_BF16.  Process-wide setting. */
+LNB_EXPORT void lnb_set_factor_mode(int mode);
 
 typedef struct {
     int    factor;          /* LNB_FACTOR_* */

@@ -140,6 +140,33 @@ def ompss_dchol_nhll(mt: int, b: int, t: int, tiles: np.ndarray) -> int:
     return _chk(lib().ompss_dchol_nhll(C.c_int(mt), C.c_int(b), C.c_int(t), _tile_table(tiles)))
 
 
+def set_factor_mode(mode: int) -> None:
+    """Update path of the FP32 factorizations: FACTOR_FP32, FACTOR_TF32X3, FACTOR_TF32, FACTOR_BF16."""
+    lib().lnb_set_factor_mode(C.c_int(mode))
+
+
+def ompss_schol_rl(n: int, b: int, t: int, A: np.ndarray, lda: int) -> int:
+    _colmajor(A, np.float32)
+    return _chk(lib().ompss_schol_rl(C.c_int(n), C.c_int(b), C.c_int(t), _p(A), C.c_int(lda)))
+
+
+def ompss_schol_ll(n: int, b: int, t: int, A: np.ndarray, lda: int) -> int:
+    _colmajor(A, np.float32)
+    return _chk(lib().ompss_schol_ll(C.c_int(n), C.c_int(b), C.c_int(t), _p(A), C.c_int(lda)))
+
+
+def ompss_schol_hrl(mt: int, b: int, t: int, tiles: np.ndarray) -> int:
+    return _chk(lib().ompss_schol_hrl(C.c_int(mt), C.c_int(b), C.c_int(t), _tile_table(tiles)))
+
+
+def ompss_schol_hll(mt: int, b: int, t: int, tiles: np.ndarray) -> int:
+    return _chk(lib().ompss_schol_hll(C.c_int(mt), C.c_int(b), C.c_int(t), _tile_table(tiles)))
+
+
+def schol_dev(At, n: int, b: int, info=None, stream=None) -> int:
+    return _chk(lib().lnb_schol_dev(C.c_int(n), C.c_int(b), _p(At), C.c_int(_ld(At)), _p(info), _stream(stream)))
+
+
 def dspdsolv_main(m: int, n: int, b: int, A: np.ndarray, B: np.ndarray) -> int:
     _colmajor(A)
     _colmajor(B)

@@ -1,0 +1,307 @@
+// k_chol_f32.cu -- FP32-storage factorization kernels for the low-precision
+// factor of the mixed-precision solver (the FP32 twins of the tile tasks:
+// task_spotrf / task_strsm / task_ssyrk / task_sgemm, tasks_potrf.c,
+// tasks_trsm.c, tasks_syrk.c, task_gemm.c built with -DSINGLE_PRECISION).
+//
+//   potrf   : leaf diagonal tile in shared memory (k_potrf.cuh)
+//   trsm    : panel solve B <- B L^-T, SIMT, left-looking over 32-column blocks
+//             with the leaf's inverted 32x32 diagonal blocks
+//   syrk    : SIMT lower-triangle update (nested diagonal tiles; plain FP32 mode)
+//   prep    : column-major panel -> K-major operand copies for the tensor-core
+//             update: TF32 hi/lo split (x = hi + lo, hi = rna_tf32(x)), or BF16
+//             scaled by a power of two per 128-row block
+//   convert : FP64 A -> FP32 lower triangle with optional symmetric diagonal
+//             equilibration  As = S A S,  S = diag(1/sqrt(a_ii))
+#include "common.cuh"
+#include "k_potrf.cuh"
+
+#include <cuda_bf16.h>
+
+namespace lnb {
+
+// ------------------------------------------------------------------------
+// panel solve, FP32 SIMT: CTA = 64 rows, 256 threads (row r = tid%64, column
+// group cg = tid/64 of 8 columns inside each 32-column block)
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_trsm_rlt_f32(const float *__restrict__ L, int64_t lda,
+                                                      const float *__restrict__ dinv, float *B, int64_t ldb,
+                                                      int64_t m, int bs)
+{
+    __shared__ float Xs[64][33];
+    __shared__ float Ls[32][33];
+    __shared__ float Ts[64][33];
+    const int tid = threadIdx.x, r = tid & 63, cg = tid >> 6;
+    const int64_t rbase = (int64_t)blockIdx.x * 64;
+    const int64_t grow = rbase + r;
+    const int nblk = (bs + 31) / 32;
+    for (int jb = 0; jb < nblk; ++jb) {
+        const int jc = jb * 32;
+        float acc[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[c] = 0.f;
+        for (int kc = 0; kc < jc; kc += 32) {
+            for (int idx = tid; idx < 64 * 32; idx += 256) {
+                const int k = idx >> 6, rr = idx & 63;
+                const int64_t gr = rbase + rr;
+                Xs[rr][k] = gr < m ? __ldcg(&B[gr + (int64_t)(kc + k) * ldb]) : 0.f;
+            }
+            for (int idx = tid; idx < 32 * 32; idx += 256) {
+                const int k = idx >> 5, c = idx & 31;
+                Ls[c][k] = (jc + c < bs) ? L[(jc + c) + (int64_t)(kc + k) * lda] : 0.f;
+            }
+            __syncthreads();
+#pragma unroll 8
+            for (int k = 0; k < 32; ++k) {
+                const float x = Xs[r][k];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) acc[c] = fmaf(x, Ls[cg * 8 + c][k], acc[c]);
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int col = jc + cg * 8 + c;
+            float v = 0.f;
+            if (grow < m && col < bs) v = B[grow + (int64_t)col * ldb] - acc[c];
+            Ts[r][cg * 8 + c] = v;
+        }
+        for (int idx = tid; idx < 32 * 32; idx += 256) {
+            const int rr = idx & 31, k = idx >> 5;  // Ls[c][k] = Dinv(c, k)
+            Ls[rr][k] = dinv[(int64_t)jb * 1024 + rr + 32 * k];
+        }
+        __syncthreads();
+        float y[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) y[c] = 0.f;
+#pragma unroll 8
+        for (int k = 0; k < 32; ++k) {
+            const float tv = Ts[r][k];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) y[c] = fmaf(tv, Ls[cg * 8 + c][k], y[c]);
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int col = jc + cg * 8 + c;
+            if (grow < m && col < bs) B[grow + (int64_t)col * ldb] = y[c];
+        }
+        __threadfence_block();
+        __syncthreads();
+    }
+}
+
+// ------------------------------------------------------------------------
+// SIMT FP32 lower update C[r,c] -= sum_k P[r,k] P[c,k] (r >= c, c in [c0,c1))
+// 64x64 tiles, 256 threads, 4x4 per thread
+// ------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_syrk_lower_f32_simt(const float *__restrict__ P, int64_t ldp, float *C,
+                                                             int64_t ldc, int64_t nrows, int64_t c0, int64_t c1,
+                                                             int kdim)
+{
+    __shared__ float As[16][68], Bs[16][68];
+    const int64_t rbase = c0 + (int64_t)blockIdx.y * 64, cbase = c0 + (int64_t)blockIdx.x * 64;
+    if (rbase + 64 <= cbase || rbase >= nrows || cbase >= c1) return;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    float acc[4][4] = {};
+    for (int k0 = 0; k0 < kdim; k0 += 16) {
+        for (int idx = threadIdx.x; idx < 16 * 64; idx += 256) {
+            const int kk = idx >> 6, mm = idx & 63;
+            const bool kin = k0 + kk < kdim;
+            const int64_t ra = rbase + mm, rb = cbase + mm;
+            As[kk][mm] = (kin && ra < nrows) ? P[ra + (int64_t)(k0 + kk) * ldp] : 0.f;
+            Bs[kk][mm] = (kin && rb < nrows) ? P[rb + (int64_t)(k0 + kk) * ldp] : 0.f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            float a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { a[i] = As[kk][ty + 16 * i]; b[i] = Bs[kk][tx + 16 * i]; }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t r = rbase + ty + 16 * i, c = cbase + tx + 16 * j;
+            if (r < nrows && c < c1 && r >= c) C[r + c * ldc] -= acc[i][j];
+        }
+}
+
+// ------------------------------------------------------------------------
+// panel prep: X (m x kb, column-major FP32) -> K-major operand copies
+// ------------------------------------------------------------------------
+LNB_DEV float tf32_rna(float x)
+{
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// mode 0: hi/lo TF32 split into two fp32 arrays; mode 1: hi only
+__global__ void __launch_bounds__(256) k_prep_tf32(const float *__restrict__ X, int64_t ldx, int64_t m, int kb,
+                                                   int kpad, float *hi, float *lo)
+{
+    __shared__ float t[32][33];
+    const int64_t r0 = (int64_t)blockIdx.x * 32;
+    const int k0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 8 rows of 32
+    for (int i = ty; i < 32; i += 8) {                        // read column k0+i, rows r0+tx
+        const int k = k0 + i;
+        const int64_t r = r0 + tx;
+        t[i][tx] = (k < kb && r < m) ? X[r + (int64_t)k * ldx] : 0.f;
+    }
+    __syncthreads();
+    for (int i = ty; i < 32; i += 8) {                        // write row r0+i, k0+tx
+        const int64_t r = r0 + i;
+        const int k = k0 + tx;
+        if (r < m && k < kpad) {
+            const float x = t[tx][i];
+            const float h = tf32_rna(x);
+            hi[r * kpad + k] = h;
+            if (lo) lo[r * kpad + k] = x - h;
+        }
+    }
+}
+
+// per 128-row block: scale = smallest power of two >= max |x| (1 if the block is zero)
+__global__ void __launch_bounds__(256) k_prep_bf16_scale(const float *__restrict__ X, int64_t ldx, int64_t m, int kb,
+                                                         float *scale)
+{
+    __shared__ float red[256];
+    const int64_t r0 = (int64_t)blockIdx.x * 128;
+    float mx = 0.f;
+    for (int idx = threadIdx.x; idx < 128 * kb; idx += 256) {
+        const int k = idx / 128, rr = idx % 128;
+        const int64_t r = r0 + rr;
+        if (r < m) mx = fmaxf(mx, fabsf(X[r + (int64_t)k * ldx]));
+    }
+    red[threadIdx.x] = mx;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] = fmaxf(red[threadIdx.x], red[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const float v = red[0];
+        scale[blockIdx.x] = v > 0.f ? exp2f(ceilf(log2f(v))) : 1.f;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_prep_bf16(const float *__restrict__ X, int64_t ldx, int64_t m, int kb,
+                                                   int kpad, const float *__restrict__ scale, __nv_bfloat16 *out)
+{
+    __shared__ float t[32][33];
+    const int64_t r0 = (int64_t)blockIdx.x * 32;
+    const int k0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int i = ty; i < 32; i += 8) {
+        const int k = k0 + i;
+        const int64_t r = r0 + tx;
+        t[i][tx] = (k < kb && r < m) ? X[r + (int64_t)k * ldx] : 0.f;
+    }
+    __syncthreads();
+    for (int i = ty; i < 32; i += 8) {
+        const int64_t r = r0 + i;
+        const int k = k0 + tx;
+        if (r < m && k < kpad) out[r * kpad + k] = __float2bfloat16_rn(t[tx][i] / scale[r >> 7]);
+    }
+}
+
+// ------------------------------------------------------------------------
+// conversions
+// ------------------------------------------------------------------------
+// s[i] = 1/sqrt(a_ii) (or 1 when equilibration is off / a_ii <= 0)
+__global__ void k_equil_scale(const double *A, int64_t lda, int64_t n, int on, double *s)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double d = A[i + i * lda];
+        s[i] = (on && d > 0.0) ? 1.0 / sqrt(d) : 1.0;
+    }
+}
+
+// lower triangle of S A S in FP32 (column-major, ld32); column j per blockIdx.y
+__global__ void k_lower_to_f32(const double *__restrict__ A, int64_t lda, int64_t n, const double *__restrict__ s,
+                               float *A32, int64_t ld32)
+{
+    for (int64_t j = blockIdx.y; j < n; j += gridDim.y) {
+        const double sj = s[j];
+        for (int64_t i = j + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+             i += (int64_t)gridDim.x * blockDim.x)
+            A32[i + j * ld32] = (float)(A[i + j * lda] * s[i] * sj);
+    }
+}
+
+}  // namespace lnb
+
+using namespace lnb;
+
+extern "C" int lnb_k_potrf_f32(float *A, int64_t lda, int bs, int64_t row0, float *dinv, lnb_status_t *st,
+                               lnb_stream_t s)
+{
+    if (bs <= 0) return 0;
+    if (bs > LEAF) return (int)cudaErrorInvalidValue;
+    const int smem = (bs * (bs + 1) + 4 * 32 * 33) * (int)sizeof(float);
+    cudaFuncSetAttribute(k_potrf_leaf<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_potrf_leaf<float><<<1, 256, smem, s>>>(A, lda, bs, row0, dinv, st);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int lnb_k_trsm_rlt_f32(const float *L, int64_t lda, const float *dinv, float *B, int64_t ldb, int64_t m,
+                                  int bs, lnb_stream_t s)
+{
+    if (m <= 0 || bs <= 0) return 0;
+    k_trsm_rlt_f32<<<(unsigned)((m + 63) / 64), 256, 0, s>>>(L, lda, dinv, B, ldb, m, bs);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int lnb_k_syrk_lower_f32_simt(const float *P, int64_t ldp, float *C, int64_t ldc, int64_t nrows,
+                                         int64_t c0, int64_t c1, int kdim, lnb_stream_t s)
+{
+    if (nrows <= c0 || c1 <= c0 || kdim <= 0) return 0;
+    dim3 grid((unsigned)((c1 - c0 + 63) / 64), (unsigned)((nrows - c0 + 63) / 64));
+    k_syrk_lower_f32_simt<<<grid, 256, 0, s>>>(P, ldp, C, ldc, nrows, c0, c1, kdim);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int lnb_k_prep_tf32(const float *X, int64_t ldx, int64_t m, int kb, int kpad, float *hi, float *lo,
+                               lnb_stream_t s)
+{
+    if (m <= 0) return 0;
+    dim3 grid((unsigned)((m + 31) / 32), (unsigned)((kpad + 31) / 32));
+    k_prep_tf32<<<grid, 256, 0, s>>>(X, ldx, m, kb, kpad, hi, lo);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int lnb_k_prep_bf16(const float *X, int64_t ldx, int64_t m, int kb, int kpad, float *scale, void *out,
+                               lnb_stream_t s)
+{
+    if (m <= 0) return 0;
+    k_prep_bf16_scale<<<(unsigned)((m + 127) / 128), 256, 0, s>>>(X, ldx, m, kb, scale);
+    lnb_prof_count(1);
+    dim3 grid((unsigned)((m + 31) / 32), (unsigned)((kpad + 31) / 32));
+    k_prep_bf16<<<grid, 256, 0, s>>>(X, ldx, m, kb, kpad, scale, (__nv_bfloat16 *)out);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int lnb_k_lower_to_f32(const double *A, int64_t lda, int64_t n, int equilibrate, double *s_out,
+                                  float *A32, int64_t ld32, lnb_stream_t s)
+{
+    if (n <= 0) return 0;
+    k_equil_scale<<<(unsigned)((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024), 256, 0, s>>>(A, lda, n, equilibrate,
+                                                                                             s_out);
+    lnb_prof_count(1);
+    dim3 grid((unsigned)((n + 255) / 256 < 32 ? (n + 255) / 256 : 32), (unsigned)(n < 65535 ? n : 65535));
+    k_lower_to_f32<<<grid, 256, 0, s>>>(A, lda, n, s_out, A32, ld32);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}

@@ -1,7 +1,7 @@
 // k_chol_f64.cu -- FP64 tile kernels of the right-looking tile Cholesky.
 //
-//  K1 potrf   : one diagonal tile, one CTA, shared-memory staged column panels
-//               (semantics of task_dpotrf -> LAPACK dpotrf 'L',
+//  K1 potrf   : leaf diagonal tile (<= 128), one CTA, tile resident in shared
+//               memory (k_potrf.cuh; task_dpotrf -> LAPACK dpotrf 'L',
 //               tasks_potrf.c:20-24; info is reported, not dropped)
 //  K2 trsm    : panel solve B <- B L^-T (task_dtrsm(R,L,T,N), chol_rlmain.c:35-38)
 //               on DMMA, left-looking over 32-column blocks, multiplying by the
@@ -11,146 +11,12 @@
 //               k-step fused into one launch, 128x128 CTA tiles on DMMA with a
 //               4-stage cp.async pipeline
 #include "common.cuh"
+#include "k_potrf.cuh"
 
 #include <math.h>
+#include <stdlib.h>
 
 namespace lnb {
-
-// ========================================================================
-// K1: diagonal tile factorization
-// ========================================================================
-// The tile (bs x bs, column-major, ld lda) stays in global memory (it is
-// L2-resident); each NB-wide column panel is staged in shared memory,
-// factored column by column, written back, and applied to the rest of the
-// tile as a register-blocked (8x8 per thread) rank-NB update of the lower
-// triangle.
-template <int NB>
-__global__ void __launch_bounds__(256) k_potrf_f64(double *A, int64_t lda, int bs, int64_t row0,
-                                                   double *dinv, lnb_status_t *st)
-{
-    extern __shared__ double sm[];
-    constexpr int LDP = NB + 1;  // panel row stride (odd: spreads banks)
-    double *Pn = sm;             // [bs][LDP], row r = tile row j0 + r
-    __shared__ int fail, fail_col;   // fail_col: tile-relative column of the bad pivot
-    const int tid = threadIdx.x;
-    if (tid == 0) { fail = 0; fail_col = bs; }
-
-    for (int j0 = 0; j0 < bs; j0 += NB) {
-        const int jb = min(NB, bs - j0);
-        const int mr = bs - j0;
-        __syncthreads();
-        // (a) stage panel: rows j0..bs, cols j0..j0+jb
-        for (int idx = tid; idx < mr * jb; idx += blockDim.x) {
-            int c = idx / mr, r = idx - c * mr;
-            Pn[r * LDP + c] = A[(int64_t)(j0 + r) + (int64_t)(j0 + c) * lda];
-        }
-        __syncthreads();
-        // (b) factor the panel column by column
-        for (int c = 0; c < jb; ++c) {
-            if (tid == 0) {
-                double d = Pn[c * LDP + c];
-                if (!(d > 0.0)) {
-                    fail = 1;
-                    fail_col = j0 + c;
-                    atomicCAS(&st->info, 0, (int)(row0 + j0 + c + 1));
-                } else {
-                    Pn[c * LDP + c] = sqrt(d);
-                }
-            }
-            __syncthreads();
-            if (fail) break;
-            const double dc = Pn[c * LDP + c];
-            for (int r = c + 1 + tid; r < mr; r += blockDim.x) Pn[r * LDP + c] /= dc;
-            __syncthreads();
-            const int w = jb - c - 1;
-            if (w > 0) {
-                const int rows = mr - c - 1;
-                for (int idx = tid; idx < rows * w; idx += blockDim.x) {
-                    int r = c + 1 + idx / w, cc = c + 1 + idx % w;
-                    if (r >= cc) Pn[r * LDP + cc] -= Pn[r * LDP + c] * Pn[cc * LDP + c];
-                }
-            }
-            __syncthreads();
-        }
-        // (c) write the factored panel back (lower part only)
-        for (int idx = tid; idx < mr * jb; idx += blockDim.x) {
-            int c = idx / mr, r = idx - c * mr;
-            if (r >= c) A[(int64_t)(j0 + r) + (int64_t)(j0 + c) * lda] = Pn[r * LDP + c];
-        }
-        if (fail) break;
-        // (e) rank-jb update of the trailing lower triangle of the tile
-        const int tr = mr - jb;
-        if (tr > 0) {
-            const int nb8 = (tr + 7) / 8;
-            const int nblk = nb8 * (nb8 + 1) / 2;
-            for (int id = tid; id < nblk; id += blockDim.x) {
-                int bi = (int)((sqrtf(8.0f * id + 1.0f) - 1.0f) * 0.5f);
-                while (bi * (bi + 1) / 2 > id) --bi;
-                while ((bi + 1) * (bi + 2) / 2 <= id) ++bi;
-                const int bj = id - bi * (bi + 1) / 2;
-                double acc[8][8];
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
-                const int ra = jb + bi * 8, rb = jb + bj * 8;
-                for (int p = 0; p < jb; ++p) {
-                    double a[8], b[8];
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        a[i] = (ra + i < mr) ? Pn[(ra + i) * LDP + p] : 0.0;
-                        b[i] = (rb + i < mr) ? Pn[(rb + i) * LDP + p] : 0.0;
-                    }
-#pragma unroll
-                    for (int i = 0; i < 8; ++i)
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-                }
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int c = rb + j;
-                    if (c >= mr) continue;
-#pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const int r = ra + i;
-                        if (r < mr && r >= c) A[(int64_t)(j0 + r) + (int64_t)(j0 + c) * lda] -= acc[i][j];
-                    }
-                }
-            }
-        }
-    }
-    // (d) inverses of the 32x32 diagonal blocks of the factored tile, read
-    // back from global memory (one warp per block, one lane per column).
-    // After a failed pivot only the columns before it are factored: the
-    // inverses treat the rest as identity, so a panel solve that follows
-    // still produces exact values in those leading columns (as LAPACK's
-    // partial factor does).
-    if (dinv != nullptr) {
-        __threadfence_block();
-        __syncthreads();
-        const int lane = tid & 31, warp = tid >> 5;
-        const int nq = (bs + 31) / 32;
-        const int lim = fail_col;
-        for (int q = warp; q < nq; q += blockDim.x / 32) {
-            const int qn = max(0, min(32, lim - q * 32));
-            const double *Lq = A + (int64_t)q * 32 * (lda + 1);
-            double *D = dinv + (int64_t)q * 1024;
-            const int c = lane;
-            for (int r = 0; r < 32; ++r) {
-                double v;
-                if (c >= qn) v = (r == c) ? 1.0 : 0.0;       // identity padding
-                else if (r < c || r >= qn) v = 0.0;
-                else if (r == c) v = 1.0 / Lq[(int64_t)c * (lda + 1)];
-                else {
-                    double s = 0.0;
-                    for (int p = c; p < r; ++p) s += Lq[r + (int64_t)p * lda] * D[p + 32 * c];
-                    v = -s / Lq[(int64_t)r * (lda + 1)];
-                }
-                D[r + 32 * c] = v;
-            }
-        }
-    }
-}
 
 // ========================================================================
 // DMMA building blocks
@@ -162,80 +28,77 @@ __global__ void __launch_bounds__(256) k_potrf_f64(double *A, int64_t lda, int b
 // ========================================================================
 // K3/K4: fused trailing update of one k-step, lower triangle only
 // ========================================================================
-namespace syrk {
-constexpr int BM = 128, BN = 128, BK = 16, ST = 4, LDS = BM + 4;
-constexpr int SMEM = 2 * ST * BK * LDS * (int)sizeof(double);
-}
+// Tile shapes are template parameters (CTA tile BM x BN, warp grid WM x WN,
+// ST pipeline stages); the launcher picks one (see lnb_k_syrk_lower_f64).
+template <int BM, int BN, int WM, int WN, int ST>
+struct SyrkCfg {
+    static constexpr int BK = 16;
+    static constexpr int THREADS = 32 * WM * WN;
+    static constexpr int LDA = BM + 4, LDB = BN + 4;     // k-major rows, = 4 mod 16 doubles
+    static constexpr int TM = BM / WM, TN = BN / WN;    // warp tile
+    static constexpr int MI = TM / 16, NI = TN / 8;     // DMMA tiles per warp
+    static constexpr int SMEM = ST * BK * (LDA + LDB) * (int)sizeof(double);
+};
 
-template <bool VEC16>
-__global__ void __launch_bounds__(256) k_syrk_lower_f64(const double *__restrict__ P, int64_t ldp,
-                                                        double *C, int64_t ldc, int64_t nrows,
-                                                        int64_t c0, int64_t c1, int kdim)
+template <class Cfg, int ST, bool VEC16>
+__global__ void __launch_bounds__(Cfg::THREADS) k_syrk_lower_f64(const double *__restrict__ P, int64_t ldp,
+                                                                 double *C, int64_t ldc, int64_t nrows,
+                                                                 int64_t c0, int64_t c1, int kdim)
 {
-    using namespace syrk;
+    constexpr int BK = Cfg::BK, LDA = Cfg::LDA, LDB = Cfg::LDB, THREADS = Cfg::THREADS;
+    constexpr int BM = Cfg::LDA - 4, BN = Cfg::LDB - 4;
+    constexpr int MI = Cfg::MI, NI = Cfg::NI, TM = Cfg::TM, TN = Cfg::TN;
+    constexpr int WN = BN / TN;
     const int tj = blockIdx.x, ti = blockIdx.y;
-    if (ti < tj) return;
     const int64_t rbase = c0 + (int64_t)ti * BM, cbase = c0 + (int64_t)tj * BN;
+    if (rbase + BM <= cbase) return;               // tile entirely above the diagonal
     if (rbase >= nrows || cbase >= c1) return;
 
     extern __shared__ double sm[];
-    double *As = sm;                     // [ST][BK][LDS]
-    double *Bs = sm + ST * BK * LDS;     // [ST][BK][LDS]
+    double *As = sm;                     // [ST][BK][LDA]
+    double *Bs = sm + ST * BK * LDA;     // [ST][BK][LDB]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wm = warp >> 2, wn = warp & 3;  // 2 x 4 warps, warp tile 64 x 32
+    const int wm = warp / WN, wn = warp % WN;
     const int g = lane >> 2, t = lane & 3;
 
     const int ktiles = (kdim + BK - 1) / BK;
 
-    auto load_stage = [&](int stage, int kt) {
-        const int k0 = kt * BK;
-        double *as = As + stage * BK * LDS, *bs = Bs + stage * BK * LDS;
+    auto load_rows = [&](double *dst, int ld, int64_t base, int rows, int k0) {
         if (VEC16) {
-#pragma unroll
-            for (int it = 0; it < (BK * BM / 2) / 256; ++it) {
-                const int idx = tid + it * 256;
-                const int kk = idx / (BM / 2), m2 = (idx % (BM / 2)) * 2;
+            for (int idx = tid; idx < BK * rows / 2; idx += THREADS) {
+                const int kk = idx / (rows / 2), m2 = (idx % (rows / 2)) * 2;
                 const bool kin = (k0 + kk) < kdim;
                 const double *colp = P + (int64_t)(kin ? k0 + kk : 0) * ldp;
-                {
-                    const int64_t r = rbase + m2;
-                    if (r + 1 < nrows) cp_async16(&as[kk * LDS + m2], colp + r, kin);
-                    else {
-                        const bool ok = kin && r < nrows;
-                        cp_async8(&as[kk * LDS + m2], colp + (ok ? r : 0), ok);
-                        cp_async8(&as[kk * LDS + m2 + 1], colp, false);
-                    }
-                }
-                {
-                    const int64_t r = cbase + m2;
-                    if (r + 1 < nrows) cp_async16(&bs[kk * LDS + m2], colp + r, kin);
-                    else {
-                        const bool ok = kin && r < nrows;
-                        cp_async8(&bs[kk * LDS + m2], colp + (ok ? r : 0), ok);
-                        cp_async8(&bs[kk * LDS + m2 + 1], colp, false);
-                    }
+                const int64_t r = base + m2;
+                if (r + 1 < nrows) {
+                    cp_async16(&dst[kk * ld + m2], colp + r, kin);
+                } else {
+                    const bool ok = kin && r < nrows;
+                    cp_async8(&dst[kk * ld + m2], colp + (ok ? r : 0), ok);
+                    cp_async8(&dst[kk * ld + m2 + 1], colp, false);
                 }
             }
         } else {
-#pragma unroll
-            for (int it = 0; it < (BK * BM) / 256; ++it) {
-                const int idx = tid + it * 256;
-                const int kk = idx / BM, m = idx % BM;
+            for (int idx = tid; idx < BK * rows; idx += THREADS) {
+                const int kk = idx / rows, m = idx % rows;
                 const bool kin = (k0 + kk) < kdim;
                 const double *colp = P + (int64_t)(kin ? k0 + kk : 0) * ldp;
-                const int64_t ra = rbase + m, rb = cbase + m;
-                cp_async8(&as[kk * LDS + m], colp + (ra < nrows ? ra : 0), kin && ra < nrows);
-                cp_async8(&bs[kk * LDS + m], colp + (rb < nrows ? rb : 0), kin && rb < nrows);
+                const int64_t r = base + m;
+                cp_async8(&dst[kk * ld + m], colp + (r < nrows ? r : 0), kin && r < nrows);
             }
         }
     };
+    auto load_stage = [&](int stage, int kt) {
+        load_rows(As + stage * BK * LDA, LDA, rbase, BM, kt * BK);
+        load_rows(Bs + stage * BK * LDB, LDB, cbase, BN, kt * BK);
+    };
 
-    double acc[4][4][4];
+    double acc[MI][NI][4];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < MI; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < NI; ++j)
 #pragma unroll
             for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
 
@@ -253,37 +116,37 @@ __global__ void __launch_bounds__(256) k_syrk_lower_f64(const double *__restrict
             if (nk < ktiles) load_stage(nk % ST, nk);
             cp_async_commit();
         }
-        const double *as = As + (kt % ST) * BK * LDS;
-        const double *bs = Bs + (kt % ST) * BK * LDS;
+        const double *as = As + (kt % ST) * BK * LDA;
+        const double *bs = Bs + (kt % ST) * BK * LDB;
 #pragma unroll
         for (int kq = 0; kq < BK / 4; ++kq) {
-            const double *ak = as + (kq * 4 + t) * LDS;
-            const double *bk = bs + (kq * 4 + t) * LDS;
-            double a0[4], a1[4], b0[4];
+            const double *ak = as + (kq * 4 + t) * LDA + wm * TM;
+            const double *bk = bs + (kq * 4 + t) * LDB + wn * TN;
+            double a0[MI], a1[MI], b0[NI];
 #pragma unroll
-            for (int mi = 0; mi < 4; ++mi) {
-                a0[mi] = ak[wm * 64 + mi * 16 + g];
-                a1[mi] = ak[wm * 64 + mi * 16 + g + 8];
+            for (int mi = 0; mi < MI; ++mi) {
+                a0[mi] = ak[mi * 16 + g];
+                a1[mi] = ak[mi * 16 + g + 8];
             }
 #pragma unroll
-            for (int ni = 0; ni < 4; ++ni) b0[ni] = bk[wn * 32 + ni * 8 + g];
+            for (int ni = 0; ni < NI; ++ni) b0[ni] = bk[ni * 8 + g];
 #pragma unroll
-            for (int mi = 0; mi < 4; ++mi)
+            for (int mi = 0; mi < MI; ++mi)
 #pragma unroll
-                for (int ni = 0; ni < 4; ++ni) dmma16x8x4(acc[mi][ni], a0[mi], a1[mi], b0[ni]);
+                for (int ni = 0; ni < NI; ++ni) dmma16x8x4(acc[mi][ni], a0[mi], a1[mi], b0[ni]);
         }
     }
     cp_async_wait<0>();
 
     // epilogue: C -= acc on r >= c inside [0,nrows) x [c0,c1)
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi) {
+    for (int mi = 0; mi < MI; ++mi) {
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) {
+        for (int ni = 0; ni < NI; ++ni) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int64_t r = rbase + wm * 64 + mi * 16 + g + ((q & 2) ? 8 : 0);
-                const int64_t c = cbase + wn * 32 + ni * 8 + 2 * t + (q & 1);
+                const int64_t r = rbase + wm * TM + mi * 16 + g + ((q & 2) ? 8 : 0);
+                const int64_t c = cbase + wn * TN + ni * 8 + 2 * t + (q & 1);
                 if (r < nrows && c < c1 && r >= c) C[r + c * ldc] -= acc[mi][ni][q];
             }
         }
@@ -492,19 +355,11 @@ extern "C" int lnb_k_potrf_f64(double *A, int64_t lda, int bs, int64_t row0, dou
                                lnb_status_t *st, lnb_stream_t s)
 {
     if (bs <= 0) return 0;
-    if (bs <= 512) {
-        const int smem = bs * 33 * (int)sizeof(double);
-        cudaFuncSetAttribute(k_potrf_f64<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_potrf_f64<32><<<1, 256, smem, s>>>(A, lda, bs, row0, dinv, st);
-        lnb_prof_count(1);
-    } else if (bs <= 1024) {
-        const int smem = bs * 17 * (int)sizeof(double);
-        cudaFuncSetAttribute(k_potrf_f64<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_potrf_f64<16><<<1, 256, smem, s>>>(A, lda, bs, row0, dinv, st);
-        lnb_prof_count(1);
-    } else {
-        return (int)cudaErrorInvalidValue;
-    }
+    if (bs > LEAF) return (int)cudaErrorInvalidValue;
+    const int smem = (bs * (bs + 1) + 4 * 32 * 33) * (int)sizeof(double);
+    cudaFuncSetAttribute(k_potrf_leaf<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_potrf_leaf<double><<<1, 256, smem, s>>>(A, lda, bs, row0, dinv, st);
+    lnb_prof_count(1);
     return (int)cudaGetLastError();
 }
 
@@ -519,24 +374,44 @@ extern "C" int lnb_k_trsm_rlt_f64(const double *L, int64_t lda, const double *di
     return (int)cudaGetLastError();
 }
 
+template <int BM, int BN, int WM, int WN, int ST>
+static int launch_syrk(const double *P, int64_t ldp, double *C, int64_t ldc, int64_t nrows, int64_t c0,
+                       int64_t c1, int kdim, lnb_stream_t s)
+{
+    using Cfg = SyrkCfg<BM, BN, WM, WN, ST>;
+    const int64_t tiles_c = (c1 - c0 + BN - 1) / BN;
+    const int64_t tiles_r = (nrows - c0 + BM - 1) / BM;
+    dim3 grid((unsigned)tiles_c, (unsigned)tiles_r);
+    const bool vec = ((uintptr_t)P % 16 == 0) && (ldp % 2 == 0) && (c0 % 2 == 0);
+    if (vec) {
+        cudaFuncSetAttribute(k_syrk_lower_f64<Cfg, ST, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+        k_syrk_lower_f64<Cfg, ST, true><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(P, ldp, C, ldc, nrows, c0, c1, kdim);
+    } else {
+        cudaFuncSetAttribute(k_syrk_lower_f64<Cfg, ST, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM);
+        k_syrk_lower_f64<Cfg, ST, false><<<grid, Cfg::THREADS, Cfg::SMEM, s>>>(P, ldp, C, ldc, nrows, c0, c1, kdim);
+    }
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+
+static int g_syrk_cfg = -1;
+
+// Tile shape of the trailing update.  0: 128x128 (8 warps, 4 stages);
+// 1: 64x64 (4 warps, 4 stages); 2: 128x64 (4 warps, 3 stages).  The default
+// is the measured-fastest on B200; LNB_SYRK_TILE overrides it (tuning).
 extern "C" int lnb_k_syrk_lower_f64(const double *P, int64_t ldp, double *C, int64_t ldc,
                                     int64_t nrows, int64_t c0, int64_t c1, int kdim, lnb_stream_t s)
 {
     if (nrows <= c0 || c1 <= c0 || kdim <= 0) return 0;
-    const int64_t tiles_c = (c1 - c0 + syrk::BN - 1) / syrk::BN;
-    const int64_t tiles_r = (nrows - c0 + syrk::BM - 1) / syrk::BM;
-    dim3 grid((unsigned)tiles_c, (unsigned)tiles_r);
-    const bool vec = ((uintptr_t)P % 16 == 0) && (ldp % 2 == 0) && (c0 % 2 == 0);
-    if (vec) {
-        cudaFuncSetAttribute(k_syrk_lower_f64<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, syrk::SMEM);
-        k_syrk_lower_f64<true><<<grid, 256, syrk::SMEM, s>>>(P, ldp, C, ldc, nrows, c0, c1, kdim);
-        lnb_prof_count(1);
-    } else {
-        cudaFuncSetAttribute(k_syrk_lower_f64<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, syrk::SMEM);
-        k_syrk_lower_f64<false><<<grid, 256, syrk::SMEM, s>>>(P, ldp, C, ldc, nrows, c0, c1, kdim);
-        lnb_prof_count(1);
+    if (g_syrk_cfg < 0) {
+        const char *e = getenv("LNB_SYRK_TILE");
+        g_syrk_cfg = e ? atoi(e) : 1;
     }
-    return (int)cudaGetLastError();
+    switch (g_syrk_cfg) {
+    case 1: return launch_syrk<64, 64, 2, 2, 4>(P, ldp, C, ldc, nrows, c0, c1, kdim, s);
+    case 2: return launch_syrk<128, 64, 2, 2, 3>(P, ldp, C, ldc, nrows, c0, c1, kdim, s);
+    default: return launch_syrk<128, 128, 2, 4, 4>(P, ldp, C, ldc, nrows, c0, c1, kdim, s);
+    }
 }
 
 extern "C" int lnb_k_gemm_f64(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,

@@ -30,8 +30,9 @@ constexpr int NRC = 64;         // rhs columns per pass
 // ------------------------------------------------------------------------
 // inverses of the diagonal blocks
 // ------------------------------------------------------------------------
-__global__ void __launch_bounds__(TH) k_trtri_blocks_f64(const double *T, int64_t ldt, int64_t n,
-                                                         char uplo, int unit, double *dinv)
+template <typename TT>
+__global__ void __launch_bounds__(TH) k_trtri_blocks(const TT *T, int64_t ldt, int64_t n, char uplo, int unit,
+                                                     double *dinv)
 {
     extern __shared__ double smx[];
     double (*X)[TH + 1] = reinterpret_cast<double (*)[TH + 1]>(smx);              // X[r][c], column c owned by thread c
@@ -41,7 +42,7 @@ __global__ void __launch_bounds__(TH) k_trtri_blocks_f64(const double *T, int64_
     const int qn = (int)((n - o) < TH ? (n - o) : TH);
     for (int r = 0; r < TH; ++r) {
         double v = 0.0;
-        if (r < qn && c < qn) v = T[(o + r) + (o + c) * ldt];
+        if (r < qn && c < qn) v = (double)T[(o + r) + (o + c) * ldt];
         Tb[r][c] = v;
     }
     __syncthreads();
@@ -73,8 +74,9 @@ __global__ void __launch_bounds__(TH) k_trtri_blocks_f64(const double *T, int64_
 // ------------------------------------------------------------------------
 // the DAG walk
 // ------------------------------------------------------------------------
+template <typename TT>
 struct TrsmArgs {
-    const double *T; int64_t ldt; const double *dinv;
+    const TT *T; int64_t ldt; const double *dinv;
     double *B; int64_t ldb; int64_t n, nrhs;
     int nb; int fwd; int tT;   // tT: op(T) = T^T
     int *ticket, *cnt, *ready;
@@ -99,7 +101,8 @@ LNB_DEV void tile_mma(const double *As, const double *Bs, double (&acc)[NRC / 8]
     }
 }
 
-__global__ void __launch_bounds__(128) k_trsm_dag_f64(TrsmArgs a)
+template <typename TT>
+__global__ void __launch_bounds__(128) k_trsm_dag(TrsmArgs<TT> a)
 {
     extern __shared__ double smd[];
     double *As = smd;              // [TH][TLD]
@@ -177,14 +180,14 @@ __global__ void __launch_bounds__(128) k_trsm_dag_f64(TrsmArgs a)
                 for (int idx = tid; idx < TH * TH; idx += 128) {
                     const int k = idx / TH, m = idx % TH;
                     double v = 0.0;
-                    if (m < in_ && k < jn) v = a.T[(oi + m) + (oj + k) * a.ldt];
+                    if (m < in_ && k < jn) v = (double)a.T[(oi + m) + (oj + k) * a.ldt];
                     As[k * TLD + m] = v;
                 }
             } else {
                 for (int idx = tid; idx < TH * TH; idx += 128) {
                     const int m = idx / TH, k = idx % TH;  // op(T)[oi+m][oj+k] = T[oj+k][oi+m]
                     double v = 0.0;
-                    if (m < in_ && k < jn) v = a.T[(oj + k) + (oi + m) * a.ldt];
+                    if (m < in_ && k < jn) v = (double)a.T[(oj + k) + (oi + m) * a.ldt];
                     As[k * TLD + m] = v;
                 }
             }
@@ -239,23 +242,23 @@ extern "C" int64_t lnb_trsm_sync_ints(int64_t n, int h)
     return 4 + 2 * nb;
 }
 
-extern "C" int lnb_k_trtri_blocks_f64(const double *T, int64_t ldt, int64_t n, int h, char uplo,
-                                      int unit, double *dinv, lnb_stream_t s)
+template <typename TT>
+static int trtri_blocks(const TT *T, int64_t ldt, int64_t n, int h, char uplo, int unit, double *dinv, lnb_stream_t s)
 {
     if (h != TH) return (int)cudaErrorInvalidValue;
     if (n <= 0) return 0;
     const int64_t nb = (n + TH - 1) / TH;
     const int smem = 2 * TH * (TH + 1) * (int)sizeof(double);
-    cudaFuncSetAttribute(k_trtri_blocks_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    k_trtri_blocks_f64<<<(unsigned)nb, TH, smem, s>>>(T, ldt, n, uplo, unit, dinv);
+    cudaFuncSetAttribute(k_trtri_blocks<TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_trtri_blocks<TT><<<(unsigned)nb, TH, smem, s>>>(T, ldt, n, uplo, unit, dinv);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }
 
-extern "C" int lnb_k_trsm_left_f64(char uplo, char trans, int64_t n, int64_t nrhs, double alpha,
-                                   const double *T, int64_t ldt, const double *dinv, int h, double *B,
-                                   int64_t ldb, int *sync, lnb_status_t *st, long long wait_ns,
-                                   int ticket0, lnb_stream_t s)
+template <typename TT>
+static int trsm_left(char uplo, char trans, int64_t n, int64_t nrhs, double alpha, const TT *T, int64_t ldt,
+                     const double *dinv, int h, double *B, int64_t ldb, int *sync, lnb_status_t *st,
+                     long long wait_ns, int ticket0, lnb_stream_t s)
 {
     if (h != TH) return (int)cudaErrorInvalidValue;
     if (n <= 0 || nrhs <= 0) return 0;
@@ -272,7 +275,7 @@ extern "C" int lnb_k_trsm_left_f64(char uplo, char trans, int64_t n, int64_t nrh
         e = cudaMemsetAsync(sync, ticket0 & 0xff, 1, s);  // ticket starts past item 0
         if (e != cudaSuccess) return (int)e;
     }
-    TrsmArgs a;
+    TrsmArgs<TT> a;
     a.T = T; a.ldt = ldt; a.dinv = dinv; a.B = B; a.ldb = ldb; a.n = n; a.nrhs = nrhs;
     a.nb = (int)((n + TH - 1) / TH);
     const bool lowerop = (uplo == 'L') == (trans == 'N');
@@ -287,8 +290,31 @@ extern "C" int lnb_k_trsm_left_f64(char uplo, char trans, int64_t n, int64_t nrh
     int64_t grid = (int64_t)sms * 4;
     if (grid > items) grid = items;
     const int smem = 2 * TH * TLD * (int)sizeof(double);
-    cudaFuncSetAttribute(k_trsm_dag_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    k_trsm_dag_f64<<<(unsigned)grid, 128, smem, s>>>(a);
+    cudaFuncSetAttribute(k_trsm_dag<TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_trsm_dag<TT><<<(unsigned)grid, 128, smem, s>>>(a);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
+}
+
+extern "C" int lnb_k_trtri_blocks_f64(const double *T, int64_t ldt, int64_t n, int h, char uplo, int unit,
+                                      double *dinv, lnb_stream_t s)
+{
+    return trtri_blocks<double>(T, ldt, n, h, uplo, unit, dinv, s);
+}
+extern "C" int lnb_k_trtri_blocks_f32(const float *T, int64_t ldt, int64_t n, int h, char uplo, int unit,
+                                      double *dinv, lnb_stream_t s)
+{
+    return trtri_blocks<float>(T, ldt, n, h, uplo, unit, dinv, s);
+}
+extern "C" int lnb_k_trsm_left_f64(char uplo, char trans, int64_t n, int64_t nrhs, double alpha, const double *T,
+                                   int64_t ldt, const double *dinv, int h, double *B, int64_t ldb, int *sync,
+                                   lnb_status_t *st, long long wait_ns, int ticket0, lnb_stream_t s)
+{
+    return trsm_left<double>(uplo, trans, n, nrhs, alpha, T, ldt, dinv, h, B, ldb, sync, st, wait_ns, ticket0, s);
+}
+extern "C" int lnb_k_trsm_left_f32(char uplo, char trans, int64_t n, int64_t nrhs, double alpha, const float *T,
+                                   int64_t ldt, const double *dinv, int h, double *B, int64_t ldb, int *sync,
+                                   lnb_status_t *st, long long wait_ns, int ticket0, lnb_stream_t s)
+{
+    return trsm_left<float>(uplo, trans, n, nrhs, alpha, T, ldt, dinv, h, B, ldb, sync, st, wait_ns, ticket0, s);
 }

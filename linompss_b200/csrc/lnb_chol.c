@@ -44,6 +44,31 @@ static int upd(const double *P, int64_t ldp, double *C, int64_t ldc, int64_t nro
     return e;
 }
 
+/* Factor the bs x bs diagonal tile at Akk on stream s.  Tiles up to 128 are
+ * one leaf launch; larger tiles run a nested right-looking pass over 128-wide
+ * sub-tiles (leaf POTRF, panel TRSM, DMMA update), the structure of the
+ * reference's nested variant (chol_nrlmain.c).  Every leaf writes the
+ * inverses of its own 32x32 diagonal blocks into dinv at its offset, so on
+ * return dinv covers the whole tile. */
+int lnb_potrf_tile_f64(double *Akk, int64_t lda, int bs, int64_t row0, double *dinv,
+                          lnb_status_t *st, cudaStream_t s)
+{
+    const int LEAF_N = 128;
+    for (int j = 0; j < bs; j += LEAF_N) {
+        const int jb = bs - j < LEAF_N ? bs - j : LEAF_N;
+        double *Ajj = Akk + j + (int64_t)j * lda;
+        double *dj = dinv + (int64_t)(j / 32) * 1024;
+        CK(lnb_k_potrf_f64(Ajj, lda, jb, row0 + j, dj, st, s), "potrf leaf");
+        const int rem = bs - j - jb;
+        if (rem > 0) {
+            CK(lnb_k_trsm_rlt_f64(Ajj, lda, dj, Ajj + jb, lda, rem, jb, s), "potrf inner trsm");
+            CK(lnb_k_syrk_lower_f64(Ajj + jb, lda, Ajj + jb + (int64_t)jb * lda, lda, rem, 0, rem, jb, s),
+               "potrf inner update");
+        }
+    }
+    return 0;
+}
+
 size_t lnb_chol_f64_ws_bytes(int n, int b)
 {
     (void)n;
@@ -70,7 +95,7 @@ int lnb_chol_f64_run(lnb_ctx *c, int n, int b, double *dA, int64_t lda, lnb_aren
         const int64_t mrem = n - k0 - bs;      /* rows below the diagonal tile */
 
         /* panel factorization (crit) */
-        CK(lnb_k_potrf_f64(Akk, lda, bs, k0, dinv, c->st, crit), "potrf");
+        { int _e = lnb_potrf_tile_f64(Akk, lda, bs, k0, dinv, c->st, crit); if (_e) return _e; }
         if (mrem > 0) CK(lnb_k_trsm_rlt_f64(Akk, lda, dinv, Akk + bs, lda, mrem, bs, crit), "trsm");
         CK(cudaEventRecord(ev_trsm, crit), "event");
         if (copy_back) {

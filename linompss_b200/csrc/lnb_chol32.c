@@ -1,0 +1,249 @@
+/*
+ * lnb_chol32.c -- the FP32-storage tile Cholesky schedule (host C).
+ *
+ * Same right-looking schedule and depth-2 look-ahead as the FP64 one
+ * (lnb_chol.c, after chol_rlmain.c:22-53), used for the FP32 twins
+ * (ompss_schol_rl: schol_rl) and for the low-precision factor of the
+ * mixed-precision solver.  The trailing update runs in one of three modes:
+ *   LNB_FACTOR_FP32   SIMT FP32 (the plain single-precision tile tasks)
+ *   LNB_FACTOR_TF32X3 tcgen05 kind::tf32, 3 products on the hi/lo split
+ *   LNB_FACTOR_BF16   tcgen05 kind::f16, BF16 operands with per-block scales
+ * For the tensor-core modes each solved panel is first rewritten as K-major
+ * operand copies (k_prep_*), double-buffered across k-steps: the copy of
+ * step k stays alive while the bulk update of step k runs, and step k+2's
+ * copy only starts after that update (the crit stream waits on it).
+ */
+#include <stdlib.h>
+#include <string.h>
+
+#include "lnb_host.h"
+
+#define CK(call, where)                                            \
+    do {                                                           \
+        int _e = (int)(call);                                      \
+        if (_e != 0) return lnb_cuda_error(_e, where);             \
+    } while (0)
+
+static int g_schol_mode = LNB_FACTOR_TF32X3;
+
+void lnb_set_factor_mode(int mode)
+{
+    if (mode == LNB_FACTOR_FP32 || mode == LNB_FACTOR_TF32X3 || mode == LNB_FACTOR_BF16 ||
+        mode == LNB_FACTOR_TF32)
+        g_schol_mode = mode;
+}
+int lnb_get_factor_mode(void) { return g_schol_mode; }
+
+static inline int64_t kpad_of(int b) { return ((int64_t)b + 63) & ~(int64_t)63; }
+
+size_t lnb_chol_f32_ws_bytes(int n, int b, int mode)
+{
+    size_t bytes = lnb_align256((size_t)((b + 31) / 32) * 1024 * sizeof(float)) + 256;
+    const int64_t kp = kpad_of(b);
+    if (mode == LNB_FACTOR_TF32X3) bytes += 4 * lnb_align256((size_t)n * kp * 4);
+    else if (mode == LNB_FACTOR_TF32) bytes += 2 * lnb_align256((size_t)n * kp * 4);
+    else if (mode == LNB_FACTOR_BF16)
+        bytes += 2 * lnb_align256((size_t)n * kp * 2) + 2 * lnb_align256((size_t)(n / 128 + 2) * 4);
+    return bytes + 4096;
+}
+
+/* one diagonal tile: leaf (<= 128) or a nested 128-wide pass with SIMT
+ * inner updates; dinv receives the tile's 32x32 block inverses */
+int lnb_potrf_tile_f32(float *Akk, int64_t lda, int bs, int64_t row0, float *dinv, lnb_status_t *st,
+                       cudaStream_t s)
+{
+    const int LEAF_N = 128;
+    for (int j = 0; j < bs; j += LEAF_N) {
+        const int jb = bs - j < LEAF_N ? bs - j : LEAF_N;
+        float *Ajj = Akk + j + (int64_t)j * lda;
+        float *dj = dinv + (int64_t)(j / 32) * 1024;
+        CK(lnb_k_potrf_f32(Ajj, lda, jb, row0 + j, dj, st, s), "potrf leaf f32");
+        const int rem = bs - j - jb;
+        if (rem > 0) {
+            CK(lnb_k_trsm_rlt_f32(Ajj, lda, dj, Ajj + jb, lda, rem, jb, s), "inner trsm f32");
+            CK(lnb_k_syrk_lower_f32_simt(Ajj + jb, lda, Ajj + jb + (int64_t)jb * lda, lda, rem, 0, rem, jb, s),
+               "inner update f32");
+        }
+    }
+    return 0;
+}
+
+typedef struct {
+    int mode;
+    int64_t kpad;
+    void *hi[2], *lo[2];
+    float *scale[2];
+} panelbuf;
+
+static int upd32(const panelbuf *pb, int slot, const float *P, int64_t ldp, float *C, int64_t ldc,
+                 int64_t nrows, int64_t c0, int64_t c1, int k, lnb_status_t *st, cudaStream_t s)
+{
+    const double w = (double)(c1 - c0);
+    const double pairs = w * (double)nrows - (double)(c0 + c1 - 1) * w / 2.0;
+    const int prof = lnb_prof_begin(s);
+    int e;
+    if (pb->mode == LNB_FACTOR_FP32) {
+        e = lnb_k_syrk_lower_f32_simt(P, ldp, C, ldc, nrows, c0, c1, k, s);
+    } else {
+        const int m = pb->mode == LNB_FACTOR_TF32X3 ? 0 : pb->mode == LNB_FACTOR_TF32 ? 1 : 2;
+        e = lnb_k_tc_syrk_lower(m, pb->hi[slot], pb->lo[slot], (int)pb->kpad, nrows, C, ldc, nrows, c0, c1, k,
+                                pb->scale[slot], st, lnb_wait_ns(), s);
+    }
+    const double opb = pb->mode == LNB_FACTOR_BF16 ? 2.0 : pb->mode == LNB_FACTOR_TF32X3 ? 8.0 : 4.0;
+    lnb_prof_end(prof, s, 2.0 * k * pairs, opb * (double)pb->kpad * ((double)(nrows - c0) + w) + 8.0 * pairs);
+    return e;
+}
+
+int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_arena *ar, cudaStream_t s)
+{
+    float *dinv = (float *)lnb_arena_take(ar, (size_t)((b + 31) / 32) * 1024 * sizeof(float));
+    if (!dinv) return lnb_set_error(LNB_ENOMEM, "chol32 workspace");
+    panelbuf pb;
+    memset(&pb, 0, sizeof pb);
+    pb.mode = mode;
+    pb.kpad = kpad_of(b);
+    for (int i = 0; i < 2; ++i) {
+        if (mode == LNB_FACTOR_TF32X3 || mode == LNB_FACTOR_TF32) {
+            pb.hi[i] = lnb_arena_take(ar, (size_t)n * pb.kpad * 4);
+            if (mode == LNB_FACTOR_TF32X3) pb.lo[i] = lnb_arena_take(ar, (size_t)n * pb.kpad * 4);
+            if (!pb.hi[i] || (mode == LNB_FACTOR_TF32X3 && !pb.lo[i]))
+                return lnb_set_error(LNB_ENOMEM, "panel copies");
+        } else if (mode == LNB_FACTOR_BF16) {
+            pb.hi[i] = lnb_arena_take(ar, (size_t)n * pb.kpad * 2);
+            pb.scale[i] = (float *)lnb_arena_take(ar, (size_t)(n / 128 + 2) * 4);
+            if (!pb.hi[i] || !pb.scale[i]) return lnb_set_error(LNB_ENOMEM, "panel copies");
+        }
+    }
+    cudaStream_t crit = c->crit;
+    cudaEvent_t ev_start = c->ev[0], ev_trsm = c->ev[1], ev_next = c->ev[2], ev_done = c->ev[3];
+    CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
+    CK(cudaEventRecord(ev_start, s), "event");
+    CK(cudaStreamWaitEvent(crit, ev_start, 0), "event wait");
+
+    const int mt = (n + b - 1) / b;
+    for (int k = 0; k < mt; ++k) {
+        const int64_t k0 = (int64_t)k * b;
+        const int bs = (int)(n - k0 < b ? n - k0 : b);
+        float *Akk = dA + k0 + k0 * lda;
+        const int64_t mrem = n - k0 - bs;
+        const int slot = k & 1;
+        { int _e = lnb_potrf_tile_f32(Akk, lda, bs, k0, dinv, c->st, crit); if (_e) return _e; }
+        if (mrem > 0) {
+            CK(lnb_k_trsm_rlt_f32(Akk, lda, dinv, Akk + bs, lda, mrem, bs, crit), "trsm f32");
+            if (mode == LNB_FACTOR_TF32X3 || mode == LNB_FACTOR_TF32)
+                CK(lnb_k_prep_tf32(Akk + bs, lda, mrem, bs, (int)pb.kpad, (float *)pb.hi[slot],
+                                   mode == LNB_FACTOR_TF32X3 ? (float *)pb.lo[slot] : NULL, crit), "prep tf32");
+            else if (mode == LNB_FACTOR_BF16)
+                CK(lnb_k_prep_bf16(Akk + bs, lda, mrem, bs, (int)pb.kpad, pb.scale[slot], pb.hi[slot], crit),
+                   "prep bf16");
+        }
+        CK(cudaEventRecord(ev_trsm, crit), "event");
+        if (mrem <= 0) break;
+        const float *P = Akk + bs;
+        float *Ct = Akk + bs + (int64_t)bs * lda;
+        const int64_t nb1 = b < mrem ? b : mrem;
+        const int64_t nb2 = (2 * (int64_t)b) < mrem ? 2 * (int64_t)b : mrem;
+        CK(upd32(&pb, slot, P, lda, Ct, lda, mrem, 0, nb1, bs, c->st, crit), "update next panel");
+        CK(cudaStreamWaitEvent(s, ev_trsm, 0), "event wait");
+        if (nb2 > nb1) CK(upd32(&pb, slot, P, lda, Ct, lda, mrem, nb1, nb2, bs, c->st, s), "update panel k+2");
+        CK(cudaEventRecord(ev_next, s), "event");
+        if (mrem > nb2) CK(upd32(&pb, slot, P, lda, Ct, lda, mrem, nb2, mrem, bs, c->st, s), "update rest");
+        CK(cudaStreamWaitEvent(crit, ev_next, 0), "event wait");
+    }
+    CK(cudaEventRecord(ev_done, crit), "event");
+    CK(cudaStreamWaitEvent(s, ev_done, 0), "event wait");
+    return 0;
+}
+
+/* ---- entry points ---------------------------------------------------------- */
+static int check_args(int n, int b, const void *A, int lda)
+{
+    if (n < 0) return lnb_set_error(LNB_EINVAL, "n = %d < 0", n);
+    if (b <= 0 || b > 1024) return lnb_set_error(LNB_EINVAL, "tile size b = %d outside 1..1024", b);
+    if (lda < (n > 1 ? n : 1)) return lnb_set_error(LNB_EINVAL, "lda = %d < n = %d", lda, n);
+    if (n > 0 && !A) return lnb_set_error(LNB_EINVAL, "A is NULL");
+    return 0;
+}
+
+int lnb_schol_dev(int n, int b, float *dA, int lda, int *info_dev, void *stream)
+{
+    int e = check_args(n, b, dA, lda);
+    if (e) return e;
+    if (n == 0) return 0;
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    void *ws = lnb_ws(c, lnb_chol_f32_ws_bytes(n, b, g_schol_mode));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    cudaStream_t s = (cudaStream_t)stream;
+    if ((e = lnb_chol_f32_run(c, n, b, dA, lda, g_schol_mode, &ar, s))) return e;
+    if (info_dev) CK(cudaMemcpyAsync(info_dev, &c->st->info, sizeof(int), cudaMemcpyDeviceToDevice, s), "info");
+    return 0;
+}
+
+static int schol_host(int n, int b, float *A, int lda)
+{
+    int e = check_args(n, b, A, lda);
+    if (e) return e;
+    if (n == 0) return 0;
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const int64_t ldd = ((int64_t)n + 31) & ~(int64_t)31;
+    const size_t abytes = (size_t)ldd * n * sizeof(float);
+    void *ws = lnb_ws(c, lnb_align256(abytes) + lnb_chol_f32_ws_bytes(n, b, g_schol_mode));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    float *dA = (float *)lnb_arena_take(&ar, abytes);
+    cudaStream_t s = c->main;
+    for (int64_t c0 = 0; c0 < n; c0 += b) {
+        const int64_t w = n - c0 < b ? n - c0 : b;
+        CK(cudaMemcpy2DAsync(dA + c0 + c0 * ldd, ldd * sizeof(float), A + c0 + c0 * (int64_t)lda,
+                             (size_t)lda * sizeof(float), (size_t)(n - c0) * sizeof(float), w,
+                             cudaMemcpyHostToDevice, s), "A in");
+    }
+    if ((e = lnb_chol_f32_run(c, n, b, dA, ldd, g_schol_mode, &ar, s))) return e;
+    for (int64_t c0 = 0; c0 < n; c0 += b) {
+        const int64_t w = n - c0 < b ? n - c0 : b;
+        CK(cudaMemcpy2DAsync(A + c0 + c0 * (int64_t)lda, (size_t)lda * sizeof(float), dA + c0 + c0 * ldd,
+                             ldd * sizeof(float), (size_t)(n - c0) * sizeof(float), w, cudaMemcpyDeviceToHost, s),
+           "L out");
+    }
+    return lnb_status_read(c, s);
+}
+
+int ompss_schol_rl(int n, int b, int t, float *A, int lda) { (void)t; return schol_host(n, b, A, lda); }
+int ompss_schol_ll(int n, int b, int t, float *A, int lda) { (void)t; return schol_host(n, b, A, lda); }
+
+static int schol_hyper(int mt, int b, float **Ah)
+{
+    if (mt < 0 || b <= 0 || b > 1024) return lnb_set_error(LNB_EINVAL, "mt = %d, b = %d", mt, b);
+    if (mt == 0) return 0;
+    if (!Ah) return lnb_set_error(LNB_EINVAL, "Ah is NULL");
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const int64_t n = (int64_t)mt * b, ldd = (n + 31) & ~(int64_t)31;
+    const size_t abytes = (size_t)ldd * n * sizeof(float);
+    void *ws = lnb_ws(c, lnb_align256(abytes) + lnb_chol_f32_ws_bytes((int)n, b, g_schol_mode));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    float *dA = (float *)lnb_arena_take(&ar, abytes);
+    cudaStream_t s = c->main;
+    for (int j = 0; j < mt; ++j)
+        for (int i = j; i < mt; ++i) {
+            if (!Ah[(int64_t)j * mt + i]) return lnb_set_error(LNB_EINVAL, "tile (%d,%d) is NULL", i, j);
+            CK(cudaMemcpy2DAsync(dA + (int64_t)i * b + (int64_t)j * b * ldd, ldd * sizeof(float),
+                                 Ah[(int64_t)j * mt + i], (size_t)b * sizeof(float), (size_t)b * sizeof(float),
+                                 (size_t)b, cudaMemcpyHostToDevice, s), "tile in");
+        }
+    int e = lnb_chol_f32_run(c, (int)n, b, dA, ldd, g_schol_mode, &ar, s);
+    if (e) return e;
+    for (int j = 0; j < mt; ++j)
+        for (int i = j; i < mt; ++i)
+            CK(cudaMemcpy2DAsync(Ah[(int64_t)j * mt + i], (size_t)b * sizeof(float),
+                                 dA + (int64_t)i * b + (int64_t)j * b * ldd, ldd * sizeof(float),
+                                 (size_t)b * sizeof(float), (size_t)b, cudaMemcpyDeviceToHost, s), "tile out");
+    return lnb_status_read(c, s);
+}
+
+int ompss_schol_hrl(int mt, int b, int t, float **Ah) { (void)t; return schol_hyper(mt, b, Ah); }
+int ompss_schol_hll(int mt, int b, int t, float **Ah) { (void)t; return schol_hyper(mt, b, Ah); }

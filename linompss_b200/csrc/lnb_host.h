@@ -57,11 +57,23 @@ long long lnb_wait_ns(void);
 int lnb_status_read(lnb_ctx *c, cudaStream_t s);
 
 /* ---- FP64 factorization schedule on device memory (lnb_chol.c) ---------- */
+/* one diagonal tile (bs <= 1024): leaf kernel or nested 128-wide pass; fills
+ * dinv with the inverses of its 32x32 diagonal blocks */
+int lnb_potrf_tile_f64(double *Akk, int64_t lda, int bs, int64_t row0, double *dinv,
+                       lnb_status_t *st, cudaStream_t s);
 size_t lnb_chol_f64_ws_bytes(int n, int b);
 /* Factor dA in place on stream s.  `copy_back` (may be NULL): host matrix to
  * receive each finished panel as soon as it is final (lower part). */
 int lnb_chol_f64_run(lnb_ctx *c, int n, int b, double *dA, int64_t lda, lnb_arena *ar,
                      cudaStream_t s, double *copy_back, int64_t ldh);
+
+/* ---- FP32-storage factorization (lnb_chol32.c) ---------------------------- */
+int lnb_potrf_tile_f32(float *Akk, int64_t lda, int bs, int64_t row0, float *dinv, lnb_status_t *st,
+                       cudaStream_t s);
+size_t lnb_chol_f32_ws_bytes(int n, int b, int mode);
+int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_arena *ar,
+                     cudaStream_t s);
+int lnb_get_factor_mode(void);
 
 /* ---- FP64 triangular solves on device memory (lnb_solve.c) --------------- */
 size_t lnb_trsm_f64_ws_bytes(int64_t n);

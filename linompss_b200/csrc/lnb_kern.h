@@ -69,6 +69,52 @@ int lnb_k_trsm_left_f64(char uplo, char trans, int64_t n, int64_t nrhs, double a
                         int64_t ldb, int *sync, lnb_status_t *st, long long wait_ns,
                         int ticket0, lnb_stream_t s);
 
+/* ---- FP32-storage factorization kernels (k_chol_f32.cu) ------------------ */
+int lnb_k_potrf_f32(float *A, int64_t lda, int bs, int64_t row0, float *dinv, lnb_status_t *st,
+                    lnb_stream_t s);
+int lnb_k_trsm_rlt_f32(const float *L, int64_t lda, const float *dinv, float *B, int64_t ldb, int64_t m,
+                       int bs, lnb_stream_t s);
+int lnb_k_syrk_lower_f32_simt(const float *P, int64_t ldp, float *C, int64_t ldc, int64_t nrows,
+                              int64_t c0, int64_t c1, int kdim, lnb_stream_t s);
+/* K-major operand copies of a solved panel X (m x kb, ld ldx): TF32 hi (and
+ * lo = x - hi when lo != NULL), or BF16 with per-128-row power-of-two scales */
+int lnb_k_prep_tf32(const float *X, int64_t ldx, int64_t m, int kb, int kpad, float *hi, float *lo,
+                    lnb_stream_t s);
+int lnb_k_prep_bf16(const float *X, int64_t ldx, int64_t m, int kb, int kpad, float *scale, void *out,
+                    lnb_stream_t s);
+/* A32 = lower(S A S) in FP32 with S = diag(1/sqrt(a_ii)) (S = I if !equilibrate) */
+int lnb_k_lower_to_f32(const double *A, int64_t lda, int64_t n, int equilibrate, double *s_out,
+                       float *A32, int64_t ld32, lnb_stream_t s);
+/* tensor-core lower update (k_tc_update.cu); mode 0 TF32x3, 1 TF32, 2 BF16.
+ * hi/lo: K-major operand copies (prow rows x kpad); C FP32 column-major. */
+int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int kpad, int64_t prow, float *C,
+                        int64_t ldc, int64_t nrows, int64_t c0, int64_t c1, int kdim, const float *scale,
+                        lnb_status_t *st, long long wait_ns, lnb_stream_t s);
+
+/* FP32-stored triangular factor, FP64 right-hand sides and arithmetic */
+int lnb_k_trtri_blocks_f32(const float *T, int64_t ldt, int64_t n, int h, char uplo, int unit, double *dinv,
+                           lnb_stream_t s);
+int lnb_k_trsm_left_f32(char uplo, char trans, int64_t n, int64_t nrhs, double alpha, const float *T,
+                        int64_t ldt, const double *dinv, int h, double *B, int64_t ldb, int *sync,
+                        lnb_status_t *st, long long wait_ns, int ticket0, lnb_stream_t s);
+
+/* ---- symmetric products and refinement vectors (k_symv.cu) --------------- */
+/* Y = A X for symmetric A given by its lower triangle (FP64, column-major),
+ * X, Y n x nrhs (ld n); Y is overwritten.  absval != 0 uses |A| (row sums of
+ * |A| with X = ones give ||A||_inf). */
+int lnb_k_symv_lower_f64(int64_t n, int64_t nrhs, const double *A, int64_t lda, const double *X, double *Y,
+                         int absval, lnb_stream_t s);
+/* R = B - Y  and per-column max |R| into rmax[nrhs] (R may alias Y) */
+int lnb_k_resid_f64(int64_t n, int64_t nrhs, const double *B, int64_t ldb, const double *Y, double *R,
+                    double *rmax, lnb_stream_t s);
+/* per-column max |X| into out[nrhs] */
+int lnb_k_colmax_f64(int64_t n, int64_t nrhs, const double *X, int64_t ldx, double *out, lnb_stream_t s);
+/* Z = diag(sc) R   (sc may be NULL: copy) */
+int lnb_k_scale_rows_f64(int64_t n, int64_t nrhs, const double *sc, const double *R, double *Z, lnb_stream_t s);
+/* X += diag(sc) Z */
+int lnb_k_axpy_scaled_f64(int64_t n, int64_t nrhs, const double *sc, const double *Z, double *X, int64_t ldx,
+                          lnb_stream_t s);
+
 /* launch accounting (lnb_runtime.c), called by every launcher */
 void lnb_prof_count(int kernels);
 

@@ -1,0 +1,286 @@
+/*
+ * lnb_mixed.c -- low-precision factor + FP64 iterative refinement (host C).
+ *
+ * The reference's refinement loop (itref.c:999-1101) keeps the residual
+ * r = b - A x, the update x += s and the stopping test in FP64 and solves the
+ * correction equation A s = r with an inner solver; its mixed-precision hooks
+ * (bblas_d2s/s2d, itref.c:1009,1037) are commented out.  This driver makes
+ * the low-precision path real:
+ *
+ *   1. As = S A S in FP32 (S = diag(1/sqrt(a_ii)) equilibration, optional),
+ *      factored As = L L^T in FP32 storage with the trailing updates on the
+ *      tensor cores (TF32x3 or per-block-scaled BF16) or SIMT FP32;
+ *   2. refinement: z = S L^-T L^-1 S r (triangular solves read the FP32 factor
+ *      and compute in FP64), x += z, r = b - A x in FP64 from the lower
+ *      triangle of the untouched FP64 A, stop at the normwise backward error
+ *      ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol (default 10 n eps);
+ *   3. if refinement stalls (backward error not halving twice in a row, or
+ *      growing), switch to CG preconditioned by the same factor, M^-1 =
+ *      S L^-T L^-1 S, starting from the current x.
+ */
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "lnb_host.h"
+
+#define CK(call, where)                                            \
+    do {                                                           \
+        int _e = (int)(call);                                      \
+        if (_e != 0) return lnb_cuda_error(_e, where);             \
+    } while (0)
+
+#define TRSV_H 64
+#define LAPACK_EPS (DBL_EPSILON / 2.0)
+
+int lnb_k_coldot_f64(int64_t n, int64_t nrhs, const double *U, const double *V, double *out, lnb_stream_t s);
+int lnb_k_pcg_xr_f64(int64_t n, int64_t nrhs, const double *num, const double *den, const double *P,
+                     const double *Q, double *X, int64_t ldx, double *R, lnb_stream_t s);
+int lnb_k_pcg_p_f64(int64_t n, int64_t nrhs, const double *num, const double *den, const double *Z, double *P,
+                    lnb_stream_t s);
+
+void lnb_ir_default_opts(lnb_ir_opts *o)
+{
+    if (!o) return;
+    o->factor = LNB_FACTOR_TF32X3;
+    o->max_iter = 30;
+    o->tol = 0.0;
+    o->equilibrate = 1;
+    o->allow_pcg = 1;
+    o->pcg_max_iter = 200;
+}
+
+typedef struct {
+    int64_t n, nrhs, ld32;
+    float *A32;
+    double *S, *dinv, *R, *Z, *Y, *P, *Q, *ones, *scal; /* scal: 8 * nrhs scalars */
+    int *sync;
+} irws;
+
+static size_t ir_ws_bytes(int64_t n, int64_t nrhs, int b, int mode)
+{
+    const int64_t ld32 = (n + 31) & ~(int64_t)31;
+    const int64_t nb = (n + TRSV_H - 1) / TRSV_H;
+    size_t s = lnb_align256((size_t)ld32 * n * 4) + lnb_align256((size_t)n * 8) * 2 +
+               lnb_align256((size_t)nb * TRSV_H * TRSV_H * 8) + 5 * lnb_align256((size_t)n * nrhs * 8) +
+               lnb_align256((size_t)8 * (nrhs + 1) * 8) +
+               lnb_align256((size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4) + 4096;
+    return s + lnb_chol_f32_ws_bytes((int)n, b, mode);
+}
+
+/* z = M^-1 r = S L^-T L^-1 S r   (in place in Z, reading R) */
+static int precond(lnb_ctx *c, const irws *w, cudaStream_t s)
+{
+    CK(lnb_k_scale_rows_f64(w->n, w->nrhs, w->S, w->R, w->Z, s), "scale");
+    CK(lnb_k_trsm_left_f32('L', 'N', w->n, w->nrhs, 1.0, w->A32, w->ld32, w->dinv, TRSV_H, w->Z, w->n, w->sync,
+                           c->st, lnb_wait_ns(), 0, s), "forward solve");
+    CK(lnb_k_trsm_left_f32('L', 'T', w->n, w->nrhs, 1.0, w->A32, w->ld32, w->dinv, TRSV_H, w->Z, w->n, w->sync,
+                           c->st, lnb_wait_ns(), 0, s), "backward solve");
+    CK(lnb_k_scale_rows_f64(w->n, w->nrhs, w->S, w->Z, w->Z, s), "scale");
+    return 0;
+}
+
+/* R = B - A X; returns the max over columns of the normwise backward error */
+static int residual(lnb_ctx *c, const irws *w, const double *dA, int64_t lda, const double *dB, int64_t ldb,
+                    const double *dX, int64_t ldx, double anorm, const double *bmax, double *be, cudaStream_t s)
+{
+    (void)c;
+    const int64_t n = w->n, nrhs = w->nrhs;
+    /* Y = X packed with ld n, then Y = A Y */
+    CK(cudaMemcpy2DAsync(w->P, n * 8, dX, ldx * 8, n * 8, nrhs, cudaMemcpyDeviceToDevice, s), "pack x");
+    CK(lnb_k_symv_lower_f64(n, nrhs, dA, lda, w->P, w->Y, 0, s), "symv");
+    CK(lnb_k_resid_f64(n, nrhs, dB, ldb, w->Y, w->R, w->scal, s), "resid");
+    CK(lnb_k_colmax_f64(n, nrhs, dX, ldx, w->scal + nrhs, s), "xmax");
+    double h[2 * 64 + 2];
+    const int64_t q2 = nrhs > 64 ? 64 : nrhs;
+    CK(cudaMemcpyAsync(h, w->scal, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, s), "read");
+    CK(cudaMemcpyAsync(h + 64, w->scal + nrhs, sizeof(double) * q2, cudaMemcpyDeviceToHost, s), "read");
+    CK(cudaStreamSynchronize(s), "sync");
+    double worst = 0.0;
+    for (int64_t q = 0; q < q2; ++q) {
+        const double den = anorm * h[64 + q] + bmax[q];
+        const double e = den > 0 ? h[q] / den : 0.0;
+        if (e > worst || e != e) worst = e;
+    }
+    *be = worst;
+    return 0;
+}
+
+int lnb_dsposv_ir_dev(int n, int nrhs, int b, const double *dA, int lda, const double *dB, int ldb, double *dX,
+                      int ldx, const lnb_ir_opts *opts_in, lnb_ir_result *res, void *stream)
+{
+    lnb_ir_opts opts;
+    if (opts_in) opts = *opts_in;
+    else lnb_ir_default_opts(&opts);
+    if (n < 0 || nrhs < 0 || b <= 0 || b > 1024 || lda < (n > 1 ? n : 1) || ldb < (n > 1 ? n : 1) ||
+        ldx < (n > 1 ? n : 1))
+        return lnb_set_error(LNB_EINVAL, "dsposv_ir arguments");
+    if (nrhs > 64) return lnb_set_error(LNB_EINVAL, "dsposv_ir: nrhs = %d > 64", nrhs);
+    int mode = opts.factor;
+    if (mode != LNB_FACTOR_FP32 && mode != LNB_FACTOR_TF32X3 && mode != LNB_FACTOR_BF16 && mode != LNB_FACTOR_TF32)
+        return lnb_set_error(LNB_EINVAL, "dsposv_ir: factor mode %d is not a low-precision mode", mode);
+    lnb_ir_result rr;
+    memset(&rr, 0, sizeof rr);
+    if (n == 0 || nrhs == 0) { if (res) *res = rr; return 0; }
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    void *ws = lnb_ws(c, ir_ws_bytes(n, nrhs, b, mode));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    irws w;
+    w.n = n; w.nrhs = nrhs; w.ld32 = ((int64_t)n + 31) & ~(int64_t)31;
+    const int64_t nb = ((int64_t)n + TRSV_H - 1) / TRSV_H;
+    w.A32 = lnb_arena_take(&ar, (size_t)w.ld32 * n * 4);
+    w.S = lnb_arena_take(&ar, (size_t)n * 8);
+    w.ones = lnb_arena_take(&ar, (size_t)n * 8);
+    w.dinv = lnb_arena_take(&ar, (size_t)nb * TRSV_H * TRSV_H * 8);
+    w.R = lnb_arena_take(&ar, (size_t)n * nrhs * 8);
+    w.Z = lnb_arena_take(&ar, (size_t)n * nrhs * 8);
+    w.Y = lnb_arena_take(&ar, (size_t)n * nrhs * 8);
+    w.P = lnb_arena_take(&ar, (size_t)n * nrhs * 8);
+    w.Q = lnb_arena_take(&ar, (size_t)n * nrhs * 8);
+    w.scal = lnb_arena_take(&ar, (size_t)8 * (nrhs + 1) * 8);
+    w.sync = lnb_arena_take(&ar, (size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4);
+    if (!w.sync) return lnb_set_error(LNB_ENOMEM, "dsposv_ir workspace");
+    cudaStream_t s = (cudaStream_t)stream;
+    const double tol = opts.tol > 0 ? opts.tol : 10.0 * n * LAPACK_EPS;
+
+    /* ---- factor ---- */
+    CK(cudaEventRecord(c->t0, s), "event");
+    CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, s), "convert");
+    int e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &ar, s);
+    if (e) return e;
+    CK(lnb_k_trtri_blocks_f32(w.A32, w.ld32, n, TRSV_H, 'L', 0, w.dinv, s), "trtri");
+    CK(cudaEventRecord(c->t1, s), "event");
+    int info = lnb_status_read(c, s);
+    if (info < 0) return info;
+    rr.info = info;
+    {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->t0, c->t1);
+        rr.factor_ms = ms;
+    }
+    if (info > 0) {
+        if (res) *res = rr;
+        return lnb_set_error(info, "low-precision factor: leading minor %d not positive", info);
+    }
+
+    /* ---- norms ---- */
+    CK(cudaEventRecord(c->t0, s), "event");
+    double anorm, bmax[64];
+    {
+        /* ||A||_inf = max row sum of |A|, from the lower triangle (symv of |A| with ones) */
+        double h = 0.0;
+        double *hones = (double *)malloc((size_t)n * 8);
+        if (!hones) return lnb_set_error(LNB_ENOMEM, "host ones");
+        for (int64_t i = 0; i < n; ++i) hones[i] = 1.0;
+        CK(cudaMemcpyAsync(w.ones, hones, (size_t)n * 8, cudaMemcpyHostToDevice, s), "ones");
+        CK(lnb_k_symv_lower_f64(n, 1, dA, lda, w.ones, w.Y, 1, s), "row sums");
+        CK(lnb_k_colmax_f64(n, 1, w.Y, n, w.scal, s), "max");
+        CK(lnb_k_colmax_f64(n, nrhs, dB, ldb, w.scal + 1, s), "bmax");
+        CK(cudaMemcpyAsync(&h, w.scal, 8, cudaMemcpyDeviceToHost, s), "read");
+        CK(cudaMemcpyAsync(bmax, w.scal + 1, (size_t)nrhs * 8, cudaMemcpyDeviceToHost, s), "read");
+        CK(cudaStreamSynchronize(s), "sync");
+        free(hones);
+        anorm = h;
+    }
+
+    /* ---- refinement ---- */
+    CK(cudaMemset2DAsync(dX, (size_t)ldx * 8, 0, (size_t)n * 8, nrhs, s), "x = 0");
+    CK(cudaMemcpy2DAsync(w.R, (size_t)n * 8, dB, (size_t)ldb * 8, (size_t)n * 8, nrhs, cudaMemcpyDeviceToDevice, s),
+       "r = b");
+    double be = INFINITY, be_prev = INFINITY;
+    int slow = 0, it;
+    for (it = 0; it < opts.max_iter; ++it) {
+        if ((e = precond(c, &w, s))) return e;
+        CK(lnb_k_axpy_scaled_f64(n, nrhs, NULL, w.Z, dX, ldx, s), "x += z");
+        be_prev = be;
+        if ((e = residual(c, &w, dA, lda, dB, ldb, dX, ldx, anorm, bmax, &be, s))) return e;
+        if (be <= tol) { ++it; break; }
+        if (!(be <= 0.5 * be_prev)) ++slow; else slow = 0;
+        if (opts.allow_pcg && (slow >= 2 || be > be_prev)) { ++it; rr.used_pcg = 1; break; }
+    }
+    rr.iterations = it;
+
+    /* ---- preconditioned CG fallback ---- */
+    if (rr.used_pcg && be > tol) {
+        double *rz = w.scal + 2 * (nrhs + 1), *pq = rz + nrhs + 1, *rz2 = pq + nrhs + 1;
+        if ((e = precond(c, &w, s))) return e;                                 /* Z = M^-1 R */
+        CK(cudaMemcpyAsync(w.P, w.Z, (size_t)n * nrhs * 8, cudaMemcpyDeviceToDevice, s), "p = z");
+        CK(lnb_k_coldot_f64(n, nrhs, w.R, w.Z, rz, s), "rz");
+        int k;
+        for (k = 0; k < opts.pcg_max_iter; ++k) {
+            CK(lnb_k_symv_lower_f64(n, nrhs, dA, lda, w.P, w.Q, 0, s), "Ap");
+            CK(lnb_k_coldot_f64(n, nrhs, w.P, w.Q, pq, s), "pq");
+            CK(lnb_k_pcg_xr_f64(n, nrhs, rz, pq, w.P, w.Q, dX, ldx, w.R, s), "x, r");
+            if ((k & 3) == 3 || k + 1 == opts.pcg_max_iter) {
+                /* true residual every 4 steps for the stopping test */
+                if ((e = residual(c, &w, dA, lda, dB, ldb, dX, ldx, anorm, bmax, &be, s))) return e;
+                if (be <= tol) { ++k; break; }
+            }
+            if ((e = precond(c, &w, s))) return e;
+            CK(lnb_k_coldot_f64(n, nrhs, w.R, w.Z, rz2, s), "rz");
+            CK(lnb_k_pcg_p_f64(n, nrhs, rz2, rz, w.Z, w.P, s), "p");
+            CK(cudaMemcpyAsync(rz, rz2, (size_t)nrhs * 8, cudaMemcpyDeviceToDevice, s), "rz");
+        }
+        rr.pcg_iterations = k;
+    }
+    CK(cudaEventRecord(c->t1, s), "event");
+    CK(cudaStreamSynchronize(s), "sync");
+    {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->t0, c->t1);
+        rr.solve_ms = ms;
+    }
+    {
+        int st = lnb_status_read(c, s);
+        if (st < 0) return st;
+    }
+    rr.backward_error = be;
+    if (res) *res = rr;
+    if (!(be <= tol))
+        return lnb_set_error(LNB_ENOCONV, "refinement stopped at backward error %.3e > tol %.3e", be, tol);
+    return 0;
+}
+
+int lnb_dsposv_ir(int n, int nrhs, int b, const double *A, int lda, const double *B, int ldb, double *X, int ldx,
+                  const lnb_ir_opts *opts, lnb_ir_result *res)
+{
+    if (n < 0 || nrhs < 0 || lda < (n > 1 ? n : 1) || ldb < (n > 1 ? n : 1) || ldx < (n > 1 ? n : 1))
+        return lnb_set_error(LNB_EINVAL, "dsposv_ir arguments");
+    if (n == 0 || nrhs == 0) return 0;
+    if (!A || !B || !X) return lnb_set_error(LNB_EINVAL, "NULL argument");
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const int64_t ldd = ((int64_t)n + 7) & ~(int64_t)7;
+    double *dA = NULL, *dB = NULL, *dX = NULL;
+    if (cudaMalloc((void **)&dA, (size_t)ldd * n * 8) != cudaSuccess ||
+        cudaMalloc((void **)&dB, (size_t)ldd * nrhs * 8) != cudaSuccess ||
+        cudaMalloc((void **)&dX, (size_t)ldd * nrhs * 8) != cudaSuccess) {
+        cudaFree(dA); cudaFree(dB); cudaFree(dX);
+        cudaGetLastError();
+        return lnb_set_error(LNB_ENOMEM, "dsposv_ir: device buffers");
+    }
+    cudaStream_t s = c->main;
+    int e = 0;
+    /* lower block-columns of A only: the solver never reads the upper triangle */
+    for (int64_t c0 = 0; c0 < n && !e; c0 += 512) {
+        const int64_t wd = n - c0 < 512 ? n - c0 : 512;
+        if (cudaMemcpy2DAsync(dA + c0 + c0 * ldd, ldd * 8, A + c0 + c0 * (int64_t)lda, (size_t)lda * 8,
+                              (size_t)(n - c0) * 8, wd, cudaMemcpyHostToDevice, s) != cudaSuccess)
+            e = lnb_cuda_error(cudaGetLastError(), "A in");
+    }
+    if (!e && cudaMemcpy2DAsync(dB, ldd * 8, B, (size_t)ldb * 8, (size_t)n * 8, nrhs, cudaMemcpyHostToDevice, s) !=
+                  cudaSuccess)
+        e = lnb_cuda_error(cudaGetLastError(), "B in");
+    if (!e) e = lnb_dsposv_ir_dev(n, nrhs, b, dA, (int)ldd, dB, (int)ldd, dX, (int)ldd, opts, res, s);
+    if (e >= 0 || e == LNB_ENOCONV) {
+        if (cudaMemcpy2DAsync(X, (size_t)ldx * 8, dX, ldd * 8, (size_t)n * 8, nrhs, cudaMemcpyDeviceToHost, s) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess)
+            e = lnb_cuda_error(cudaGetLastError(), "X out");
+    }
+    cudaFree(dA); cudaFree(dB); cudaFree(dX);
+    return e;
+}

@@ -71,7 +71,7 @@ int task_dpotrf(ompsslapack_t uplo, int n, double *A, int lda, int p)
         e = put(dA, ldd, A, lda, n, n, s);
     }
     if (!e) e = (int)cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s) ? LNB_ECUDA : 0;
-    if (!e) e = lnb_k_potrf_f64(dA, ldd, n, 0, dinv, c->st, s) ? lnb_cuda_error(LNB_ECUDA, "potrf") : 0;
+    if (!e) e = lnb_potrf_tile_f64(dA, ldd, n, 0, dinv, c->st, s);
     if (!e) e = get(u == 'U' ? tmp : A, u == 'U' ? n : lda, dA, ldd, n, n, s);
     int info = e ? e : lnb_status_read(c, s);
     if (u == 'U' && info >= 0) {

@@ -1,0 +1,111 @@
+"""GPU parity of the FP32 tile Cholesky (ompss_schol_rl, the reference's
+schol_rl) in each update mode, through the C ABI.
+
+Tolerances are per mode, stated against the FP32 unit roundoff u32:
+  FP32 (SIMT) and TF32x3 (tcgen05, hi/lo split): FP32-level factor,
+      ||A - L L^T|| / (n u32 ||A||) <= 10 and entrywise close to the
+      reference's own FP32 output (golden) / the FP64 factor
+  TF32 (one product, 10-bit mantissa operands) and BF16 (8-bit):
+      the factor is a preconditioner-grade approximation; bounds scale with
+      the operand precision (2^-11, 2^-8).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+U32 = np.finfo(np.float32).eps / 2
+
+MODES = {"fp32": 1, "tf32x3": 2, "bf16": 3, "tf32": 4}
+# bound on ||A - L L^T||_inf / (||A||_inf n) per mode
+RESID = {"fp32": 10 * U32, "tf32x3": 10 * U32, "tf32": 2.0 ** -11, "bf16": 2.0 ** -8}
+
+
+@pytest.fixture(scope="module")
+def lnb(cuda):
+    import linompss_b200
+    yield linompss_b200
+    linompss_b200.set_factor_mode(linompss_b200.FACTOR_TF32X3)
+
+
+def resid32(A0, L):
+    n = A0.shape[0]
+    Lt = np.tril(L.astype(np.float64))
+    R = Lt @ Lt.T - A0.astype(np.float64)
+    return np.abs(R).sum(axis=1).max() / (np.abs(A0).sum(axis=1).max() * n)
+
+
+@pytest.mark.parametrize("mode", ["fp32", "tf32x3", "tf32", "bf16"])
+def test_schol_golden(lnb, golden_dir, mode):
+    d = np.load(os.path.join(golden_dir, "schol_rl_n96_b32.npz"))
+    lnb.set_factor_mode(MODES[mode])
+    A = np.asfortranarray(d["A"].copy())
+    assert lnb.ompss_schol_rl(96, 32, 32, A, 96) == 0
+    assert resid32(d["A"], A) <= RESID[mode]
+    if mode in ("fp32", "tf32x3"):
+        np.testing.assert_allclose(np.tril(A), np.tril(d["out"]), rtol=0,
+                                   atol=64 * U32 * np.abs(d["out"]).max())
+    np.testing.assert_array_equal(np.triu(A, 1), np.triu(d["A"], 1))
+
+
+@pytest.mark.parametrize("mode", ["fp32", "tf32x3", "tf32", "bf16"])
+@pytest.mark.parametrize("n,b", [(130, 64), (300, 128), (1000, 256), (1024, 512), (2048, 256), (777, 200)])
+def test_schol_modes_sizes(lnb, mode, n, b):
+    lnb.set_factor_mode(MODES[mode])
+    A0 = O.spd_covariance(n, 1.0, seed=n + b)
+    A = np.asfortranarray(A0.astype(np.float32))
+    assert lnb.ompss_schol_rl(n, b, b, A, n) == 0
+    r = resid32(A0, A)
+    assert r <= RESID[mode], r
+    if mode in ("fp32", "tf32x3"):
+        L = np.linalg.cholesky(A0)
+        np.testing.assert_allclose(np.tril(A), L, rtol=0, atol=2e-5 * np.abs(L).max())
+
+
+def test_tf32x3_matches_fp32_simt(lnb):
+    """The split product recovers FP32-level accuracy: TF32x3 and the SIMT
+    FP32 update agree to FP32 rounding, far closer than a single TF32 product."""
+    n, b = 1536, 256
+    A0 = O.spd_covariance(n, 0.1, seed=7).astype(np.float32)
+    out = {}
+    for mode in ("fp32", "tf32x3", "tf32"):
+        lnb.set_factor_mode(MODES[mode])
+        A = np.asfortranarray(A0.copy())
+        assert lnb.ompss_schol_rl(n, b, b, A, n) == 0
+        out[mode] = np.tril(A).astype(np.float64)
+    d3 = np.abs(out["tf32x3"] - out["fp32"]).max()
+    d1 = np.abs(out["tf32"] - out["fp32"]).max()
+    assert d3 < 1e-4 and d3 * 20 < d1, (d3, d1)
+
+
+def test_schol_hypermatrix(lnb):
+    lnb.set_factor_mode(MODES["tf32x3"])
+    mt, b = 4, 64
+    n = mt * b
+    A0 = O.spd_covariance(n, 1.0, seed=3).astype(np.float32)
+    tiles = np.zeros((mt, mt, b, b), dtype=np.float32)
+    for j in range(mt):
+        for i in range(mt):
+            tiles[j, i] = A0[i * b:(i + 1) * b, j * b:(j + 1) * b].T
+    assert lnb.ompss_schol_hrl(mt, b, b, tiles) == 0
+    L = np.linalg.cholesky(A0.astype(np.float64))
+    for j in range(mt):
+        for i in range(j, mt):
+            got = tiles[j, i].T.astype(np.float64)
+            ref = L[i * b:(i + 1) * b, j * b:(j + 1) * b]
+            if i == j:
+                got, ref = np.tril(got), np.tril(ref)
+            np.testing.assert_allclose(got, ref, rtol=0, atol=2e-5 * np.abs(L).max())
+
+
+@pytest.mark.parametrize("mode", ["fp32", "tf32x3"])
+def test_schol_not_spd(lnb, mode):
+    lnb.set_factor_mode(MODES[mode])
+    n, b = 400, 128
+    A0 = O.spd_diag_dominant(n, seed=2).astype(np.float32)
+    A0[300, 300] = -5.0
+    A = np.asfortranarray(A0.copy())
+    assert lnb.ompss_schol_rl(n, b, b, A, n) == 301

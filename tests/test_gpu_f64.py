@@ -150,7 +150,8 @@ def test_dtrsm_golden(lnb, golden_dir, case):
 def test_dtrsm_vs_oracle_ragged(lnb, uplo, trans, diag):
     rng = np.random.default_rng(1)
     m, n = 203, 17
-    T = np.asfortranarray(rng.uniform(-1, 1, (m, m)) + 4 * m * np.eye(m))
+    # well conditioned for both diagonal kinds: small off-diagonal entries
+    T = np.asfortranarray(rng.uniform(-1, 1, (m, m)) / m + (1.0 if diag == "U" else 2.0) * np.eye(m))
     B0 = np.asfortranarray(rng.uniform(-1, 1, (m, n)))
     B1, B2 = B0.copy(order="F"), B0.copy(order="F")
     lnb.ompss_dtrsm("L", uplo, trans, diag, m, n, 64, 0.5, T, m, B1, m)
