@@ -1,25 +1,31 @@
 #!/usr/bin/env python3
-"""Benchmark: FP64-accurate SPD solve (tile Cholesky + forward/backward solves).
+"""Benchmark: FP64-accurate SPD solve, mixed-precision refinement vs plain FP64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload fp64|mixed]
+                    [--workload mixed|fp64|bf16]
 
-One step = one SPD solve A x = b of the workload (factor + both triangular
-solves, plus refinement for the mixed workload) on one batch of synthetic
-input already resident in HBM.  The metric is TFLOP/s with the FP64-equivalent
-flop count n^3/3 + 2 n^2 nrhs (the same count for plain and mixed solves).
+One step = one solve A X = B to FP64 backward error (<= 10 n eps) on one batch
+of synthetic input already resident in HBM.  The metric is TFLOP/s with the
+FP64-equivalent flop count n^3/3 + 2 n^2 nrhs, the same count for plain and
+mixed solves, so the values compare time to solution directly.
 
-Workloads (synthetic, seeded, shapes and distributions of the reference
-configurations):
-  fp64  : n = 16384, tile b = 512, 1 rhs, A = G G^T / n + 1e-2 I, G ~ N(0,1)
-          (plain FP64 tile Cholesky with DMMA updates)
-Inputs are 2 GiB (> L2), and the factor runs in place, so A is restored from a
-pristine copy before every step, outside the timed events (which also flushes
-L2 between steps).
+Workloads (seeded synthetic inputs with the reference configurations' shapes
+and distributions):
+  mixed (default): n = 32768, b = 512, 1 rhs, A = G G^T/n + 1e-3 I, G ~ N(0,1):
+        TF32x3 tensor-core factor in FP32 storage + FP64 refinement.  The plain
+        FP64 tile Cholesky of the same matrix is timed in the same run
+        ("fp64_plain") so the line carries the mixed / plain speed-up.
+  fp64: n = 16384, b = 512, 1 rhs, A = G G^T/n + 1e-2 I: plain FP64 factor
+        (DMMA) + triangular solves.
+  bf16: n = 49152, b = 1024, 8 rhs, A = D (G G^T/n + 1e-2 I) D, D = diag(10^u),
+        u ~ U[-2,2]: per-block-scaled BF16 factor, equilibration, refinement
+        with PCG fallback.
+Inputs are larger than L2 (126 MB); the plain FP64 factor runs in place, so its
+A is restored from a pristine copy before every step outside the timed events.
 
-Multi-GPU: a single SPD system does not shard (the tile Cholesky exchanges a
-panel at every k-step), so N GPUs run N independent replicas, one rank per
-GPU, and value = N * flops / max-over-ranks time ("scaling": "weak").
+Multi-GPU: one SPD system does not shard (the tile Cholesky exchanges a panel
+at every k-step), so N GPUs run N independent replicas, one rank per GPU, and
+value = N * flops / max-over-ranks time ("scaling": "weak").
 """
 from __future__ import annotations
 
@@ -35,8 +41,14 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "FP64-accurate SPD solve TFLOP/s (FP64-equivalent n^3/3+2n^2*nrhs)"
+METRIC = "FP64-accurate SPD solve TFLOP/s (FP64-equivalent n^3/3+2n^2*nrhs): mixed-prec IR vs plain FP64"
 UNIT = "TFLOP/s"
+
+WORKLOADS = {
+    "mixed": dict(n=32768, b=512, nrhs=1, delta=1e-3, scaled=False, factor="TF32X3"),
+    "fp64": dict(n=16384, b=512, nrhs=1, delta=1e-2, scaled=False, factor="FP64"),
+    "bf16": dict(n=49152, b=1024, nrhs=8, delta=1e-2, scaled=True, factor="BF16"),
+}
 
 
 def parse():
@@ -45,13 +57,20 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="fp64", choices=["fp64"])
-    p.add_argument("--n", type=int, default=16384)
-    p.add_argument("--b", type=int, default=512)
-    p.add_argument("--nrhs", type=int, default=1)
+    p.add_argument("--workload", default="mixed", choices=sorted(WORKLOADS))
+    p.add_argument("--n", type=int, default=None)
+    p.add_argument("--b", type=int, default=None)
+    p.add_argument("--nrhs", type=int, default=None)
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    return p.parse_args()
+    p.add_argument("--no-plain", action="store_true", help="skip the plain-FP64 comparison (mixed/bf16)")
+    a = p.parse_args()
+    w = dict(WORKLOADS[a.workload])
+    for k in ("n", "b", "nrhs"):
+        if getattr(a, k) is not None:
+            w[k] = getattr(a, k)
+    a.w = w
+    return a
 
 
 def flops_of(n, nrhs):
@@ -68,9 +87,11 @@ def dist_init():
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
@@ -146,40 +167,61 @@ class Clocks:
 # ----------------------------------------------------------------------------
 # workload generation (device, seeded)
 # ----------------------------------------------------------------------------
-def make_spd(n, delta, seed, device):
+def make_spd(n, delta, seed, device, scaled=False):
+    """A = G G^T/n + delta I (symmetric, so row- and column-major agree);
+    scaled: A = D A D with D = diag(10^u), u ~ U[-2, 2]."""
     import torch
     g = torch.Generator(device=device)
     g.manual_seed(seed)
+    A = torch.empty(n, n, dtype=torch.float64, device=device)
+    chunk = 8192
     G = torch.randn(n, n, dtype=torch.float64, device=device, generator=g)
-    A = torch.mm(G, G.t()).div_(n)
+    for r0 in range(0, n, chunk):          # blockwise product keeps the peak memory at 2 n^2
+        A[r0:r0 + chunk] = G[r0:r0 + chunk] @ G.t()
     del G
+    A.div_(n)
     A.diagonal().add_(delta)
-    return A  # symmetric: row-major == column-major
-
-
-def measure_fp64_peak(device):
-    """cuBLAS dgemm throughput on this GPU (denominator of the DMMA roofline)."""
-    import torch
-    n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device=device)
-    b = torch.randn(n, n, dtype=torch.float64, device=device)
-    torch.mm(a, b)
-    torch.cuda.synchronize()
-    best = 0.0
-    for _ in range(3):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        torch.mm(a, b)
-        e1.record()
-        torch.cuda.synchronize()
-        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
-    del a, b
+    if scaled:
+        d = torch.pow(10.0, torch.rand(n, dtype=torch.float64, device=device, generator=g) * 4.0 - 2.0)
+        A.mul_(d[:, None]).mul_(d[None, :])
     torch.cuda.empty_cache()
-    return best
+    return A
+
+
+def measure_peaks(device):
+    """cuBLAS throughput on this GPU for the roofline denominators: FP64 dgemm
+    (the DMMA path has no entry in MEASURED_PEAKS.json) and TF32 sgemm."""
+    import torch
+    out = {}
+    n = 8192
+    for name, dt, tf32 in (("fp64", torch.float64, False), ("tf32", torch.float32, True)):
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        a = torch.randn(n, n, dtype=dt, device=device)
+        b = torch.randn(n, n, dtype=dt, device=device)
+        torch.mm(a, b)
+        torch.cuda.synchronize()
+        best = 0.0
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.mm(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+        out[name] = best
+        del a, b
+    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.cuda.empty_cache()
+    try:
+        out["bf16"] = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]
+        out["hbm_gbs"] = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]
+    except Exception:
+        out["bf16"], out["hbm_gbs"] = 1590.0, 6650.0
+    return out
 
 
 # ----------------------------------------------------------------------------
-# CPU: the reference (oracle/_ref) or the oracle port, bounded sample
+# CPU: the reference build (oracle/_ref) or the oracle port, bounded sample
 # ----------------------------------------------------------------------------
 def cpu_run(n, b, nrhs, steps, warmup, A_host=None):
     """Times dspdsolv_main of the reference build (OpenBLAS, all host threads)
@@ -214,26 +256,29 @@ def cpu_run(n, b, nrhs, steps, warmup, A_host=None):
 def reference_arm(args, world, rank):
     if rank != 0:
         return
-    # bounded sample of the workload: the same distribution at n = 8192
-    n = min(args.n, 8192)
+    w = args.w
+    # bounded sample of the workload: same distribution at n = 8192 (the reference
+    # has no mixed-precision path: its FP64-accurate solve is dspdsolv_main)
+    n = min(w["n"], 8192)
+    b = min(w["b"], 512)
+    A = None
     try:
         import torch
         if torch.cuda.is_available():
-            A = make_spd(n, 1e-2, 0, "cuda").cpu().numpy()
-        else:
-            A = None
+            A = make_spd(n, w["delta"], 0, "cuda", w["scaled"]).cpu().numpy()
     except Exception:
         A = None
-    v, kind, cores, sec = cpu_run(n, args.b, args.nrhs, args.steps, args.warmup, A)
+    v, kind, cores, sec = cpu_run(n, b, w["nrhs"], args.steps, args.warmup, A)
     line = {"metric": METRIC, "value": round(v, 6), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"spd_fp64_n{n}_b{args.b}_rhs{args.nrhs}", "n": n, "b": args.b,
-                       "nrhs": args.nrhs, "sample_of": f"n={args.n}"},
+            "config": {"workload": f"spd_{args.workload}_n{w['n']}_b{w['b']}_rhs{w['nrhs']}",
+                       "sample": f"n={n} b={b}", "n": n, "b": b, "nrhs": w["nrhs"]},
             "cpu_baseline": {"value": round(v, 6), "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": f"dspdsolv_main n={n} b={args.b} nrhs={args.nrhs}, "
-                                       f"OpenBLAS threads={cores}, median of {args.steps}"},
+                             "sample": f"dspdsolv_main n={n} b={b} nrhs={w['nrhs']} of the {args.workload} "
+                                       f"workload's distribution, OpenBLAS threads={cores}, median of "
+                                       f"{args.steps} after {args.warmup} warm-up"},
             "e2e": {"value": round(v, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -241,136 +286,15 @@ def reference_arm(args, world, rank):
 # ----------------------------------------------------------------------------
 # our arm
 # ----------------------------------------------------------------------------
-def ours_arm(args, world, rank, local):
-    import numpy as np
-    import torch
-
-    import linompss_b200 as lnb
-
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    L = lnb.lib()
-    n, b, nrhs = args.n, args.b, args.nrhs
-    fl = flops_of(n, nrhs)
-
-    peak_fp64 = measure_fp64_peak(dev)
-
-    A0 = make_spd(n, 1e-2, 1234 + rank, dev)
-    g = torch.Generator(device=dev)
-    g.manual_seed(99 + rank)
-    B0 = torch.randn(nrhs, n, dtype=torch.float64, device=dev, generator=g)  # column-major (nrhs, ld=n)
-    A = torch.empty_like(A0)
-    B = torch.empty_like(B0)
-    info = torch.zeros(1, dtype=torch.int32, device=dev)
-    s = torch.cuda.current_stream()
-
-    def one_step(timed):
-        A.copy_(A0)
-        B.copy_(B0)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(s)
-        lnb.dposv_dev(A, B, n, nrhs, b, info=info, stream=s)
-        e1.record(s)
-        return e0, e1
-
-    for _ in range(args.warmup):
-        one_step(False)
-    torch.cuda.synchronize()
-    assert int(info.item()) == 0, "warm-up factorization failed"
-
-    barrier(world)
-    torch.cuda.synchronize()
-    L.lnb_prof_reset()
-    L.lnb_prof_enable(1)
-    evs = []
-    with Clocks(local) as clk:
-        for _ in range(args.steps):
-            evs.append(one_step(True))
-        torch.cuda.synchronize()
-    barrier(world)
-    L.lnb_prof_enable(0)
-    prof = lnb_prof(L)
-    total_ms = sum(e0.elapsed_time(e1) for e0, e1 in evs)
-    ms_step = allmax(world, total_ms / args.steps)
-    value = world * fl / (ms_step * 1e-3) / 1e12
-
-    # correctness of the timed result (last step)
-    X = B.double()
-    bw = backward_error_dev(A0, X, B0)
-    assert int(info.item()) == 0 and bw <= 10 * n * np.finfo(float).eps, f"backward error {bw}"
-
-    # e2e: the host entry point dspdsolv_main on pinned host buffers
-    e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 3))
-    Ah0 = A0.cpu().pin_memory()
-    Bh0 = B0.cpu().pin_memory()
-    Ah = torch.empty_like(Ah0).pin_memory()
-    Bh = torch.empty_like(Bh0).pin_memory()
-    e2e_t = []
-    for i in range(e2e_steps + 1):
-        Ah.copy_(Ah0)
-        Bh.copy_(Bh0)
-        torch.cuda.synchronize()
-        barrier(world)
-        t0 = time.perf_counter()
-        rc = lnb.dspdsolv_main(n, nrhs, b, Ah.numpy().T, Bh.numpy().T)  # column-major views
-        t1 = time.perf_counter()
-        assert rc == 0
-        if i > 0:  # first call warms the pinned-path
-            e2e_t.append(t1 - t0)
-    e2e_sec = allmax(world, statistics.mean(e2e_t))
-    Xh = Bh.numpy().T
-    bw_e2e = backward_error_dev(A0, torch.from_numpy(np.ascontiguousarray(Xh.T)).to(dev), B0)
-    assert bw_e2e <= 10 * n * np.finfo(float).eps
-    nblk = (n + b - 1) // b
-    lower_elems = sum((n - j * b) * min(b, n - j * b) for j in range(nblk))
-    h2d = 8 * (lower_elems + n * nrhs)
-    d2h = 8 * (lower_elems + n * nrhs)
-
-    roof = None
-    if prof["update_ms"] > 0:
-        per_launch_flops = prof["update_flops"] / prof["update_launches"]
-        per_launch_ms = prof["update_ms"] / prof["update_launches"]
-        ach = per_launch_flops / (per_launch_ms * 1e-3) / 1e12
-        roof = {"bound": "tensor", "achieved": round(ach, 3), "peak": round(peak_fp64, 3), "unit": "TFLOP/s",
-                "frac": round(ach / peak_fp64, 4), "traffic": traffic_from_profiles("syrk_lower_f64", n, b),
-                "kernel": "k_syrk_lower_f64 (DMMA trailing update)",
-                "peak_source": "cuBLAS dgemm 8192^3 measured in this run (FP64 has no entry in "
-                               "MEASURED_PEAKS.json)",
-                "update_share_of_step": round(prof["update_ms"] / total_ms, 4)}
-
-    line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"spd_fp64_n{n}_b{b}_rhs{nrhs}", "n": n, "b": b, "nrhs": nrhs,
-                       "matrix": "G G^T/n + 1e-2 I, G~N(0,1)", "factor": "fp64 (DMMA)",
-                       "l2": "inputs (2 GiB) larger than L2; A restored between steps",
-                       "parallelism": f"replicas x{world}", "backward_error": bw},
-            "e2e": {"value": round(world * fl / e2e_sec / 1e12, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_sec * 1e3, 3),
-                    "api": "dspdsolv_main (host pointers, pinned), wall clock"},
-            "roofline": roof,
-            "gpu_launches": prof["launches"],
-            "clocks": clk.summary()}
-
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        ns = min(n, 8192)
-        Asample = make_spd(ns, 1e-2, 0, dev).cpu().numpy()
-        v, kind, cores, sec = cpu_run(ns, b, nrhs, 2, 1, Asample)
-        line["cpu_baseline"] = {"value": round(v, 6), "unit": UNIT, "cores": cores, "kind": kind,
-                                "sample": f"dspdsolv_main n={ns} b={b} nrhs={nrhs} (reference build, "
-                                          f"OpenBLAS {cores} threads), median of 2 after 1 warm-up, "
-                                          f"{sec:.2f} s each"}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-
-
 def backward_error_dev(A, X, B):
-    """||B - A X||_inf / (||A||_inf ||X||_inf + ||B||_inf); X, B as (nrhs, n) column-major rows."""
-    import torch
-    R = B.t() - A @ X.t()
+    """max over columns of ||B - A X||_inf / (||A||_inf ||X||_inf + ||B||_inf);
+    X, B as (nrhs, n) tensors (rows = columns of the column-major matrices)."""
     an = A.abs().sum(dim=1).max()
-    return float(R.abs().max() / (an * X.abs().max() + B.abs().max()))
+    worst = 0.0
+    for q in range(X.shape[0]):
+        r = B[q] - A @ X[q]
+        worst = max(worst, float(r.abs().max() / (an * X[q].abs().max() + B[q].abs().max())))
+    return worst
 
 
 def lnb_prof(L):
@@ -382,14 +306,205 @@ def lnb_prof(L):
     return {k: getattr(p, k) for k, _ in P._fields_}
 
 
-def traffic_from_profiles(kernel, n, b):
-    """DRAM bytes per launch of `kernel` from a committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
+def traffic_from_profiles(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
     try:
-        d = json.load(open(path))
+        d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
         return d.get(kernel, {}).get("dram_bytes_per_launch")
     except Exception:
         return None
+
+
+def ours_arm(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import linompss_b200 as lnb
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L = lnb.lib()
+    w = args.w
+    n, b, nrhs = w["n"], w["b"], w["nrhs"]
+    fl = flops_of(n, nrhs)
+    eps = np.finfo(float).eps / 2
+    peaks = measure_peaks(dev)
+
+    A0 = make_spd(n, w["delta"], 1234 + rank, dev, w["scaled"])
+    g = torch.Generator(device=dev)
+    g.manual_seed(99 + rank)
+    B0 = torch.randn(nrhs, n, dtype=torch.float64, device=dev, generator=g)   # column-major (nrhs, ld=n)
+    s = torch.cuda.current_stream()
+    mixed = w["factor"] != "FP64"
+
+    if mixed:
+        X = torch.zeros_like(B0)
+        opts = lnb.ir_opts(factor=getattr(lnb, "FACTOR_" + w["factor"]), max_iter=40, pcg_max_iter=400)
+        last = {}
+
+        def run_step():
+            rc, res = lnb.dsposv_ir_dev(A0, B0, X, n, nrhs, b, opts, stream=s)
+            assert rc == 0, (rc, res, lnb.last_error())
+            last.update(res)
+    else:
+        A = torch.empty_like(A0)
+        B = torch.empty_like(B0)
+        info = torch.zeros(1, dtype=torch.int32, device=dev)
+
+        def prep():
+            A.copy_(A0)
+            B.copy_(B0)
+
+        def run_step():
+            lnb.dposv_dev(A, B, n, nrhs, b, info=info, stream=s)
+
+    def timed_steps(k, prof):
+        evs = []
+        for _ in range(k):
+            if not mixed:
+                prep()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            run_step()
+            e1.record(s)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(bb) for a, bb in evs)
+
+    timed_steps(args.warmup, False)
+    barrier(world)
+    torch.cuda.synchronize()
+    L.lnb_prof_reset()
+    L.lnb_prof_enable(1)
+    with Clocks(local) as clk:
+        total_ms = timed_steps(args.steps, True)
+    barrier(world)
+    L.lnb_prof_enable(0)
+    prof = lnb_prof(L)
+    ms_step = allmax(world, total_ms / args.steps)
+    value = world * fl / (ms_step * 1e-3) / 1e12
+
+    Xres = X if mixed else B
+    bw = backward_error_dev(A0, Xres, B0)
+    assert bw <= 10 * n * eps, f"backward error {bw}"
+    if not mixed:
+        assert int(info.item()) == 0
+
+    line = {"metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if not mixed else "f64 (factor " +
+            w["factor"].lower() + ")", "data": "synthetic",
+            "config": {"workload": f"spd_{args.workload}_n{n}_b{b}_rhs{nrhs}", "n": n, "b": b, "nrhs": nrhs,
+                       "matrix": ("D (G G^T/n + %g I) D" if w["scaled"] else "G G^T/n + %g I") % w["delta"],
+                       "factor": w["factor"].lower(), "backward_error": bw,
+                       "l2": "inputs larger than L2 (126 MB); plain-FP64 A restored between steps",
+                       "parallelism": f"replicas x{world}"},
+            "gpu_launches": prof["launches"]}
+    if mixed:
+        line["config"]["ir"] = {k: last.get(k) for k in ("iterations", "used_pcg", "pcg_iterations",
+                                                         "factor_ms", "solve_ms", "backward_error")}
+
+    # roofline of the dominant kernel (the trailing update), timed live
+    if prof["update_ms"] > 0:
+        per_flops = prof["update_flops"] / prof["update_launches"]
+        per_ms = prof["update_ms"] / prof["update_launches"]
+        ach = per_flops / (per_ms * 1e-3) / 1e12
+        if w["factor"] == "FP64":
+            peak, src, kern = peaks["fp64"], "cuBLAS dgemm 8192^3 measured in this run", "k_syrk_lower_f64 (DMMA)"
+        elif w["factor"] == "TF32X3":
+            peak, src = peaks["tf32"] / 3.0, "cuBLAS TF32 GEMM 8192^3 measured in this run, / 3 products"
+            kern = "k_tc_syrk_lower<TF32X3> (tcgen05)"
+        elif w["factor"] == "BF16":
+            peak, src, kern = peaks["bf16"], "MEASURED_PEAKS.json bf16_tflops", "k_tc_syrk_lower<BF16> (tcgen05)"
+        else:
+            peak, src, kern = peaks["tf32"], "cuBLAS TF32 GEMM measured in this run", "k_tc_syrk_lower"
+        line["roofline"] = {"bound": "tensor", "achieved": round(ach, 3), "peak": round(peak, 3),
+                            "unit": "TFLOP/s", "frac": round(ach / peak, 4),
+                            "traffic": traffic_from_profiles(kern.split()[0]),
+                            "kernel": kern, "peak_source": src,
+                            "update_share_of_step": round(prof["update_ms"] / total_ms, 4),
+                            "flops_note": "algorithmic flops per launch: 2 k per updated lower-triangle element"}
+
+    # plain FP64 on the same matrix, same run: the comparison the metric names
+    if mixed and not args.no_plain:
+        Ap = torch.empty_like(A0)
+        Bp = torch.empty_like(B0)
+        infop = torch.zeros(1, dtype=torch.int32, device=dev)
+        tp = []
+        for i in range(2 + max(1, min(args.steps, 3))):
+            Ap.copy_(A0)
+            Bp.copy_(B0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            lnb.dposv_dev(Ap, Bp, n, nrhs, b, info=infop, stream=s)
+            e1.record(s)
+            torch.cuda.synchronize()
+            if i >= 2:
+                tp.append(e0.elapsed_time(e1))
+        plain_ms = allmax(world, statistics.mean(tp))
+        bwp = backward_error_dev(A0, Bp, B0)
+        line["fp64_plain"] = {"ms_per_step": round(plain_ms, 3), "value": round(world * fl / plain_ms / 1e9, 4),
+                              "backward_error": bwp, "speedup_mixed_vs_plain": round(plain_ms / ms_step, 3)}
+        del Ap, Bp
+        torch.cuda.empty_cache()
+
+    # e2e through the host entry point, pinned host buffers, copies inside
+    e2e_steps = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 3))
+    Ah = A0.cpu().pin_memory()
+    Bh = B0.cpu().pin_memory()
+    nblk = (n + b - 1) // b
+    lower_elems = sum((n - j * b) * min(b, n - j * b) for j in range(nblk))
+    e2e_t = []
+    if mixed:
+        Xh = torch.zeros_like(Bh).pin_memory()
+        res = lnb.IrResult()
+        lower512 = sum((n - c0) * min(512, n - c0) for c0 in range(0, n, 512))
+        for i in range(e2e_steps + 1):
+            barrier(world)
+            t0 = time.perf_counter()
+            rc = L.lnb_dsposv_ir(C.c_int(n), C.c_int(nrhs), C.c_int(b), C.c_void_p(Ah.data_ptr()), C.c_int(n),
+                                 C.c_void_p(Bh.data_ptr()), C.c_int(n), C.c_void_p(Xh.data_ptr()), C.c_int(n),
+                                 C.byref(opts), C.byref(res))
+            t1 = time.perf_counter()
+            assert rc == 0, lnb.last_error()
+            if i > 0:
+                e2e_t.append(t1 - t0)
+        bw_e2e = backward_error_dev(A0, Xh.to(dev), B0)
+        h2d, d2h = 8 * (lower512 + n * nrhs), 8 * n * nrhs
+        api = "lnb_dsposv_ir (host pointers, pinned), wall clock"
+    else:
+        Ahw = torch.empty_like(Ah).pin_memory()
+        Bhw = torch.empty_like(Bh).pin_memory()
+        for i in range(e2e_steps + 1):
+            Ahw.copy_(Ah)
+            Bhw.copy_(Bh)
+            barrier(world)
+            t0 = time.perf_counter()
+            rc = lnb.dspdsolv_main(n, nrhs, b, Ahw.numpy().T, Bhw.numpy().T)
+            t1 = time.perf_counter()
+            assert rc == 0
+            if i > 0:
+                e2e_t.append(t1 - t0)
+        bw_e2e = backward_error_dev(A0, Bhw.to(dev), B0)
+        h2d, d2h = 8 * (lower_elems + n * nrhs), 8 * (lower_elems + n * nrhs)
+        api = "dspdsolv_main (host pointers, pinned), wall clock"
+    assert bw_e2e <= 10 * n * eps, bw_e2e
+    e2e_sec = allmax(world, statistics.mean(e2e_t))
+    line["e2e"] = {"value": round(world * fl / e2e_sec / 1e12, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_sec * 1e3, 3), "api": api}
+    line["clocks"] = clk.summary()
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ns = min(n, 8192)
+        bs = min(b, 512)
+        Asample = make_spd(ns, w["delta"], 0, dev, w["scaled"]).cpu().numpy()
+        v, kind, cores, sec = cpu_run(ns, bs, nrhs, 2, 1, Asample)
+        line["cpu_baseline"] = {"value": round(v, 6), "unit": UNIT, "cores": cores, "kind": kind,
+                                "sample": f"dspdsolv_main n={ns} b={bs} nrhs={nrhs} (reference build, "
+                                          f"OpenBLAS {cores} threads), median of 2 after 1 warm-up, "
+                                          f"{sec:.2f} s each"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
 
 
 def main():

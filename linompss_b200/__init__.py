@@ -32,7 +32,7 @@ LIB_PATH = os.path.join(_HERE, "liblinompss_b200.so")
 
 LNB_OK, LNB_EINVAL, LNB_ENODEV, LNB_ECUDA, LNB_ENOMEM, LNB_ETIMEOUT, LNB_ENOCONV, LNB_ETOOBIG = (
     0, -1, -2, -3, -4, -5, -6, -7)
-FACTOR_FP64, FACTOR_FP32, FACTOR_TF32X3, FACTOR_BF16 = 0, 1, 2, 3
+FACTOR_FP64, FACTOR_FP32, FACTOR_TF32X3, FACTOR_BF16, FACTOR_TF32 = 0, 1, 2, 3, 4
 
 
 class LinompssError(RuntimeError):
@@ -258,6 +258,56 @@ def dtrsm_dev(uplo: str, trans: str, diag: str, m: int, n: int, alpha: float, At
                   C.c_void_p, C.c_int, C.c_void_p]
     return _chk(f(uplo.encode(), trans.encode(), diag.encode(), m, n, alpha, _p(At), _ld(At), _p(Bt), _ld(Bt),
                   _stream(stream)))
+
+
+class IrOpts(C.Structure):
+    """lnb_ir_opts"""
+    _fields_ = [("factor", C.c_int), ("max_iter", C.c_int), ("tol", C.c_double), ("equilibrate", C.c_int),
+                ("allow_pcg", C.c_int), ("pcg_max_iter", C.c_int)]
+
+
+class IrResult(C.Structure):
+    """lnb_ir_result"""
+    _fields_ = [("iterations", C.c_int), ("pcg_iterations", C.c_int), ("used_pcg", C.c_int),
+                ("refactored_tiles", C.c_int), ("backward_error", C.c_double), ("factor_ms", C.c_double),
+                ("solve_ms", C.c_double), ("info", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+def ir_opts(**kw) -> IrOpts:
+    o = IrOpts()
+    lib().lnb_ir_default_opts(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def dsposv_ir(A: np.ndarray, B: np.ndarray, b: int, opts: IrOpts | None = None):
+    """Mixed-precision solve A X = B (host arrays, column-major).  Returns
+    (rc, X, result dict); rc is 0 or LNB_ENOCONV (the call still returns X)."""
+    _colmajor(A)
+    B = np.asfortranarray(B.reshape(A.shape[0], -1))
+    n, nrhs = B.shape
+    X = np.zeros((n, nrhs), order="F")
+    res = IrResult()
+    rc = lib().lnb_dsposv_ir(C.c_int(n), C.c_int(nrhs), C.c_int(b), _p(A), C.c_int(A.shape[0]), _p(B),
+                             C.c_int(n), _p(X), C.c_int(n), C.byref(opts) if opts is not None else None,
+                             C.byref(res))
+    if rc < 0 and rc != LNB_ENOCONV:
+        raise LinompssError(rc, last_error())
+    return rc, X, res.as_dict()
+
+
+def dsposv_ir_dev(At, Bt, Xt, n: int, nrhs: int, b: int, opts: IrOpts | None = None, stream=None):
+    res = IrResult()
+    rc = lib().lnb_dsposv_ir_dev(C.c_int(n), C.c_int(nrhs), C.c_int(b), _p(At), C.c_int(_ld(At)), _p(Bt),
+                                 C.c_int(_ld(Bt)), _p(Xt), C.c_int(_ld(Xt)),
+                                 C.byref(opts) if opts is not None else None, C.byref(res), _stream(stream))
+    if rc < 0 and rc != LNB_ENOCONV:
+        raise LinompssError(rc, last_error())
+    return rc, res.as_dict()
 
 
 def set_wait_limit_us(us: int) -> None:

@@ -305,3 +305,119 @@ extern "C" int lnb_k_lower_to_f32(const double *A, int64_t lda, int64_t n, int e
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }
+
+// ------------------------------------------------------------------------
+// FP64 refactor of a failed low-precision diagonal tile
+// ------------------------------------------------------------------------
+namespace lnb {
+// T[r,c] = s_r A[r,c] s_c for r >= c (bs x bs, FP64, ld ldt)
+__global__ void k_scaled_tile_f64(const double *A, int64_t lda, const double *s, int bs, double *T, int64_t ldt)
+{
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < bs * bs; idx += gridDim.x * blockDim.x) {
+        const int c = idx / bs, r = idx % bs;
+        if (r >= c) T[r + (int64_t)c * ldt] = s[r] * A[r + (int64_t)c * lda] * s[c];
+    }
+}
+// D (m x k, FP64, ld ldd) = X (FP32, ld ldx)
+__global__ void k_f32_to_f64(const float *X, int64_t ldx, int64_t m, int64_t k, double *D, int64_t ldd)
+{
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < m * k;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = idx / m, r = idx % m;
+        D[r + c * ldd] = (double)X[r + c * ldx];
+    }
+}
+// lower triangle of the FP64 tile back into FP32
+__global__ void k_f64_to_f32_lower(const double *T, int64_t ldt, int bs, float *X, int64_t ldx)
+{
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < bs * bs; idx += gridDim.x * blockDim.x) {
+        const int c = idx / bs, r = idx % bs;
+        if (r >= c) X[r + (int64_t)c * ldx] = (float)T[r + (int64_t)c * ldt];
+    }
+}
+// T[i,i] += shift; also copies src -> T first when src != NULL (lower part)
+__global__ void k_restore_shift(const double *src, double *T, int64_t ldt, int bs, double shift)
+{
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < bs * bs; idx += gridDim.x * blockDim.x) {
+        const int c = idx / bs, r = idx % bs;
+        if (r >= c) T[r + (int64_t)c * ldt] = src[r + (int64_t)c * ldt] + (r == c ? shift : 0.0);
+    }
+}
+// max |T[i,i]| into out[0] (one CTA)
+__global__ void k_diag_absmax(const double *T, int64_t ldt, int bs, double *out)
+{
+    __shared__ double red[256];
+    double m = 0.0;
+    for (int i = threadIdx.x; i < bs; i += 256) m = fmax(m, fabs(T[i + (int64_t)i * ldt]));
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = red[0];
+}
+// inverses of the 32x32 diagonal blocks of an FP32 factored tile (warp per block)
+__global__ void k_dinv32_f32(const float *L, int64_t ldl, int bs, float *dinv)
+{
+    __shared__ float X[32][33];
+    const int q = blockIdx.x, c = threadIdx.x, o = q * 32;
+    const int qn = bs - o < 32 ? bs - o : 32;
+    for (int r = 0; r < 32; ++r) {
+        float v;
+        if (c >= qn) v = (r == c) ? 1.f : 0.f;
+        else if (r < c || r >= qn) v = 0.f;
+        else if (r == c) v = 1.f / L[(o + c) + (int64_t)(o + c) * ldl];
+        else {
+            float s = 0.f;
+            for (int p = c; p < r; ++p) s += L[(o + r) + (int64_t)(o + p) * ldl] * X[p][c];
+            v = -s / L[(o + r) + (int64_t)(o + r) * ldl];
+        }
+        X[r][c] = v;
+        __syncwarp();
+    }
+    for (int r = 0; r < 32; ++r) dinv[(int64_t)q * 1024 + r + 32 * c] = X[r][c];
+}
+}  // namespace lnb
+
+static unsigned g1(int64_t work) { int64_t b = (work + 255) / 256; return (unsigned)(b < 4096 ? (b > 0 ? b : 1) : 4096); }
+
+extern "C" int lnb_k_scaled_tile_f64(const double *A, int64_t lda, const double *s, int bs, double *T, int64_t ldt,
+                                     lnb_stream_t st)
+{
+    k_scaled_tile_f64<<<g1((int64_t)bs * bs), 256, 0, st>>>(A, lda, s, bs, T, ldt);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+extern "C" int lnb_k_f32_to_f64(const float *X, int64_t ldx, int64_t m, int64_t k, double *D, int64_t ldd,
+                                lnb_stream_t st)
+{
+    if (m <= 0 || k <= 0) return 0;
+    k_f32_to_f64<<<g1(m * k), 256, 0, st>>>(X, ldx, m, k, D, ldd);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+extern "C" int lnb_k_f64_to_f32_lower(const double *T, int64_t ldt, int bs, float *X, int64_t ldx, lnb_stream_t st)
+{
+    k_f64_to_f32_lower<<<g1((int64_t)bs * bs), 256, 0, st>>>(T, ldt, bs, X, ldx);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+extern "C" int lnb_k_restore_shift(const double *src, double *T, int64_t ldt, int bs, double shift, lnb_stream_t st)
+{
+    k_restore_shift<<<g1((int64_t)bs * bs), 256, 0, st>>>(src, T, ldt, bs, shift);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+extern "C" int lnb_k_diag_absmax(const double *T, int64_t ldt, int bs, double *out, lnb_stream_t st)
+{
+    k_diag_absmax<<<1, 256, 0, st>>>(T, ldt, bs, out);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+extern "C" int lnb_k_dinv32_f32(const float *L, int64_t ldl, int bs, float *dinv, lnb_stream_t st)
+{
+    k_dinv32_f32<<<(unsigned)((bs + 31) / 32), 32, 0, st>>>(L, ldl, bs, dinv);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}

@@ -75,6 +75,71 @@ typedef struct {
     float *scale[2];
 } panelbuf;
 
+int lnb_k_scaled_tile_f64(const double *A, int64_t lda, const double *s, int bs, double *T, int64_t ldt,
+                          cudaStream_t st);
+int lnb_k_f32_to_f64(const float *X, int64_t ldx, int64_t m, int64_t k, double *D, int64_t ldd, cudaStream_t st);
+int lnb_k_f64_to_f32_lower(const double *T, int64_t ldt, int bs, float *X, int64_t ldx, cudaStream_t st);
+int lnb_k_restore_shift(const double *src, double *T, int64_t ldt, int bs, double shift, cudaStream_t st);
+int lnb_k_diag_absmax(const double *T, int64_t ldt, int bs, double *out, cudaStream_t st);
+int lnb_k_dinv32_f32(const float *L, int64_t ldl, int bs, float *dinv, cudaStream_t st);
+
+#define RF_KC 2048
+
+size_t lnb_refactor_ws_bytes(int b)
+{
+    return 2 * lnb_align256((size_t)b * b * 8) + lnb_align256((size_t)b * RF_KC * 8) +
+           lnb_align256((size_t)((b + 31) / 32) * 1024 * 8) + 1024;
+}
+
+/* FP64 diagonal-tile refactor after a failed low-precision pivot in tile
+ * [k0, k0+bs): the tile's Schur complement is recomputed in FP64 from the
+ * original matrix and the finished FP32 panel rows,
+ *     T = S_k A_kk S_k - L_k,0:k0 L_k,0:k0^T,
+ * factored in FP64 (with a growing diagonal shift if even that is not
+ * positive definite), and written back as the FP32 factor tile together
+ * with its 32x32 block inverses.  Returns 0 when the tile was repaired,
+ * > 0 if it could not be. */
+static int refactor_tile(lnb_ctx *c, lnb_refactor_ctx *rf, float *dA, int64_t lda, int64_t k0, int bs, int b,
+                         float *dinv, lnb_arena *ar_in, cudaStream_t s)
+{
+    lnb_arena ar = *ar_in;   /* scratch is released on return */
+    double *T = lnb_arena_take(&ar, (size_t)b * b * 8), *T0 = lnb_arena_take(&ar, (size_t)b * b * 8);
+    double *chunk = lnb_arena_take(&ar, (size_t)b * RF_KC * 8);
+    double *dinv64 = lnb_arena_take(&ar, (size_t)((b + 31) / 32) * 1024 * 8);
+    if (!dinv64) return lnb_set_error(LNB_ENOMEM, "refactor workspace");
+    CK(cudaMemsetAsync(&c->st->info, 0, sizeof(int), s), "info reset");
+    CK(lnb_k_scaled_tile_f64(rf->A + k0 + k0 * rf->lda, rf->lda, rf->S + k0, bs, T, b, s), "tile");
+    for (int64_t kc = 0; kc < k0; kc += RF_KC) {
+        const int64_t kw = k0 - kc < RF_KC ? k0 - kc : RF_KC;
+        CK(lnb_k_f32_to_f64(dA + k0 + kc * lda, lda, bs, kw, chunk, bs, s), "panel rows");
+        CK(lnb_k_syrk_lower_f64(chunk, bs, T, b, bs, 0, bs, (int)kw, s), "schur");
+    }
+    CK(cudaMemcpyAsync(T0, T, (size_t)b * bs * 8, cudaMemcpyDeviceToDevice, s), "backup");
+    double dmax = 0.0;
+    int info = 1;
+    for (int t = 0; t < 8 && info != 0; ++t) {
+        if (t > 0) {
+            if (t == 1) {
+                CK(lnb_k_diag_absmax(T0, b, bs, chunk, s), "diag max");
+                CK(cudaMemcpyAsync(&dmax, chunk, 8, cudaMemcpyDeviceToHost, s), "read");
+                CK(cudaStreamSynchronize(s), "sync");
+            }
+            const double shift = dmax * ldexp(1.0, -24 + 4 * t);
+            CK(lnb_k_restore_shift(T0, T, b, bs, shift, s), "shift");
+            CK(cudaMemsetAsync(&c->st->info, 0, sizeof(int), s), "info reset");
+            rf->shifted++;
+        }
+        { int e = lnb_potrf_tile_f64(T, b, bs, k0, dinv64, c->st, s); if (e) return e; }
+        info = lnb_status_read(c, s);
+        if (info < 0) return info;
+    }
+    if (info != 0) return info;
+    CK(lnb_k_f64_to_f32_lower(T, b, bs, dA + k0 + k0 * lda, lda, s), "write back");
+    CK(lnb_k_dinv32_f32(dA + k0 + k0 * lda, lda, bs, dinv, s), "block inverses");
+    rf->refactored++;
+    return 0;
+}
+
 static int upd32(const panelbuf *pb, int slot, const float *P, int64_t ldp, float *C, int64_t ldc,
                  int64_t nrows, int64_t c0, int64_t c1, int k, lnb_status_t *st, cudaStream_t s)
 {
@@ -94,7 +159,8 @@ static int upd32(const panelbuf *pb, int slot, const float *P, int64_t ldp, floa
     return e;
 }
 
-int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_arena *ar, cudaStream_t s)
+int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_refactor_ctx *rf,
+                     lnb_arena *ar, cudaStream_t s)
 {
     float *dinv = (float *)lnb_arena_take(ar, (size_t)((b + 31) / 32) * 1024 * sizeof(float));
     if (!dinv) return lnb_set_error(LNB_ENOMEM, "chol32 workspace");
@@ -128,6 +194,15 @@ int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode,
         const int64_t mrem = n - k0 - bs;
         const int slot = k & 1;
         { int _e = lnb_potrf_tile_f32(Akk, lda, bs, k0, dinv, c->st, crit); if (_e) return _e; }
+        if (rf) {
+            /* the refinement driver wants a usable factor: check this tile now */
+            int info = lnb_status_read(c, crit);
+            if (info < 0) return info;
+            if (info > 0) {
+                int e = refactor_tile(c, rf, dA, lda, k0, bs, b, dinv, ar, crit);
+                if (e) return e;
+            }
+        }
         if (mrem > 0) {
             CK(lnb_k_trsm_rlt_f32(Akk, lda, dinv, Akk + bs, lda, mrem, bs, crit), "trsm f32");
             if (mode == LNB_FACTOR_TF32X3 || mode == LNB_FACTOR_TF32)
@@ -176,7 +251,7 @@ int lnb_schol_dev(int n, int b, float *dA, int lda, int *info_dev, void *stream)
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     cudaStream_t s = (cudaStream_t)stream;
-    if ((e = lnb_chol_f32_run(c, n, b, dA, lda, g_schol_mode, &ar, s))) return e;
+    if ((e = lnb_chol_f32_run(c, n, b, dA, lda, g_schol_mode, NULL, &ar, s))) return e;
     if (info_dev) CK(cudaMemcpyAsync(info_dev, &c->st->info, sizeof(int), cudaMemcpyDeviceToDevice, s), "info");
     return 0;
 }
@@ -201,7 +276,7 @@ static int schol_host(int n, int b, float *A, int lda)
                              (size_t)lda * sizeof(float), (size_t)(n - c0) * sizeof(float), w,
                              cudaMemcpyHostToDevice, s), "A in");
     }
-    if ((e = lnb_chol_f32_run(c, n, b, dA, ldd, g_schol_mode, &ar, s))) return e;
+    if ((e = lnb_chol_f32_run(c, n, b, dA, ldd, g_schol_mode, NULL, &ar, s))) return e;
     for (int64_t c0 = 0; c0 < n; c0 += b) {
         const int64_t w = n - c0 < b ? n - c0 : b;
         CK(cudaMemcpy2DAsync(A + c0 + c0 * (int64_t)lda, (size_t)lda * sizeof(float), dA + c0 + c0 * ldd,
@@ -235,7 +310,7 @@ static int schol_hyper(int mt, int b, float **Ah)
                                  Ah[(int64_t)j * mt + i], (size_t)b * sizeof(float), (size_t)b * sizeof(float),
                                  (size_t)b, cudaMemcpyHostToDevice, s), "tile in");
         }
-    int e = lnb_chol_f32_run(c, (int)n, b, dA, ldd, g_schol_mode, &ar, s);
+    int e = lnb_chol_f32_run(c, (int)n, b, dA, ldd, g_schol_mode, NULL, &ar, s);
     if (e) return e;
     for (int j = 0; j < mt; ++j)
         for (int i = j; i < mt; ++i)

@@ -71,8 +71,19 @@ int lnb_chol_f64_run(lnb_ctx *c, int n, int b, double *dA, int64_t lda, lnb_aren
 int lnb_potrf_tile_f32(float *Akk, int64_t lda, int bs, int64_t row0, float *dinv, lnb_status_t *st,
                        cudaStream_t s);
 size_t lnb_chol_f32_ws_bytes(int n, int b, int mode);
-int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_arena *ar,
-                     cudaStream_t s);
+/* FP64 diagonal-tile refactor context: when passed to lnb_chol_f32_run, a
+ * diagonal tile whose low-precision pivot is not positive is rebuilt from
+ * the original FP64 matrix (lower part, equilibration S) and refactored in
+ * FP64; the arena must then also hold lnb_refactor_ws_bytes(b). */
+typedef struct {
+    const double *A;
+    int64_t lda;
+    const double *S;
+    int refactored, shifted;
+} lnb_refactor_ctx;
+size_t lnb_refactor_ws_bytes(int b);
+int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_refactor_ctx *rf,
+                     lnb_arena *ar, cudaStream_t s);
 int lnb_get_factor_mode(void);
 
 /* ---- FP64 triangular solves on device memory (lnb_solve.c) --------------- */

@@ -66,7 +66,7 @@ static size_t ir_ws_bytes(int64_t n, int64_t nrhs, int b, int mode)
                lnb_align256((size_t)nb * TRSV_H * TRSV_H * 8) + 5 * lnb_align256((size_t)n * nrhs * 8) +
                lnb_align256((size_t)8 * (nrhs + 1) * 8) +
                lnb_align256((size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4) + 4096;
-    return s + lnb_chol_f32_ws_bytes((int)n, b, mode);
+    return s + lnb_chol_f32_ws_bytes((int)n, b, mode) + lnb_refactor_ws_bytes(b);
 }
 
 /* z = M^-1 r = S L^-T L^-1 S r   (in place in Z, reading R) */
@@ -87,9 +87,9 @@ static int residual(lnb_ctx *c, const irws *w, const double *dA, int64_t lda, co
 {
     (void)c;
     const int64_t n = w->n, nrhs = w->nrhs;
-    /* Y = X packed with ld n, then Y = A Y */
-    CK(cudaMemcpy2DAsync(w->P, n * 8, dX, ldx * 8, n * 8, nrhs, cudaMemcpyDeviceToDevice, s), "pack x");
-    CK(lnb_k_symv_lower_f64(n, nrhs, dA, lda, w->P, w->Y, 0, s), "symv");
+    /* Q = X packed with ld n (Q is free here: PCG recomputes it each step), Y = A Q */
+    CK(cudaMemcpy2DAsync(w->Q, n * 8, dX, ldx * 8, n * 8, nrhs, cudaMemcpyDeviceToDevice, s), "pack x");
+    CK(lnb_k_symv_lower_f64(n, nrhs, dA, lda, w->Q, w->Y, 0, s), "symv");
     CK(lnb_k_resid_f64(n, nrhs, dB, ldb, w->Y, w->R, w->scal, s), "resid");
     CK(lnb_k_colmax_f64(n, nrhs, dX, ldx, w->scal + nrhs, s), "xmax");
     double h[2 * 64 + 2];
@@ -149,8 +149,13 @@ int lnb_dsposv_ir_dev(int n, int nrhs, int b, const double *dA, int lda, const d
     /* ---- factor ---- */
     CK(cudaEventRecord(c->t0, s), "event");
     CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, s), "convert");
-    int e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &ar, s);
-    if (e) return e;
+    lnb_refactor_ctx rf = {dA, lda, w.S, 0, 0};
+    int e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &rf, &ar, s);
+    rr.refactored_tiles = rf.refactored;
+    if (e) {
+        if (e > 0 && res) { rr.info = e; *res = rr; }
+        return e > 0 ? lnb_set_error(e, "low-precision factor: tile at row %d could not be refactored", e) : e;
+    }
     CK(lnb_k_trtri_blocks_f32(w.A32, w.ld32, n, TRSV_H, 'L', 0, w.dinv, s), "trtri");
     CK(cudaEventRecord(c->t1, s), "event");
     int info = lnb_status_read(c, s);

@@ -1,0 +1,109 @@
+"""Mixed precision: low-precision factor + FP64 refinement (lnb_dsposv_ir).
+
+The bar is the north star's: FP64-level normwise backward error
+||b - A x||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 10 n eps (eps = 2^-53),
+reached from an FP32 / TF32x3 / BF16 factor; the forward error against the
+FP64 solution is bounded by cond(A) times that.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+EPS = np.finfo(np.float64).eps / 2
+
+
+@pytest.fixture(scope="module")
+def lnb(cuda):
+    import linompss_b200
+    return linompss_b200
+
+
+def check(lnb, A0, B0, b, factor, **kw):
+    n = A0.shape[0]
+    opts = lnb.ir_opts(factor=factor, **kw)
+    rc, X, res = lnb.dsposv_ir(A0.copy(order="F"), B0, b, opts)
+    assert rc == 0, (rc, res, lnb.last_error())
+    be = O.backward_error_np(A0, X, B0)
+    assert be <= 10 * n * EPS, (be, res)
+    assert res["backward_error"] <= 10 * n * EPS
+    return X, res
+
+
+@pytest.mark.parametrize("factor", ["FACTOR_TF32X3", "FACTOR_FP32", "FACTOR_BF16", "FACTOR_TF32"])
+def test_ir_well_conditioned(lnb, factor):
+    n, b = 2048, 256
+    A0 = O.spd_covariance(n, 1e-1, seed=1)
+    B0 = np.asfortranarray(np.random.default_rng(1).standard_normal((n, 1)))
+    X, res = check(lnb, A0, B0, b, getattr(lnb, factor))
+    Xref = np.linalg.solve(A0, B0)
+    assert np.abs(X - Xref).max() / np.abs(Xref).max() <= 1e-10
+    if factor in ("FACTOR_TF32X3", "FACTOR_FP32"):
+        assert res["iterations"] <= 4 and not res["used_pcg"]
+
+
+@pytest.mark.parametrize("delta", [1e-1, 1e-3, 1e-5])
+def test_ir_tf32x3_delta_sweep(lnb, delta):
+    """configs[2]'s matrix family G G^T/n + delta I at reduced n (cond ~4e1..4e5)."""
+    n, b = 3072, 512
+    A0 = O.spd_covariance(n, delta, seed=2)
+    B0 = np.asfortranarray(np.random.default_rng(2).standard_normal((n, 1)))
+    X, res = check(lnb, A0, B0, b, lnb.FACTOR_TF32X3)
+    assert res["iterations"] <= 12
+
+
+def test_ir_bf16_badly_scaled_multi_rhs(lnb):
+    """configs[3]'s family D (G G^T/n + delta I) D, D = diag(10^u), u ~ U[-2,2],
+    8 right-hand sides, at reduced n; BF16 factor + equilibration + PCG fallback."""
+    n, b, nrhs = 2048, 512, 8
+    rng = np.random.default_rng(3)
+    D = 10.0 ** rng.uniform(-2, 2, n)
+    A0 = O.fortran(D[:, None] * O.spd_covariance(n, 1e-4, seed=3) * D[None, :])
+    B0 = np.asfortranarray(rng.standard_normal((n, nrhs)))
+    X, res = check(lnb, A0, B0, b, lnb.FACTOR_BF16, max_iter=40, pcg_max_iter=400)
+
+
+def test_ir_bf16_without_equilibration_still_refines(lnb):
+    n, b = 1024, 256
+    A0 = O.spd_covariance(n, 1e-2, seed=4)
+    B0 = np.asfortranarray(np.random.default_rng(4).standard_normal((n, 2)))
+    check(lnb, A0, B0, b, lnb.FACTOR_BF16, equilibrate=0, max_iter=40)
+
+
+def test_ir_pcg_fallback_triggers(lnb):
+    """A BF16 factor of a cond ~4e5 matrix cannot refine plainly (cond * u_bf16 >> 1):
+    the stall detector must switch to PCG, which then converges."""
+    n, b = 2048, 256
+    A0 = O.spd_covariance(n, 1e-5, seed=5)
+    B0 = np.asfortranarray(np.random.default_rng(5).standard_normal((n, 1)))
+    X, res = check(lnb, A0, B0, b, lnb.FACTOR_BF16, max_iter=30, pcg_max_iter=800)
+    assert res["used_pcg"] == 1 and res["pcg_iterations"] > 0
+
+
+def test_ir_reports_noconv_when_disallowed(lnb):
+    n, b = 1024, 256
+    A0 = O.spd_covariance(n, 1e-6, seed=6)
+    B0 = np.asfortranarray(np.random.default_rng(6).standard_normal((n, 1)))
+    opts = lnb.ir_opts(factor=lnb.FACTOR_BF16, allow_pcg=0, max_iter=3)
+    rc, X, res = lnb.dsposv_ir(A0.copy(order="F"), B0, b, opts)
+    assert rc == lnb.LNB_ENOCONV
+    assert res["iterations"] == 3 and res["backward_error"] > 10 * n * EPS
+
+
+def test_ir_device_api_leaves_A_untouched(lnb, cuda):
+    import torch
+    n, b, nrhs = 1536, 256, 3
+    A0 = O.spd_covariance(n, 1e-2, seed=7)
+    B0 = np.random.default_rng(7).standard_normal((n, nrhs))
+    At = torch.tensor(np.ascontiguousarray(A0.T), device=cuda)
+    Bt = torch.tensor(np.ascontiguousarray(B0.T), device=cuda)
+    Xt = torch.zeros_like(Bt)
+    A_before = At.clone()
+    rc, res = lnb.dsposv_ir_dev(At, Bt, Xt, n, nrhs, b, lnb.ir_opts(factor=lnb.FACTOR_TF32X3))
+    torch.cuda.synchronize()
+    assert rc == 0
+    assert torch.equal(At, A_before)
+    X = Xt.cpu().numpy().T
+    assert O.backward_error_np(A0, X, B0) <= 10 * n * EPS
+    assert res["factor_ms"] > 0 and res["solve_ms"] > 0
