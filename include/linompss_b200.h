@@ -145,7 +145,6 @@ LNB_EXPORT int ompss_ditref(int n, int bm, const double *A, int lda, const doubl
  * stream. */
 LNB_EXPORT int lnb_dchol_dev(int n, int b, double *dA, int lda, int *info_dev, void *stream);
 LNB_EXPORT int lnb_schol_dev(int n, int b, float *dA, int lda, int *info_dev, void *stream);
-
 /* Triangular solves with the lower factor: trans 'N' solves L Y = B,
  * 'T' solves L^T X = B, 'B' (both) solves L L^T X = B.  dB: n x nrhs, ld = ldb. */
 LNB_EXPORT int lnb_dpotrs_dev(int n, int nrhs, const double *dL, int lda, double *dB, int ldb,
@@ -223,6 +222,14 @@ LNB_EXPORT int lnb_batched_posv_dev(int count, const int *n_dev, const int *nrhs
                                     const double *dA, const double *dB, double *dX,
                                     int mode, int max_iter, int *info_dev, int *iters_dev,
                                     void *stream);
+/* Autotuner: times the candidate panel widths of the per-system factorization
+ * on this batch (synchronous) and keeps the fastest for later
+ * lnb_batched_posv_dev calls of the same mode.  Returns the chosen width.
+ * Each system's A_s is n x n FP64 with both triangles stored. */
+LNB_EXPORT int lnb_batched_autotune(int count, const int *n_dev, const int *nrhs_dev,
+                                    const int64_t *a_off_dev, const int64_t *b_off_dev,
+                                    const double *dA, const double *dB, double *dX,
+                                    int mode, int max_iter, void *stream);
 
 /* ======================================================================== */
 /* 5. Runtime                                                                 */

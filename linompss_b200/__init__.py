@@ -310,6 +310,37 @@ def dsposv_ir_dev(At, Bt, Xt, n: int, nrhs: int, b: int, opts: IrOpts | None = N
     return rc, res.as_dict()
 
 
+def _batched_args(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode, max_iter):
+    count = int(n_dev.numel())
+    return [C.c_int(count), _p(n_dev), _p(nrhs_dev), _p(a_off_dev), _p(b_off_dev), _p(dA), _p(dB), _p(dX),
+            C.c_int(mode), C.c_int(max_iter)]
+
+
+def batched_posv_dev(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode=FACTOR_FP32, max_iter=10,
+                     info=None, iters=None, stream=None) -> int:
+    """count = n_dev.numel() systems; int32 sizes, int64 offsets (elements) into the flat
+    FP64 buffers dA (n x n each, full symmetric) and dB/dX (n x nrhs each)."""
+    args = _batched_args(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode, max_iter)
+    return _chk(lib().lnb_batched_posv_dev(*args, _p(info), _p(iters), _stream(stream)))
+
+
+def batched_autotune(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode=FACTOR_FP32, max_iter=10,
+                     stream=None) -> int:
+    args = _batched_args(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode, max_iter)
+    return _chk(lib().lnb_batched_autotune(*args, _stream(stream)))
+
+
+def spotrs_dev(Lt, Bt, n: int, nrhs: int, which: str = "B", stream=None) -> int:
+    return _chk(lib().lnb_spotrs_dev(C.c_int(n), C.c_int(nrhs), _p(Lt), C.c_int(_ld(Lt)), _p(Bt),
+                                     C.c_int(_ld(Bt)), C.c_char(which.encode()), _stream(stream)))
+
+
+def sspdsolv_main(m: int, n: int, b: int, A: np.ndarray, B: np.ndarray) -> int:
+    _colmajor(A, np.float32)
+    _colmajor(B, np.float32)
+    return _chk(lib().sspdsolv_main(C.c_int(m), C.c_int(n), C.c_int(b), _p(A), _p(B)))
+
+
 def set_wait_limit_us(us: int) -> None:
     lib().lnb_set_wait_limit_us(C.c_longlong(us))
 

@@ -123,12 +123,20 @@ __global__ void __launch_bounds__(256) k_syrk_lower_f32_simt(const float *__rest
         }
         __syncthreads();
     }
+    float cv[4][4];   // loads first, then stores (avoids serialized read-modify-writes)
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int64_t r = rbase + ty + 16 * i, c = cbase + tx + 16 * j;
-            if (r < nrows && c < c1 && r >= c) C[r + c * ldc] -= acc[i][j];
+            cv[i][j] = (r < nrows && c < c1 && r >= c) ? C[r + c * ldc] : 0.f;
+        }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t r = rbase + ty + 16 * i, c = cbase + tx + 16 * j;
+            if (r < nrows && c < c1 && r >= c) C[r + c * ldc] = cv[i][j] - acc[i][j];
         }
 }
 
@@ -418,6 +426,26 @@ extern "C" int lnb_k_diag_absmax(const double *T, int64_t ldt, int bs, double *o
 extern "C" int lnb_k_dinv32_f32(const float *L, int64_t ldl, int bs, float *dinv, lnb_stream_t st)
 {
     k_dinv32_f32<<<(unsigned)((bs + 31) / 32), 32, 0, st>>>(L, ldl, bs, dinv);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+
+namespace lnb {
+__global__ void k_f64_to_f32(const double *D, int64_t ldd, int64_t m, int64_t k, float *X, int64_t ldx)
+{
+    for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < m * k;
+         idx += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = idx / m, r = idx % m;
+        X[r + c * ldx] = (float)D[r + c * ldd];
+    }
+}
+}  // namespace lnb
+
+extern "C" int lnb_k_f64_to_f32(const double *D, int64_t ldd, int64_t m, int64_t k, float *X, int64_t ldx,
+                                lnb_stream_t st)
+{
+    if (m <= 0 || k <= 0) return 0;
+    k_f64_to_f32<<<g1(m * k), 256, 0, st>>>(D, ldd, m, k, X, ldx);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }

@@ -138,18 +138,28 @@ __global__ void __launch_bounds__(Cfg::THREADS) k_syrk_lower_f64(const double *_
     }
     cp_async_wait<0>();
 
-    // epilogue: C -= acc on r >= c inside [0,nrows) x [c0,c1)
+    // epilogue: C -= acc on r >= c inside [0,nrows) x [c0,c1).  Per m16 row
+    // block, every load is issued before any store (through one pointer the
+    // compiler would otherwise serialize each read-modify-write).
 #pragma unroll
     for (int mi = 0; mi < MI; ++mi) {
+        double cv[NI][4];
 #pragma unroll
-        for (int ni = 0; ni < NI; ++ni) {
+        for (int ni = 0; ni < NI; ++ni)
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 const int64_t r = rbase + wm * TM + mi * 16 + g + ((q & 2) ? 8 : 0);
                 const int64_t c = cbase + wn * TN + ni * 8 + 2 * t + (q & 1);
-                if (r < nrows && c < c1 && r >= c) C[r + c * ldc] -= acc[mi][ni][q];
+                cv[ni][q] = (r < nrows && c < c1 && r >= c) ? C[r + c * ldc] : 0.0;
             }
-        }
+#pragma unroll
+        for (int ni = 0; ni < NI; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int64_t r = rbase + wm * TM + mi * 16 + g + ((q & 2) ? 8 : 0);
+                const int64_t c = cbase + wn * TN + ni * 8 + 2 * t + (q & 1);
+                if (r < nrows && c < c1 && r >= c) C[r + c * ldc] = cv[ni][q] - acc[mi][ni][q];
+            }
     }
 }
 

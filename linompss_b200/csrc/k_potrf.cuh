@@ -7,10 +7,10 @@
 // sub-tiles), the structure of the reference's nested variant
 // (chol_nrlmain.c).
 //
-// The whole tile lives in shared memory (128 x 129 doubles = 129 KB).  Each
-// 16-column panel is factored by warp 0 alone, entirely in registers with
-// shuffles (no block barriers inside the panel); the other warps then apply
-// the rank-16 update to the trailing lower triangle in shared memory.  At the
+// The whole tile lives in shared memory (128 x 129 doubles = 129 KB).  For
+// each 16-column panel, warp 0 factors the 16 x 16 diagonal block in
+// registers with shuffles; then all threads solve the rows below it (one row
+// per thread) and apply the rank-16 update to the trailing lower triangle.  At the
 // end the inverses of the tile's 32x32 diagonal blocks (used by the panel
 // TRSM) are computed from the factor in shared memory.
 #pragma once
@@ -41,50 +41,33 @@ __global__ void __launch_bounds__(256) k_potrf_leaf(T *A, int64_t lda, int bs, i
     for (int j0 = 0; j0 < bs; j0 += LP) {
         const int jb = min(LP, bs - j0);
         if (warp == 0) {
-            // rows j0 + lane + 32*s, s < 4, columns j0 .. j0+jb
-            T x[4][LP];
+            // (1) the jb x jb diagonal block in registers: lane l holds row j0+l
+            T x[LP];
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const int r = j0 + lane + 32 * s;
-#pragma unroll
-                for (int c = 0; c < LP; ++c)
-                    x[s][c] = (r < bs && c < jb && r >= j0 + c) ? S[r * LDS + j0 + c] : T(0);
-            }
+            for (int c = 0; c < LP; ++c)
+                x[c] = (lane < jb && c < jb && lane >= c) ? S[(j0 + lane) * LDS + j0 + c] : T(0);
             int bad = bs;
 #pragma unroll
             for (int c = 0; c < LP; ++c) {
                 if (c < jb && bad == bs) {
-                    // diagonal element of column c lives in lane c, slot 0
-                    const T d = __shfl_sync(0xffffffffu, x[0][c], c);
+                    const T d = __shfl_sync(0xffffffffu, x[c], c);
                     if (!(d > T(0))) {
                         bad = j0 + c;
                     } else {
                         const T dd = sqrt(d);
-#pragma unroll
-                        for (int s = 0; s < 4; ++s) {
-                            const int rel = lane + 32 * s;
-                            if (rel == c) x[s][c] = dd;
-                            else if (rel > c) x[s][c] = x[s][c] / dd;
-                        }
+                        if (lane == c) x[c] = dd;
+                        else if (lane > c) x[c] = x[c] / dd;
 #pragma unroll
                         for (int cc = c + 1; cc < LP; ++cc) {
-                            const T l = __shfl_sync(0xffffffffu, x[0][c], cc);  // L[j0+cc][j0+c]
-#pragma unroll
-                            for (int s = 0; s < 4; ++s) {
-                                const int rel = lane + 32 * s;
-                                if (rel >= cc) x[s][cc] -= x[s][c] * l;
-                            }
+                            const T l = __shfl_sync(0xffffffffu, x[c], cc);   // L[j0+cc][j0+c]
+                            if (lane >= cc) x[cc] -= x[c] * l;
                         }
                     }
                 }
             }
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const int r = j0 + lane + 32 * s;
-#pragma unroll
-                for (int c = 0; c < LP; ++c)
-                    if (r < bs && c < jb && r >= j0 + c) S[r * LDS + j0 + c] = x[s][c];
-            }
+            for (int c = 0; c < LP; ++c)
+                if (lane < jb && c < jb && lane >= c) S[(j0 + lane) * LDS + j0 + c] = x[c];
             if (lane == 0 && bad < bs) {
                 fail_col = bad;
                 atomicCAS(&st->info, 0, (int)(row0 + bad + 1));
@@ -92,6 +75,22 @@ __global__ void __launch_bounds__(256) k_potrf_leaf(T *A, int64_t lda, int bs, i
         }
         __syncthreads();
         if (fail_col < bs) break;
+        // (2) rows below the diagonal block: X = B L^-T, one row per thread,
+        //     L read from shared memory (the same element by all threads)
+        for (int r = j0 + jb + tid; r < bs; r += blockDim.x) {
+            T x[LP];
+#pragma unroll
+            for (int c = 0; c < LP; ++c) {
+                if (c < jb) {
+                    T v = S[r * LDS + j0 + c];
+#pragma unroll
+                    for (int p = 0; p < c; ++p) v -= x[p] * S[(j0 + c) * LDS + j0 + p];
+                    x[c] = v / S[(j0 + c) * LDS + j0 + c];
+                    S[r * LDS + j0 + c] = x[c];
+                }
+            }
+        }
+        __syncthreads();
         // rank-jb update of the trailing lower triangle, 4x4 blocks per thread
         const int t0 = j0 + jb, tr = bs - t0;
         if (tr > 0) {

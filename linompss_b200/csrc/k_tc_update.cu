@@ -10,11 +10,13 @@
 //   MODE_BF16   : P = s_blk * bf16(P / s_blk) with a power-of-two scale per
 //                 128-row block; one kind::f16 MMA, epilogue multiplies by
 //                 s_i * s_j
-// CTA tile 128 x 128, K staged 128 bytes at a time by TMA (128B swizzle, no
-// multicast), accumulator in TMEM (128 columns).  Warp roles: warp 0 lane 0
-// issues TMA, warp 1 lane 0 issues tcgen05.mma, all four warps run the
-// epilogue (tcgen05.ld -> registers -> C).  Every mbarrier wait is bounded;
-// on expiry the CTA records a timeout, drains what it issued and frees TMEM.
+// Output tiles 128 x 128, K staged 128 bytes at a time by TMA (128B swizzle,
+// no multicast), one persistent CTA per SM walking the launch's tile list,
+// two TMEM accumulators (2 x 128 columns) so the epilogue of one tile
+// overlaps the mainloop of the next.  Warp roles: warp 0 lane 0 issues TMA,
+// warp 1 lane 0 issues tcgen05.mma, warps 2..5 run the epilogue (tcgen05.ld
+// -> registers -> C).  Every mbarrier wait is bounded; on expiry the CTA
+// records a timeout, drains what it issued and frees TMEM.
 #include <cuda.h>
 
 #include "tc_sm100.cuh"
@@ -35,42 +37,73 @@ struct TcCfg {
     static constexpr int SMEM = ST * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 };
 
+// Tiles of one launch: the lower part of a (tiles_r x tiles_c) grid of 128 x 128
+// tiles whose origin is (c0, c0); tile (ti, tj) holds rows c0+128 ti.., columns
+// c0+128 tj..  It is needed when it reaches r >= c, i.e. ti >= tj (square tiles,
+// common origin).  Linear index l = ti (ti + 1) / 2 + tj over ti >= tj, limited to
+// tj < tiles_c.
+struct TileList {
+    int tiles_r, tiles_c;
+    int64_t count;
+};
+
+LNB_DEV void tile_of(const TileList &tl, int64_t l, int &ti, int &tj)
+{
+    // rows ti < tiles_c contribute ti + 1 tiles each, later rows tiles_c each
+    const int64_t tri = (int64_t)tl.tiles_c * (tl.tiles_c + 1) / 2;
+    if (l < tri) {
+        int r = (int)((sqrt(8.0 * (double)l + 1.0) - 1.0) * 0.5);
+        while ((int64_t)r * (r + 1) / 2 > l) --r;
+        while ((int64_t)(r + 1) * (r + 2) / 2 <= l) ++r;
+        ti = r;
+        tj = (int)(l - (int64_t)r * (r + 1) / 2);
+    } else {
+        const int64_t q = l - tri;
+        ti = tl.tiles_c + (int)(q / tl.tiles_c);
+        tj = (int)(q % tl.tiles_c);
+    }
+}
+
+// Persistent, warp-specialized: warp 0 = TMA producer, warp 1 = MMA issuer
+// (and TMEM owner), warps 2..5 = epilogue.  TMEM holds two 128x128 fp32
+// accumulators so the epilogue of one tile overlaps the mainloop of the next.
 template <int MODE>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(192, 1)
     k_tc_syrk_lower(const __grid_constant__ CUtensorMap tm_a, const __grid_constant__ CUtensorMap tm_b,
-                    float *C, int64_t ldc, int64_t nrows, int64_t c0, int64_t c1, int kdim,
+                    float *C, int64_t ldc, int64_t nrows, int64_t c0, int64_t c1, int kdim, TileList tl,
                     const float *scale, lnb_status_t *st, long long wait_ns)
 {
     using Cfg = TcCfg<MODE>;
     constexpr int ST = Cfg::ST;
-    const int tj = blockIdx.x, ti = blockIdx.y;
-    const int64_t rbase = c0 + (int64_t)ti * Cfg::BM, cbase = c0 + (int64_t)tj * Cfg::BN;
-    if (rbase + Cfg::BM <= cbase || rbase >= nrows || cbase >= c1) return;
-
     extern __shared__ __align__(1024) unsigned char smraw[];
     unsigned char *sm = (unsigned char *)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
     uint64_t *full = (uint64_t *)(sm + ST * Cfg::STAGE_BYTES);
     uint64_t *empty = full + ST;
-    uint64_t *accb = empty + ST;
-    uint32_t *tmem_slot = (uint32_t *)(accb + 1);
+    uint64_t *acc_full = empty + ST;      // [2]
+    uint64_t *acc_empty = acc_full + 2;   // [2]
+    uint32_t *tmem_slot = (uint32_t *)(acc_empty + 2);
     __shared__ volatile int abort_flag;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ktiles = (kdim + Cfg::BKE - 1) / Cfg::BKE;
+    const int64_t G = gridDim.x;
 
     if (tid == 0) {
         for (int s = 0; s < ST; ++s) {
             tc::mbar_init(&full[s], 1);
             tc::mbar_init(&empty[s], 1);
         }
-        tc::mbar_init(accb, 1);
+        for (int a = 0; a < 2; ++a) {
+            tc::mbar_init(&acc_full[a], 1);
+            tc::mbar_init(&acc_empty[a], 128);
+        }
         tc::fence_mbar_init();
         abort_flag = 0;
         tc::prefetch_tmap(&tm_a);
         tc::prefetch_tmap(&tm_b);
     }
-    if (warp == 0) {
-        tc::tmem_alloc(tmem_slot, 128);
+    if (warp == 1) {
+        tc::tmem_alloc(tmem_slot, 256);
         tc::tmem_relinquish();
     }
     tc::fence_before_sync();
@@ -78,99 +111,140 @@ __global__ void __launch_bounds__(128, 1)
     tc::fence_after_sync();
     const uint32_t tmem = *tmem_slot;
 
-    if (tid == 0) {
-        // ---------------- TMA producer ----------------
-        int issued = 0;
-        for (int kt = 0; kt < ktiles; ++kt) {
-            const int s = kt % ST, u = kt / ST;
-            if (kt >= ST && !tc::mbar_wait(&empty[s], (u - 1) & 1, wait_ns, &abort_flag, st)) {
-                if (!abort_flag) { abort_flag = 1; atomicCAS(&st->timeout, 0, 10); }
-                break;
-            }
-            unsigned char *base = sm + s * Cfg::STAGE_BYTES;
-            tc::mbar_arrive_expect_tx(&full[s], Cfg::STAGE_BYTES);
-            const int kx = kt * Cfg::BKE;
-            if (MODE == MODE_TF32X3) {
-                tc::tma_load_2d(base + 0 * Cfg::TILE_BYTES, &tm_a, &full[s], kx, (int)rbase);   // A hi
-                tc::tma_load_2d(base + 1 * Cfg::TILE_BYTES, &tm_b, &full[s], kx, (int)rbase);   // A lo
-                tc::tma_load_2d(base + 2 * Cfg::TILE_BYTES, &tm_a, &full[s], kx, (int)cbase);   // B hi
-                tc::tma_load_2d(base + 3 * Cfg::TILE_BYTES, &tm_b, &full[s], kx, (int)cbase);   // B lo
-            } else {
-                tc::tma_load_2d(base + 0 * Cfg::TILE_BYTES, &tm_a, &full[s], kx, (int)rbase);
-                tc::tma_load_2d(base + 1 * Cfg::TILE_BYTES, &tm_a, &full[s], kx, (int)cbase);
-            }
-            issued = kt + 1;
-        }
-        // drain: every stage load issued must land before the CTA can exit
-        for (int kt = (issued > ST ? issued - ST : 0); kt < issued; ++kt)
-            tc::mbar_wait(&full[kt % ST], (kt / ST) & 1, wait_ns, &abort_flag, st);
-    } else if (tid == 32) {
-        // ---------------- MMA issuer ----------------
-        constexpr uint32_t ID = (MODE == MODE_BF16) ? tc::idesc(1, 128, 128) : tc::idesc(2, 128, 128);
-        uint32_t accumulate = 0;
-        for (int kt = 0; kt < ktiles; ++kt) {
-            const int s = kt % ST, u = kt / ST;
-            if (!tc::mbar_wait(&full[s], u & 1, wait_ns, &abort_flag, st)) {
-                if (!abort_flag) { abort_flag = 1; atomicCAS(&st->timeout, 0, 11); }
-                break;
-            }
-            tc::fence_after_sync();
-            const uint32_t base = smem_u32(sm + s * Cfg::STAGE_BYTES);
-#pragma unroll
-            for (int kk = 0; kk < 128 / Cfg::KSTEP_BYTES; ++kk) {
-                const uint32_t off = kk * Cfg::KSTEP_BYTES;
-                if (MODE == MODE_TF32X3) {
-                    const uint64_t ahi = tc::sdesc_kmajor_sw128(base + 0 * Cfg::TILE_BYTES + off);
-                    const uint64_t alo = tc::sdesc_kmajor_sw128(base + 1 * Cfg::TILE_BYTES + off);
-                    const uint64_t bhi = tc::sdesc_kmajor_sw128(base + 2 * Cfg::TILE_BYTES + off);
-                    const uint64_t blo = tc::sdesc_kmajor_sw128(base + 3 * Cfg::TILE_BYTES + off);
-                    tc::mma_tf32(tmem, alo, bhi, ID, accumulate);
-                    tc::mma_tf32(tmem, ahi, blo, ID, 1);
-                    tc::mma_tf32(tmem, ahi, bhi, ID, 1);
-                } else {
-                    const uint64_t a = tc::sdesc_kmajor_sw128(base + 0 * Cfg::TILE_BYTES + off);
-                    const uint64_t b = tc::sdesc_kmajor_sw128(base + 1 * Cfg::TILE_BYTES + off);
-                    if (MODE == MODE_BF16) tc::mma_f16(tmem, a, b, ID, accumulate);
-                    else tc::mma_tf32(tmem, a, b, ID, accumulate);
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer ----------------
+            int64_t kt_global = 0, issued = 0;
+            for (int64_t l = blockIdx.x; l < tl.count && !abort_flag; l += G) {
+                int ti, tj;
+                tile_of(tl, l, ti, tj);
+                const int rbase = (int)(c0 + (int64_t)ti * 128), cbase = (int)(c0 + (int64_t)tj * 128);
+                for (int kt = 0; kt < ktiles; ++kt, ++kt_global) {
+                    const int s = (int)(kt_global % ST);
+                    const int64_t u = kt_global / ST;
+                    if (kt_global >= ST && !tc::mbar_wait(&empty[s], (uint32_t)((u - 1) & 1), wait_ns, &abort_flag, st)) {
+                        if (!abort_flag) { abort_flag = 1; atomicCAS(&st->timeout, 0, 10); }
+                        break;
+                    }
+                    unsigned char *base = sm + s * Cfg::STAGE_BYTES;
+                    tc::mbar_arrive_expect_tx(&full[s], Cfg::STAGE_BYTES);
+                    const int kx = kt * Cfg::BKE;
+                    if (MODE == MODE_TF32X3) {
+                        tc::tma_load_2d(base + 0 * Cfg::TILE_BYTES, &tm_a, &full[s], kx, rbase);   // A hi
+                        tc::tma_load_2d(base + 1 * Cfg::TILE_BYTES, &tm_b, &full[s], kx, rbase);   // A lo
+                        tc::tma_load_2d(base + 2 * Cfg::TILE_BYTES, &tm_a, &full[s], kx, cbase);   // B hi
+                        tc::tma_load_2d(base + 3 * Cfg::TILE_BYTES, &tm_b, &full[s], kx, cbase);   // B lo
+                    } else {
+                        tc::tma_load_2d(base + 0 * Cfg::TILE_BYTES, &tm_a, &full[s], kx, rbase);
+                        tc::tma_load_2d(base + 1 * Cfg::TILE_BYTES, &tm_a, &full[s], kx, cbase);
+                    }
+                    issued = kt_global + 1;
                 }
-                accumulate = 1;
             }
-            tc::mma_commit(&empty[s]);     // stage s free once these MMAs have read it
+            // drain: the loads still in flight must land before the CTA exits
+            for (int64_t k = (issued > ST ? issued - ST : 0); k < issued; ++k)
+                tc::mbar_wait(&full[k % ST], (uint32_t)((k / ST) & 1), wait_ns, &abort_flag, st);
         }
-        tc::mma_commit(accb);              // accumulator complete (covers every MMA issued)
-    }
-    __syncwarp();
-
-    // ---------------- epilogue: TMEM -> registers -> C ----------------
-    const bool ok = tc::mbar_wait(accb, 0, wait_ns, &abort_flag, st);
-    tc::fence_after_sync();
-    if (!ok && !abort_flag) { abort_flag = 1; atomicCAS(&st->timeout, 0, 12); }
-    // tcgen05.ld is warp-collective: the whole warp takes the same branch
-    const bool do_epi = __all_sync(0xffffffffu, ok && !abort_flag);
-    if (do_epi) {
-        const int64_t r = rbase + warp * 32 + lane;
-        float sr = 1.f;
-        if (MODE == MODE_BF16 && r < nrows) sr = scale[r >> 7];
-#pragma unroll 1
-        for (int ch = 0; ch < Cfg::BN / 32; ++ch) {
-            float v[32];
-            tc::tmem_ld_32x32b_x32(tmem + ((uint32_t)(warp * 32) << 16) + ch * 32, v);
-            if (r < nrows) {
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer ----------------
+            constexpr uint32_t ID = (MODE == MODE_BF16) ? tc::idesc(1, 128, 128) : tc::idesc(2, 128, 128);
+            int64_t kt_global = 0;
+            int lt = 0;
+            for (int64_t l = blockIdx.x; l < tl.count && !abort_flag; l += G, ++lt) {
+                const int acc = lt & 1;
+                if (lt >= 2 && !tc::mbar_wait(&acc_empty[acc], (uint32_t)(((lt >> 1) - 1) & 1), wait_ns, &abort_flag, st)) {
+                    if (!abort_flag) { abort_flag = 1; atomicCAS(&st->timeout, 0, 13); }
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t d = tmem + acc * 128;
+                uint32_t accumulate = 0;
+                for (int kt = 0; kt < ktiles; ++kt, ++kt_global) {
+                    const int s = (int)(kt_global % ST);
+                    const int64_t u = kt_global / ST;
+                    if (!tc::mbar_wait(&full[s], (uint32_t)(u & 1), wait_ns, &abort_flag, st)) {
+                        if (!abort_flag) { abort_flag = 1; atomicCAS(&st->timeout, 0, 11); }
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    const uint32_t base = smem_u32(sm + s * Cfg::STAGE_BYTES);
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int64_t c = cbase + ch * 32 + j;
-                    if (c < c1 && r >= c) {
-                        float x = v[j];
-                        if (MODE == MODE_BF16) x *= sr * scale[c >> 7];
-                        C[r + c * ldc] -= x;
+                    for (int kk = 0; kk < 128 / Cfg::KSTEP_BYTES; ++kk) {
+                        const uint32_t off = kk * Cfg::KSTEP_BYTES;
+                        if (MODE == MODE_TF32X3) {
+                            const uint64_t ahi = tc::sdesc_kmajor_sw128(base + 0 * Cfg::TILE_BYTES + off);
+                            const uint64_t alo = tc::sdesc_kmajor_sw128(base + 1 * Cfg::TILE_BYTES + off);
+                            const uint64_t bhi = tc::sdesc_kmajor_sw128(base + 2 * Cfg::TILE_BYTES + off);
+                            const uint64_t blo = tc::sdesc_kmajor_sw128(base + 3 * Cfg::TILE_BYTES + off);
+                            tc::mma_tf32(d, alo, bhi, ID, accumulate);
+                            tc::mma_tf32(d, ahi, blo, ID, 1);
+                            tc::mma_tf32(d, ahi, bhi, ID, 1);
+                        } else {
+                            const uint64_t am = tc::sdesc_kmajor_sw128(base + 0 * Cfg::TILE_BYTES + off);
+                            const uint64_t bm = tc::sdesc_kmajor_sw128(base + 1 * Cfg::TILE_BYTES + off);
+                            if (MODE == MODE_BF16) tc::mma_f16(d, am, bm, ID, accumulate);
+                            else tc::mma_tf32(d, am, bm, ID, accumulate);
+                        }
+                        accumulate = 1;
+                    }
+                    tc::mma_commit(&empty[s]);      // stage s free once these MMAs have read it
+                }
+                tc::mma_commit(&acc_full[acc]);     // accumulator acc complete
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------- epilogue warps 2..5: TMEM -> registers -> C ----------------
+        const int q = warp & 3;                     // TMEM lane quarter this warp may access
+        const int et = tid - 64;                    // 0..127
+        int lt = 0;
+        for (int64_t l = blockIdx.x; l < tl.count; l += G, ++lt) {
+            int ti, tj;
+            tile_of(tl, l, ti, tj);
+            const int acc = lt & 1;
+            const bool ok = tc::mbar_wait(&acc_full[acc], (uint32_t)((lt >> 1) & 1), wait_ns, &abort_flag, st);
+            tc::fence_after_sync();
+            if (!ok && !abort_flag) { abort_flag = 1; atomicCAS(&st->timeout, 0, 12); }
+            if (!__all_sync(0xffffffffu, ok && !abort_flag)) break;
+            const int64_t rbase = c0 + (int64_t)ti * 128, cbase = c0 + (int64_t)tj * 128;
+            const int64_t r = rbase + q * 32 + lane;
+            float sr = 1.f;
+            if (MODE == MODE_BF16 && r < nrows) sr = scale[r >> 7];
+#pragma unroll 1
+            for (int ch = 0; ch < 4; ++ch) {
+                float v[32];
+                tc::tmem_ld_32x32b_x32(tmem + acc * 128 + ((uint32_t)(q * 32) << 16) + ch * 32, v);
+                if (r < nrows) {
+                    // all 32 loads first, then the stores: loads and stores through one
+                    // pointer would otherwise be serialized into 32 memory round trips
+                    float cv[32];
+                    float *crow = C + r + (cbase + ch * 32) * ldc;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int64_t c = cbase + ch * 32 + j;
+                        cv[j] = (c < c1 && r >= c) ? crow[(int64_t)j * ldc] : 0.f;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int64_t c = cbase + ch * 32 + j;
+                        if (c < c1 && r >= c) {
+                            float x = v[j];
+                            if (MODE == MODE_BF16) x *= sr * scale[c >> 7];
+                            crow[(int64_t)j * ldc] = cv[j] - x;
+                        }
                     }
                 }
             }
+            tc::fence_before_sync();
+            tc::mbar_arrive(&acc_empty[acc]);       // 128 arrivals release the accumulator
+            (void)et;
         }
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, 128);
+    if (warp == 1) tc::tmem_dealloc(tmem, 256);
 }
 
 // ---- host: tensor maps ---------------------------------------------------------
@@ -223,25 +297,36 @@ extern "C" int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int
     int e = make_map(&ta, hi, prow, kpad, mode == MODE_BF16);
     if (!e) e = make_map(&tb, mode == MODE_TF32X3 ? lo : hi, prow, kpad, mode == MODE_BF16);
     if (e) return e;
-    dim3 grid((unsigned)((c1 - c0 + 127) / 128), (unsigned)((nrows - c0 + 127) / 128));
+    TileList tl;
+    tl.tiles_c = (int)((c1 - c0 + 127) / 128);
+    tl.tiles_r = (int)((nrows - c0 + 127) / 128);
+    {
+        const int64_t tc_ = tl.tiles_c, tr_ = tl.tiles_r;
+        const int64_t m = tc_ < tr_ ? tc_ : tr_;
+        tl.count = m * (m + 1) / 2 + (tr_ > tc_ ? (tr_ - tc_) * tc_ : 0);
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    dim3 grid((unsigned)(tl.count < sms ? tl.count : sms));
     switch (mode) {
     case MODE_TF32X3:
         cudaFuncSetAttribute(k_tc_syrk_lower<MODE_TF32X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              TcCfg<MODE_TF32X3>::SMEM);
-        k_tc_syrk_lower<MODE_TF32X3><<<grid, 128, TcCfg<MODE_TF32X3>::SMEM, s>>>(ta, tb, C, ldc, nrows, c0, c1,
-                                                                                kdim, scale, st, wait_ns);
+        k_tc_syrk_lower<MODE_TF32X3><<<grid, 192, TcCfg<MODE_TF32X3>::SMEM, s>>>(ta, tb, C, ldc, nrows, c0, c1,
+                                                                                kdim, tl, scale, st, wait_ns);
         break;
     case MODE_TF32:
         cudaFuncSetAttribute(k_tc_syrk_lower<MODE_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              TcCfg<MODE_TF32>::SMEM);
-        k_tc_syrk_lower<MODE_TF32><<<grid, 128, TcCfg<MODE_TF32>::SMEM, s>>>(ta, tb, C, ldc, nrows, c0, c1, kdim,
-                                                                            scale, st, wait_ns);
+        k_tc_syrk_lower<MODE_TF32><<<grid, 192, TcCfg<MODE_TF32>::SMEM, s>>>(ta, tb, C, ldc, nrows, c0, c1, kdim,
+                                                                            tl, scale, st, wait_ns);
         break;
     default:
         cudaFuncSetAttribute(k_tc_syrk_lower<MODE_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              TcCfg<MODE_BF16>::SMEM);
-        k_tc_syrk_lower<MODE_BF16><<<grid, 128, TcCfg<MODE_BF16>::SMEM, s>>>(ta, tb, C, ldc, nrows, c0, c1, kdim,
-                                                                            scale, st, wait_ns);
+        k_tc_syrk_lower<MODE_BF16><<<grid, 192, TcCfg<MODE_BF16>::SMEM, s>>>(ta, tb, C, ldc, nrows, c0, c1, kdim,
+                                                                            tl, scale, st, wait_ns);
         break;
     }
     lnb_prof_count(1);

@@ -101,16 +101,50 @@ LNB_DEV void tile_mma(const double *As, const double *Bs, double (&acc)[NRC / 8]
     }
 }
 
+// stage op(T)(block row oi, block col oj) as As[k][m] = op(T)[oi+m][oj+k] (zero-padded)
+template <typename TT>
+LNB_DEV void stage_tile(const TrsmArgs<TT> &a, double *As, int64_t oi, int in_, int64_t oj, int jn, int tid)
+{
+    if (!a.tT) {
+        for (int idx = tid; idx < TH * TH; idx += 128) {
+            const int k = idx / TH, m = idx % TH;
+            As[k * TLD + m] = (m < in_ && k < jn) ? (double)a.T[(oi + m) + (oj + k) * a.ldt] : 0.0;
+        }
+    } else {
+        for (int idx = tid; idx < TH * TH; idx += 128) {
+            const int m = idx / TH, k = idx % TH;     // op(T)[oi+m][oj+k] = T[oj+k][oi+m]
+            As[k * TLD + m] = (m < in_ && k < jn) ? (double)a.T[(oj + k) + (oi + m) * a.ldt] : 0.0;
+        }
+    }
+}
+
+// rhs rows [o, o+rows) x columns [r0, r0+nr) as Bs[k][cc] (k-major), zero-padded
+LNB_DEV void stage_rhs(const double *B, int64_t ldb, double *Bs, int64_t o, int rows, int64_t r0, int nr, int tid)
+{
+    for (int idx = tid; idx < TH * NRC; idx += 128) {
+        const int cc = idx / TH, k = idx % TH;
+        Bs[k * TLD + cc] = (k < rows && cc < nr) ? __ldcg(&B[(o + k) + (r0 + cc) * ldb]) : 0.0;
+    }
+}
+
+// Work items in row order of the lower block triangle (virtual rows, reversed
+// for an upper op(T)): row ii holds the off-diagonal updates U(ii, jj) for
+// jj <= ii-2, then the row item R(ii).  R(ii) absorbs the sub-diagonal update
+// U(ii, ii-1) -- the only one on the critical chain --, so the chain per
+// block is R(ii-1) -> R(ii): wait X_{ii-1}, one prefetched 64x64 tile product,
+// one prefetched inverse product, publish X_ii.  Every item waits only on
+// items with smaller tickets.
 template <typename TT>
 __global__ void __launch_bounds__(128) k_trsm_dag(TrsmArgs<TT> a)
 {
     extern __shared__ double smd[];
-    double *As = smd;              // [TH][TLD]
-    double *Bs = smd + TH * TLD;   // [TH][TLD]
+    double *As = smd;                  // [TH][TLD] tile of op(T)
+    double *Ds = smd + TH * TLD;       // [TH][TLD] inverse of the diagonal block
+    double *Bs = smd + 2 * TH * TLD;   // [TH][TLD] rhs chunk
     __shared__ int s_item, s_ok;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, g = lane >> 2, t = lane & 3;
     const int nb = a.nb;
-    const int64_t total = (int64_t)nb * (nb + 1) / 2;
+    const int64_t total = 1 + (int64_t)nb * (nb - 1) / 2;
 
     while (true) {
         if (tid == 0) s_item = atomicAdd(a.ticket, 1);
@@ -119,78 +153,85 @@ __global__ void __launch_bounds__(128) k_trsm_dag(TrsmArgs<TT> a)
         __syncthreads();
         if (item >= total) break;
 
-        // decode: virtual column jj starts at S(jj) = jj*nb - jj*(jj-1)/2
-        const double B2 = 2.0 * nb + 1.0;
-        int jj = (int)((B2 - sqrt(B2 * B2 - 8.0 * (double)item)) * 0.5);
-        if (jj < 0) jj = 0;
-        if (jj > nb - 1) jj = nb - 1;
-        while (jj > 0 && (int64_t)jj * nb - (int64_t)jj * (jj - 1) / 2 > item) --jj;
-        while (jj + 1 < nb && (int64_t)(jj + 1) * nb - (int64_t)(jj + 1) * jj / 2 <= item) ++jj;
-        const int off = (int)(item - ((int64_t)jj * nb - (int64_t)jj * (jj - 1) / 2));
-        const int j = a.fwd ? jj : nb - 1 - jj;              // column block (source)
-        const int64_t oj = (int64_t)j * TH;
-        const int jn = (int)((a.n - oj) < TH ? (a.n - oj) : TH);
+        // decode: row ii >= 1 starts at 1 + (ii-1) ii / 2
+        int ii = 0, off = 0;
+        if (item > 0) {
+            ii = (int)((1.0 + sqrt(1.0 + 8.0 * (double)(item - 1))) * 0.5);
+            if (ii < 1) ii = 1;
+            while (ii > 1 && 1 + (int64_t)(ii - 1) * ii / 2 > item) --ii;
+            while (1 + (int64_t)ii * (ii + 1) / 2 <= item) ++ii;
+            off = (int)(item - (1 + (int64_t)(ii - 1) * ii / 2));
+        }
+        const bool row_item = (ii == 0) || (off == ii - 1);
+        const int i = a.fwd ? ii : nb - 1 - ii;
+        const int64_t oi = (int64_t)i * TH;
+        const int in_ = (int)((a.n - oi) < TH ? (a.n - oi) : TH);
 
-        if (off == 0) {
-            // ---- diagonal item: X_j = inv(op(T)_jj) B_j ----
-            // inverse first (independent of the dependency)
-            const double *D = a.dinv + (int64_t)j * TH * TH;
+        if (row_item) {
+            // ---- R(ii): X_i = inv(op T_ii) (B_i - op(T)_{i,p} X_p),  p = previous block ----
+            const double *D = a.dinv + (int64_t)i * TH * TH;
             for (int idx = tid; idx < TH * TH; idx += 128) {
-                const int k = idx / TH, m = idx % TH;   // As[k][m] = inv(op T_jj)[m][k]
-                As[k * TLD + m] = a.tT ? D[k + TH * m] : D[m + TH * k];
+                const int k = idx / TH, m = idx % TH;   // Ds[k][m] = inv(op T_ii)[m][k]
+                Ds[k * TLD + m] = a.tT ? D[k + TH * m] : D[m + TH * k];
             }
+            const int p = a.fwd ? i - 1 : i + 1;
+            const int64_t op_ = (int64_t)p * TH;
+            const int pn = ii > 0 ? (int)((a.n - op_) < TH ? (a.n - op_) : TH) : 0;
+            if (ii > 0) stage_tile(a, As, oi, in_, op_, pn, tid);
             if (tid == 0) {
-                s_ok = wait_geq(&a.cnt[j], jj, a.wait_ns, a.st);
+                s_ok = wait_geq(&a.cnt[i], ii - 1, a.wait_ns, a.st);
+                if (s_ok && ii > 0) s_ok = wait_geq(&a.ready[p], 1, a.wait_ns, a.st);
                 if (!s_ok) { atomicCAS(&a.st->timeout, 0, 1); a.st->timeout_item = (int)item; }
             }
             __syncthreads();
             if (!s_ok) return;
             for (int64_t r0 = 0; r0 < a.nrhs; r0 += NRC) {
                 const int nr = (int)((a.nrhs - r0) < NRC ? (a.nrhs - r0) : NRC);
-                for (int idx = tid; idx < TH * NRC; idx += 128) {
-                    const int cc = idx / TH, k = idx % TH;   // Bs[k][cc] = B[oj+k, r0+cc]
-                    double v = 0.0;
-                    if (k < jn && cc < nr) v = __ldcg(&a.B[(oj + k) + (r0 + cc) * a.ldb]);
-                    Bs[k * TLD + cc] = v;
-                }
-                __syncthreads();
                 double acc[NRC / 8][4];
-                tile_mma(As, Bs, acc, w, g, t, (nr + 7) / 8);
+                if (ii > 0) {
+                    stage_rhs(a.B, a.ldb, Bs, op_, pn, r0, nr, tid);      // X_p
+                    __syncthreads();
+                    tile_mma(As, Bs, acc, w, g, t, (nr + 7) / 8);
+                    __syncthreads();
+                } else {
+#pragma unroll
+                    for (int ni = 0; ni < NRC / 8; ++ni)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[ni][q] = 0.0;
+                }
+                // Bs[m][cc] = B_i - acc   (m becomes k of the inverse product)
 #pragma unroll
                 for (int ni = 0; ni < NRC / 8; ++ni)
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const int m = w * 16 + g + ((q & 2) ? 8 : 0);
                         const int cc = ni * 8 + 2 * t + (q & 1);
-                        if (m < jn && cc < nr) a.B[(oj + m) + (r0 + cc) * a.ldb] = acc[ni][q];
+                        double v = 0.0;
+                        if (m < in_ && cc < nr) v = __ldcg(&a.B[(oi + m) + (r0 + cc) * a.ldb]) - acc[ni][q];
+                        Bs[m * TLD + cc] = v;
+                    }
+                __syncthreads();
+                tile_mma(Ds, Bs, acc, w, g, t, (nr + 7) / 8);
+#pragma unroll
+                for (int ni = 0; ni < NRC / 8; ++ni)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int m = w * 16 + g + ((q & 2) ? 8 : 0);
+                        const int cc = ni * 8 + 2 * t + (q & 1);
+                        if (m < in_ && cc < nr) a.B[(oi + m) + (r0 + cc) * a.ldb] = acc[ni][q];
                     }
                 __syncthreads();
             }
             __threadfence();
             __syncthreads();
-            if (tid == 0) st_release(&a.ready[j], 1);
+            if (tid == 0) st_release(&a.ready[i], 1);
         } else {
-            // ---- update item: B_i -= op(T)_ij X_j ----
-            const int ii = jj + off;
-            const int i = a.fwd ? ii : nb - 1 - ii;              // target block
-            const int64_t oi = (int64_t)i * TH;
-            const int in_ = (int)((a.n - oi) < TH ? (a.n - oi) : TH);
-            // stage op(T)_ij (rows of block i, cols of block j) as As[k][m] = op(T)[oi+m][oj+k]
-            if (!a.tT) {
-                for (int idx = tid; idx < TH * TH; idx += 128) {
-                    const int k = idx / TH, m = idx % TH;
-                    double v = 0.0;
-                    if (m < in_ && k < jn) v = (double)a.T[(oi + m) + (oj + k) * a.ldt];
-                    As[k * TLD + m] = v;
-                }
-            } else {
-                for (int idx = tid; idx < TH * TH; idx += 128) {
-                    const int m = idx / TH, k = idx % TH;  // op(T)[oi+m][oj+k] = T[oj+k][oi+m]
-                    double v = 0.0;
-                    if (m < in_ && k < jn) v = (double)a.T[(oj + k) + (oi + m) * a.ldt];
-                    As[k * TLD + m] = v;
-                }
-            }
+            // ---- U(ii, jj): B_i -= op(T)_ij X_j ----
+            const int jj = off;
+            const int j = a.fwd ? jj : nb - 1 - jj;
+            const int64_t oj = (int64_t)j * TH;
+            const int jn = (int)((a.n - oj) < TH ? (a.n - oj) : TH);
+            stage_tile(a, As, oi, in_, oj, jn, tid);
             if (tid == 0) {
                 s_ok = wait_geq(&a.ready[j], 1, a.wait_ns, a.st);
                 if (!s_ok) { atomicCAS(&a.st->timeout, 0, 2); a.st->timeout_item = (int)item; }
@@ -199,12 +240,7 @@ __global__ void __launch_bounds__(128) k_trsm_dag(TrsmArgs<TT> a)
             if (!s_ok) return;
             for (int64_t r0 = 0; r0 < a.nrhs; r0 += NRC) {
                 const int nr = (int)((a.nrhs - r0) < NRC ? (a.nrhs - r0) : NRC);
-                for (int idx = tid; idx < TH * NRC; idx += 128) {
-                    const int cc = idx / TH, k = idx % TH;
-                    double v = 0.0;
-                    if (k < jn && cc < nr) v = __ldcg(&a.B[(oj + k) + (r0 + cc) * a.ldb]);
-                    Bs[k * TLD + cc] = v;
-                }
+                stage_rhs(a.B, a.ldb, Bs, oj, jn, r0, nr, tid);
                 __syncthreads();
                 double acc[NRC / 8][4];
                 tile_mma(As, Bs, acc, w, g, t, (nr + 7) / 8);
@@ -286,10 +322,10 @@ static int trsm_left(char uplo, char trans, int64_t n, int64_t nrhs, double alph
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int64_t items = (int64_t)a.nb * (a.nb + 1) / 2;
+    const int64_t items = 1 + (int64_t)a.nb * (a.nb - 1) / 2;
     int64_t grid = (int64_t)sms * 4;
     if (grid > items) grid = items;
-    const int smem = 2 * TH * TLD * (int)sizeof(double);
+    const int smem = 3 * TH * TLD * (int)sizeof(double);
     cudaFuncSetAttribute(k_trsm_dag<TT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     k_trsm_dag<TT><<<(unsigned)grid, 128, smem, s>>>(a);
     lnb_prof_count(1);

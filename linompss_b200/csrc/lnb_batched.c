@@ -1,0 +1,95 @@
+/*
+ * lnb_batched.c -- batched uneven SPD solves (host C).
+ *
+ * One call = two launches on the caller's stream: a device-side counting sort
+ * of the systems by size (largest first) and the persistent solver
+ * (k_batched.cu).  Nothing synchronizes the host, so the call can be
+ * captured in a CUDA graph once the workspace exists (any earlier call, or
+ * lnb_batched_autotune, creates it).
+ *
+ * Autotuning: the panel width of the per-system factorization (16 or 32) is
+ * chosen per mode by lnb_batched_autotune, which times both variants on the
+ * caller's own batch and keeps the faster one for the rest of the process.
+ */
+#include <string.h>
+
+#include "lnb_host.h"
+
+size_t lnb_batched_scratch_bytes(int grid, int fp64);
+int lnb_k_batched_posv(int count, const int *n, const int *nrhs, const int64_t *a_off, const int64_t *b_off,
+                       const double *A, const double *B, double *X, void *scratch, int grid, const int *order,
+                       int *ticket, int *info, int *iters, int max_iter, int fp64, int pw, cudaStream_t s);
+int lnb_k_batch_order(int count, const int *n, int *order, cudaStream_t s);
+
+#define CK(call, where)                                            \
+    do {                                                           \
+        int _e = (int)(call);                                      \
+        if (_e != 0) return lnb_cuda_error(_e, where);             \
+    } while (0)
+
+static int g_pw[2] = {32, 32};   /* tuned panel width: [fp32 mode, fp64 mode] */
+
+static int batched_run(int count, const int *n, const int *nrhs, const int64_t *a_off, const int64_t *b_off,
+                       const double *dA, const double *dB, double *dX, int mode, int max_iter, int *info,
+                       int *iters, cudaStream_t s, int pw)
+{
+    if (count < 0) return lnb_set_error(LNB_EINVAL, "count = %d < 0", count);
+    if (count == 0) return 0;
+    if (!n || !nrhs || !a_off || !b_off || !dA || !dB || !dX) return lnb_set_error(LNB_EINVAL, "NULL argument");
+    if (mode != LNB_FACTOR_FP32 && mode != LNB_FACTOR_FP64)
+        return lnb_set_error(LNB_EINVAL, "batched: mode must be LNB_FACTOR_FP32 or LNB_FACTOR_FP64");
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const int fp64 = mode == LNB_FACTOR_FP64;
+    const int grid = c->sms;
+    const size_t sb = lnb_batched_scratch_bytes(grid, fp64);
+    void *ws = lnb_ws(c, lnb_align256(sb) + lnb_align256((size_t)count * 4) + 512);
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    void *scratch = lnb_arena_take(&ar, sb);
+    int *order = lnb_arena_take(&ar, (size_t)count * 4);
+    int *ticket = lnb_arena_take(&ar, 64);
+    if (!ticket) return lnb_set_error(LNB_ENOMEM, "batched workspace");
+    CK(lnb_k_batch_order(count, n, order, s), "order");
+    CK(lnb_k_batched_posv(count, n, nrhs, a_off, b_off, dA, dB, dX, scratch, grid, order, ticket, info, iters,
+                          max_iter > 0 ? max_iter : 10, fp64, pw, s), "batched");
+    return 0;
+}
+
+int lnb_batched_posv_dev(int count, const int *n_dev, const int *nrhs_dev, const int64_t *a_off_dev,
+                         const int64_t *b_off_dev, const double *dA, const double *dB, double *dX, int mode,
+                         int max_iter, int *info_dev, int *iters_dev, void *stream)
+{
+    return batched_run(count, n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode, max_iter, info_dev,
+                       iters_dev, (cudaStream_t)stream, g_pw[mode == LNB_FACTOR_FP64]);
+}
+
+int lnb_batched_autotune(int count, const int *n_dev, const int *nrhs_dev, const int64_t *a_off_dev,
+                         const int64_t *b_off_dev, const double *dA, const double *dB, double *dX, int mode,
+                         int max_iter, void *stream)
+{
+    cudaStream_t s = (cudaStream_t)stream;
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const int cand[2] = {16, 32};
+    float best = 1e30f;
+    int pick = 32;
+    for (int k = 0; k < 2; ++k) {
+        for (int rep = 0; rep < 2; ++rep) {   /* first run warms up */
+            CK(cudaEventRecord(c->t0, s), "event");
+            int e = batched_run(count, n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode, max_iter, NULL,
+                                NULL, s, cand[k]);
+            if (e) return e;
+            CK(cudaEventRecord(c->t1, s), "event");
+            CK(cudaEventSynchronize(c->t1), "sync");
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, c->t0, c->t1);
+            if (rep == 1 && ms < best) {
+                best = ms;
+                pick = cand[k];
+            }
+        }
+    }
+    g_pw[mode == LNB_FACTOR_FP64] = pick;
+    return pick;
+}

@@ -13,6 +13,7 @@
  * step k stays alive while the bulk update of step k runs, and step k+2's
  * copy only starts after that update (the crit stream waits on it).
  */
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -322,3 +323,91 @@ static int schol_hyper(int mt, int b, float **Ah)
 
 int ompss_schol_hrl(int mt, int b, int t, float **Ah) { (void)t; return schol_hyper(mt, b, Ah); }
 int ompss_schol_hll(int mt, int b, int t, float **Ah) { (void)t; return schol_hyper(mt, b, Ah); }
+
+/* ---- FP32 solves ---------------------------------------------------------
+ * The triangular solves with an FP32 factor compute in FP64 (k_trsv.cu reads
+ * the FP32 tiles and accumulates in double); FP32 right-hand sides are
+ * widened on the way in and rounded on the way out. */
+#define TRSV_H 64
+int lnb_k_f64_to_f32(const double *D, int64_t ldd, int64_t m, int64_t k, float *X, int64_t ldx, cudaStream_t st);
+
+static int spotrs_run(lnb_ctx *c, int64_t n, int64_t nrhs, const float *dL, int64_t lda, float *dB, int64_t ldb,
+                      char which, lnb_arena *ar, cudaStream_t s)
+{
+    const int64_t nb = (n + TRSV_H - 1) / TRSV_H;
+    double *dinv = lnb_arena_take(ar, (size_t)nb * TRSV_H * TRSV_H * 8);
+    double *Z = lnb_arena_take(ar, (size_t)n * nrhs * 8);
+    int *sync = lnb_arena_take(ar, (size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4);
+    if (!sync) return lnb_set_error(LNB_ENOMEM, "spotrs workspace");
+    CK(lnb_k_trtri_blocks_f32(dL, lda, n, TRSV_H, 'L', 0, dinv, s), "trtri");
+    CK(lnb_k_f32_to_f64(dB, ldb, n, nrhs, Z, n, s), "widen");
+    if (which == 'N' || which == 'B')
+        CK(lnb_k_trsm_left_f32('L', 'N', n, nrhs, 1.0, dL, lda, dinv, TRSV_H, Z, n, sync, c->st, lnb_wait_ns(), 0, s),
+           "forward");
+    if (which == 'T' || which == 'B')
+        CK(lnb_k_trsm_left_f32('L', 'T', n, nrhs, 1.0, dL, lda, dinv, TRSV_H, Z, n, sync, c->st, lnb_wait_ns(), 0, s),
+           "backward");
+    CK(lnb_k_f64_to_f32(Z, n, n, nrhs, dB, ldb, s), "round");
+    return 0;
+}
+
+static size_t spotrs_ws_bytes(int64_t n, int64_t nrhs)
+{
+    const int64_t nb = (n + TRSV_H - 1) / TRSV_H;
+    return lnb_align256((size_t)nb * TRSV_H * TRSV_H * 8) + lnb_align256((size_t)n * nrhs * 8) +
+           lnb_align256((size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4) + 1024;
+}
+
+int lnb_spotrs_dev(int n, int nrhs, const float *dL, int lda, float *dB, int ldb, char which, void *stream)
+{
+    if (n < 0 || nrhs < 0 || lda < (n > 1 ? n : 1) || ldb < (n > 1 ? n : 1))
+        return lnb_set_error(LNB_EINVAL, "spotrs sizes");
+    if (which != 'N' && which != 'T' && which != 'B') return lnb_set_error(LNB_EINVAL, "spotrs which");
+    if (n == 0 || nrhs == 0) return 0;
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    void *ws = lnb_ws(c, spotrs_ws_bytes(n, nrhs));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    cudaStream_t s = (cudaStream_t)stream;
+    CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
+    return spotrs_run(c, n, nrhs, dL, lda, dB, ldb, which, &ar, s);
+}
+
+/* sspdsolv_main (spdsolv_main.c:10-20 built with -DSINGLE_PRECISION) */
+int sspdsolv_main(int m, int nrhs, int b, float *A, float *B)
+{
+    if (m < 0 || nrhs < 0 || b <= 0 || b > 1024) return lnb_set_error(LNB_EINVAL, "spdsolv arguments");
+    if (m == 0) return 0;
+    if (!A || (nrhs > 0 && !B)) return lnb_set_error(LNB_EINVAL, "NULL matrix");
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const int64_t ldd = ((int64_t)m + 31) & ~(int64_t)31;
+    const size_t abytes = (size_t)ldd * m * 4, bbytes = (size_t)ldd * (nrhs ? nrhs : 1) * 4;
+    void *ws = lnb_ws(c, lnb_align256(abytes) + lnb_align256(bbytes) + lnb_chol_f32_ws_bytes(m, b, g_schol_mode) +
+                             spotrs_ws_bytes(m, nrhs ? nrhs : 1));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    float *dA = lnb_arena_take(&ar, abytes), *dB = lnb_arena_take(&ar, bbytes);
+    cudaStream_t s = c->main;
+    for (int64_t c0 = 0; c0 < m; c0 += b) {
+        const int64_t w = m - c0 < b ? m - c0 : b;
+        CK(cudaMemcpy2DAsync(dA + c0 + c0 * ldd, ldd * 4, A + c0 + c0 * (int64_t)m, (size_t)m * 4,
+                             (size_t)(m - c0) * 4, w, cudaMemcpyHostToDevice, s), "A in");
+    }
+    if (nrhs > 0)
+        CK(cudaMemcpy2DAsync(dB, ldd * 4, B, (size_t)m * 4, (size_t)m * 4, nrhs, cudaMemcpyHostToDevice, s), "B in");
+    lnb_arena ar2 = ar;
+    int e = lnb_chol_f32_run(c, m, b, dA, ldd, g_schol_mode, NULL, &ar2, s);
+    if (e) return e;
+    if (nrhs > 0) {
+        if ((e = spotrs_run(c, m, nrhs, dA, ldd, dB, ldd, 'B', &ar, s))) return e;
+        CK(cudaMemcpy2DAsync(B, (size_t)m * 4, dB, ldd * 4, (size_t)m * 4, nrhs, cudaMemcpyDeviceToHost, s), "X out");
+    }
+    for (int64_t c0 = 0; c0 < m; c0 += b) {
+        const int64_t w = m - c0 < b ? m - c0 : b;
+        CK(cudaMemcpy2DAsync(A + c0 + c0 * (int64_t)m, (size_t)m * 4, dA + c0 + c0 * ldd, ldd * 4,
+                             (size_t)(m - c0) * 4, w, cudaMemcpyDeviceToHost, s), "L out");
+    }
+    return lnb_status_read(c, s);
+}
