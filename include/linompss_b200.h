@@ -145,6 +145,21 @@ LNB_EXPORT int ompss_ditref(int n, int bm, const double *A, int lda, const doubl
  * stream. */
 LNB_EXPORT int lnb_dchol_dev(int n, int b, double *dA, int lda, int *info_dev, void *stream);
 LNB_EXPORT int lnb_schol_dev(int n, int b, float *dA, int lda, int *info_dev, void *stream);
+
+/* FP64 tile Cholesky that allocates no device memory.  No counterpart in the
+ * reference.  For callers that cannot call cudaMalloc: code whose device
+ * memory is owned by another manager (a caching allocator or a fixed arena
+ * holding the whole HBM), and code on a latency-critical path where
+ * cudaMalloc's implicit synchronization is not acceptable.
+ * Same result as lnb_dchol_dev (A = L L^T in place, lower), computed on the
+ * caller's stream only.  Its scratch (block inverses + status word) is a
+ * fixed file-scope device array of 256 KB held by every GPU that loads the
+ * library until exit; tile sizes b > 1024 are rejected with LNB_ETOOBIG.
+ * The first call on a device looks up that array's device address; make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU (other streams, other host threads) race. */
+LNB_EXPORT int lnb_dchol_noalloc_dev(int n, int b, double *dA, int lda, int *info_dev, void *stream);
+
 /* Triangular solves with the lower factor: trans 'N' solves L Y = B,
  * 'T' solves L^T X = B, 'B' (both) solves L L^T X = B.  dB: n x nrhs, ld = ldb. */
 LNB_EXPORT int lnb_dpotrs_dev(int n, int nrhs, const double *dL, int lda, double *dB, int ldb,
