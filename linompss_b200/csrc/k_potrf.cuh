@@ -74,14 +74,16 @@ __global__ void __launch_bounds__(256) k_potrf_leaf(T *A, int64_t lda, int bs, i
             }
         }
         __syncthreads();
-        if (fail_col < bs) break;
+        // after a failed pivot only the columns before it are finished, for
+        // every row of the tile (as LAPACK's column-by-column potf2 leaves them)
+        const int jv = fail_col < bs ? fail_col - j0 : jb;
         // (2) rows below the diagonal block: X = B L^-T, one row per thread,
         //     L read from shared memory (the same element by all threads)
         for (int r = j0 + jb + tid; r < bs; r += blockDim.x) {
             T x[LP];
 #pragma unroll
             for (int c = 0; c < LP; ++c) {
-                if (c < jb) {
+                if (c < jv) {
                     T v = S[r * LDS + j0 + c];
 #pragma unroll
                     for (int p = 0; p < c; ++p) v -= x[p] * S[(j0 + c) * LDS + j0 + p];
@@ -91,6 +93,7 @@ __global__ void __launch_bounds__(256) k_potrf_leaf(T *A, int64_t lda, int bs, i
             }
         }
         __syncthreads();
+        if (fail_col < bs) break;
         // rank-jb update of the trailing lower triangle, 4x4 blocks per thread
         const int t0 = j0 + jb, tr = bs - t0;
         if (tr > 0) {

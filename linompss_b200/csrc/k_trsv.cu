@@ -311,6 +311,14 @@ static int trsm_left(char uplo, char trans, int64_t n, int64_t nrhs, double alph
         e = cudaMemsetAsync(sync, ticket0 & 0xff, 1, s);  // ticket starts past item 0
         if (e != cudaSuccess) return (int)e;
     }
+    if (nrhs <= 8) {
+        if constexpr (sizeof(TT) == 8)
+            return lnb_k_trsm_chain_f64(uplo, trans, n, nrhs, (const double *)T, ldt, dinv, B, ldb, sync, st,
+                                        wait_ns, s);
+        else
+            return lnb_k_trsm_chain_f32(uplo, trans, n, nrhs, (const float *)T, ldt, dinv, B, ldb, sync, st,
+                                        wait_ns, s);
+    }
     TrsmArgs<TT> a;
     a.T = T; a.ldt = ldt; a.dinv = dinv; a.B = B; a.ldb = ldb; a.n = n; a.nrhs = nrhs;
     a.nb = (int)((n + TH - 1) / TH);

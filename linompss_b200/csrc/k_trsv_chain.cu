@@ -1,0 +1,518 @@
+// k_trsv_chain.cu -- blocked triangular solves with few right-hand sides
+// (nrhs <= 8): op(T) X = B, T triangular, FP64 arithmetic on FP64 or FP32 T.
+//
+// Semantics of bblas_dltrsm (bblas_trsm.h:116-202) and of the two solves of
+// dspdsolv_main (spdsolv_main.c:15,17), as k_trsv.cu.  With one or a few
+// right-hand sides the solve is a chain of nb = n/64 dependent diagonal
+// steps with O(n^2) independent work hanging off it, so the launch is
+// organised around the chain:
+//
+//   * one CTA (the first to draw a ticket) walks the chain.  Its 8 compute
+//     warps keep the last W solution blocks in shared memory and apply the W
+//     sub-diagonal tiles of each block row themselves, so no global-memory
+//     round trip sits between two chain steps.  The W band tiles of the next
+//     step stream in by cp.async while the current step computes, and the
+//     inverse of the next diagonal block streams into registers.
+//   * a loader warp of the same CTA waits until the far-off-diagonal updates
+//     of upcoming block rows are complete and stages those right-hand-side
+//     rows into shared memory ahead of the compute warps;
+//   * a publisher warp makes each finished solution block visible to the
+//     whole GPU (fence + release flag) off the compute warps' path;
+//   * every other CTA takes work items (row i, a chunk of CW tiles j <=
+//     i-W-1) from an atomic ticket in row order.  An item streams its tiles
+//     (double-buffered across items) before it waits for its solution blocks,
+//     then subtracts op(T)_ij X_j from B_i with atomics and bumps the row's
+//     counter.  Items of row i only wait on blocks j < i-W, which the chain
+//     produced before it needs row i, so the walk cannot deadlock.
+// Every wait is bounded and reports a site code in the status word.
+#include "common.cuh"
+#include "tc_sm100.cuh"
+
+namespace lnb {
+namespace chain {
+
+constexpr int TH = 64;              // block size
+constexpr int NCOMP = 256;          // compute threads: m = t>>2, kq = t&3
+constexpr int NTHR = NCOMP + 64;    // + publisher warp + loader warp
+constexpr int NBUF = 4;             // right-hand-side slots staged ahead
+
+// band width W handled by the chain CTA, worker chunk CW (tiles per item)
+template <typename TT> struct Cfg;
+template <> struct Cfg<float> { static constexpr int W = 4, CW = 4; };
+template <> struct Cfg<double> { static constexpr int W = 2, CW = 2; };
+
+// Padded leading dimension of a staged 64 x 64 tile S[col * LD + row].
+// TR (op = transpose) reads rows of S with 16-byte vectors, 2 columns per
+// 8-lane phase: LD == 16 words mod 32.  !TR reads 4 columns x 8 rows per
+// phase (scalar): LD == 8 floats mod 32, or 4 doubles mod 16.
+template <typename TT, bool TR> struct Ld;
+template <> struct Ld<float, true> { static constexpr int v = 80; };
+template <> struct Ld<float, false> { static constexpr int v = 72; };
+template <> struct Ld<double, true> { static constexpr int v = 72; };
+template <> struct Ld<double, false> { static constexpr int v = 68; };
+
+template <typename TT>
+struct Args {
+    const TT *T; int64_t ldt; const double *dinv;
+    double *B; int64_t ldb; int64_t n; int nrhs;
+    int nb, fwd, vec;           // vec: T and ldt allow 16-byte copies
+    int *ticket, *cnt, *ready;  // cnt/ready indexed by chain position
+    lnb_status_t *st; long long wait_ns;
+};
+
+LNB_DEV void cp_async4(void *smem, const void *gmem)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(smem)), "l"(gmem));
+}
+LNB_DEV void cp_async_el(float *d, const float *g) { cp_async4(d, g); }
+LNB_DEV void cp_async_el(double *d, const double *g) { cp_async8(d, g, true); }
+
+// named barrier over `count` threads that also ANDs a predicate
+LNB_DEV bool bar_and(int id, int count, bool pred)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id), "r"(count)
+        : "memory");
+    return r != 0;
+}
+
+template <typename TT>
+LNB_DEV int blen(const Args<TT> &a, int i)
+{
+    const int64_t o = (int64_t)i * TH;
+    return (int)((a.n - o) < TH ? (a.n - o) : TH);
+}
+// actual block index of chain position p
+template <typename TT>
+LNB_DEV int blk(const Args<TT> &a, int p) { return a.fwd ? p : a.nb - 1 - p; }
+
+// Stage the stored block holding op(T)(i, j) as S[col * LD + row], zero
+// outside the matrix; cp.async, caller commits.
+template <typename TT, bool TR>
+LNB_DEV void stage_tile(const Args<TT> &a, TT *S, int i, int j, int tid, int nthr)
+{
+    constexpr int LD = Ld<TT, TR>::v;
+    constexpr int EPC = 16 / (int)sizeof(TT);
+    constexpr int CPC = TH / EPC;
+    const int rb = TR ? j : i, cb = TR ? i : j;
+    const int rows = blen(a, rb), cols = blen(a, cb);
+    const TT *src = a.T + (int64_t)rb * TH + (int64_t)cb * TH * a.ldt;
+    for (int idx = tid; idx < TH * CPC; idx += nthr) {
+        const int col = idx / CPC, r = (idx % CPC) * EPC;
+        TT *d = S + col * LD + r;
+        const TT *g = src + r + (int64_t)col * a.ldt;
+        if (col >= cols || r >= rows) {
+            cp_async16(d, a.T, false);
+        } else if (a.vec && r + EPC <= rows) {
+            cp_async16(d, g, true);
+        } else {
+#pragma unroll
+            for (int e = 0; e < EPC; ++e) {
+                if (r + e < rows) cp_async_el(d + e, g + e);
+                else d[e] = (TT)0;
+            }
+        }
+    }
+}
+
+// part[r] += sum over this lane's 16 k of op[m][k] * X[r * 64 + k]
+template <typename TT, int NR, bool TR>
+LNB_DEV void gemv_tile(const TT *S, const double *X, int m, int kq, double (&part)[NR])
+{
+    constexpr int LD = Ld<TT, TR>::v;
+    if constexpr (TR) {
+        constexpr int EPC = 16 / (int)sizeof(TT);
+#pragma unroll
+        for (int u = 0; u < 16 / EPC; ++u) {
+            const int k0 = EPC * (kq + 4 * u);
+            TT v[EPC];
+            if constexpr (EPC == 4) {
+                const float4 q = *reinterpret_cast<const float4 *>(S + m * LD + k0);
+                v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+            } else {
+                const double2 q = *reinterpret_cast<const double2 *>(S + m * LD + k0);
+                v[0] = q.x; v[1] = q.y;
+            }
+#pragma unroll
+            for (int e = 0; e < EPC; ++e)
+#pragma unroll
+                for (int r = 0; r < NR; ++r) part[r] = fma((double)v[e], X[r * TH + k0 + e], part[r]);
+        }
+    } else {
+#pragma unroll
+        for (int v = 0; v < 16; ++v) {
+            const int k = kq + 4 * v;
+            const double t = (double)S[k * LD + m];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) part[r] = fma(t, X[r * TH + k], part[r]);
+        }
+    }
+}
+
+// k owned by lane kq for the j-th inverse element (same partition as the
+// FP64 tiles, so the reads of the staged vector are conflict-free)
+template <bool TR>
+LNB_DEV int kd(int kq, int j) { return TR ? 2 * (kq + 4 * (j >> 1)) + (j & 1) : kq + 4 * j; }
+
+// inverse of op(T) on diagonal block i, this lane's 16 entries of row m
+template <bool TR>
+LNB_DEV void load_dinv(const double *dinv, int i, int m, int kq, double (&dv)[16])
+{
+    const double *D = dinv + (int64_t)i * TH * TH;   // inv(T_ii), column-major
+    if constexpr (TR) {
+        // inv(T_ii^T)[m][k] = D[k + 64 m]
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const double2 q = __ldg(reinterpret_cast<const double2 *>(D + TH * m + 2 * (kq + 4 * u)));
+            dv[2 * u] = q.x; dv[2 * u + 1] = q.y;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) dv[j] = __ldg(D + m + TH * kd<false>(kq, j));
+    }
+}
+
+template <int NR>
+LNB_DEV void quad_sum(double (&p)[NR])
+{
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        p[r] += __shfl_xor_sync(0xffffffffu, p[r], 1);
+        p[r] += __shfl_xor_sync(0xffffffffu, p[r], 2);
+    }
+}
+
+// ---- worker items ------------------------------------------------------------
+// Row (chain position) p holds need(p) = ceil(max(0, p - W) / CW) items;
+// F(p) = sum_{q<p} need(q) = G(p - 1 - W), G(S) = sum_{s=1..S} ceil(s/CW).
+template <int W, int CW>
+LNB_DEV int64_t items_before(int p)
+{
+    const int64_t S = (int64_t)p - 1 - W;
+    if (S <= 0) return 0;
+    const int64_t q = S / CW, b = S % CW;
+    return CW * q * (q + 1) / 2 + b * (q + 1);
+}
+template <int W, int CW>
+LNB_DEV int need_of(int p) { return p > W ? (p - W + CW - 1) / CW : 0; }
+
+template <int W, int CW>
+LNB_DEV void decode(int64_t q, int nb, int &row, int &chunk)
+{
+    int lo = 0, hi = nb - 1;   // largest row with items_before(row) <= q
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items_before<W, CW>(mid) <= q) lo = mid; else hi = mid - 1;
+    }
+    row = lo;
+    chunk = (int)(q - items_before<W, CW>(lo));
+}
+
+struct ChainBars {
+    uint64_t bfull[NBUF], bempty[NBUF], xfull[2], xempty[2];
+    int abort;
+};
+
+template <typename TT, int NR, bool TR>
+__global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
+{
+    constexpr int W = Cfg<TT>::W, CW = Cfg<TT>::CW;
+    constexpr int LD = Ld<TT, TR>::v;
+    constexpr int TS = TH * LD;           // elements per staged tile
+    extern __shared__ __align__(128) unsigned char sm_raw[];
+    __shared__ int64_t s_item;
+    __shared__ int s_ok;
+    const int tid = threadIdx.x;
+    const int nb = a.nb;
+
+    if (tid == 0) s_item = atomicAdd(a.ticket, 1);
+    __syncthreads();
+    int64_t item = s_item;
+
+    if (item == 0) {
+        // ================= the chain CTA =================
+        TT *tiles = reinterpret_cast<TT *>(sm_raw);                                  // [2][W][TS]
+        double *ring = reinterpret_cast<double *>(sm_raw + sizeof(TT) * 2 * W * TS);  // [W+1][NR][64]
+        double *bbuf = ring + (W + 1) * NR * TH;                                      // [NBUF][NR][64]
+        double *accs = bbuf + NBUF * NR * TH;                                         // [NR][64]
+        ChainBars *cb = reinterpret_cast<ChainBars *>(accs + NR * TH);
+        if (tid == 0) {
+            for (int q = 0; q < NBUF; ++q) { tc::mbar_init(&cb->bfull[q], 32); tc::mbar_init(&cb->bempty[q], NCOMP); }
+            for (int q = 0; q < 2; ++q) { tc::mbar_init(&cb->xfull[q], NCOMP); tc::mbar_init(&cb->xempty[q], 1); }
+            cb->abort = 0;
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        const int warp = tid >> 5, lane = tid & 31;
+
+        if (warp == 8) {
+            // ---- publisher: X_p visible GPU-wide, then ready[p] ----
+            for (int p = 0; p < nb; ++p) {
+                bool ok = true;
+                if (lane == 0) ok = tc::mbar_wait(&cb->xfull[p & 1], (p >> 1) & 1, a.wait_ns, &cb->abort, a.st);
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) {
+                    if (lane == 0) { cb->abort = 1; atomicCAS(&a.st->timeout, 0, 4); a.st->timeout_item = p; }
+                    return;
+                }
+                if (lane == 0) {
+                    __threadfence();
+                    st_release(&a.ready[p], 1);
+                    tc::mbar_arrive(&cb->xempty[p & 1]);
+                }
+            }
+            return;
+        }
+        if (warp == 9) {
+            // ---- loader: B rows of chain position p once its items are done ----
+            for (int p = 0; p < nb; ++p) {
+                const int slot = p % NBUF;
+                bool ok = true;
+                if (lane == 0) {
+                    if (p >= NBUF)
+                        ok = tc::mbar_wait(&cb->bempty[slot], ((p / NBUF) - 1) & 1, a.wait_ns, &cb->abort, a.st);
+                    if (ok) ok = wait_geq(&a.cnt[p], need_of<W, CW>(p), a.wait_ns, a.st);
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                if (!ok) {
+                    if (lane == 0) { cb->abort = 1; atomicCAS(&a.st->timeout, 0, 5); a.st->timeout_item = p; }
+                    return;
+                }
+                const int i = blk(a, p);
+                const int64_t oi = (int64_t)i * TH;
+                const int in_ = blen(a, i);
+                double *dst = bbuf + slot * NR * TH;
+#pragma unroll
+                for (int q = 0; q < 2 * NR; ++q) {
+                    const int idx = lane + 32 * q, r = idx / TH, mm = idx % TH;
+                    dst[idx] = (mm < in_ && r < a.nrhs) ? __ldcg(a.B + (oi + mm) + (int64_t)r * a.ldb) : 0.0;
+                }
+                __syncwarp();
+                tc::mbar_arrive(&cb->bfull[slot]);
+            }
+            return;
+        }
+
+        // ---- compute warps ----
+        const int m = tid >> 2, kq = tid & 3;
+        double dA[16], dB[16];
+        load_dinv<TR>(a.dinv, blk(a, 0), m, kq, dA);
+        bool okp = true;
+        // one chain step at position p; dcur holds inv(op T_pp), dnext receives the next one
+        auto step = [&](int p, double (&dcur)[16], double (&dnext)[16]) -> bool {
+            cp_async_wait<0>();
+            if (!bar_and(1, NCOMP, okp && !*(volatile int *)&cb->abort)) return false;
+            // prefetch the band tiles of position p+1 and its inverse
+            if (p + 1 < nb) {
+                const int ip = blk(a, p + 1);
+#pragma unroll
+                for (int k = 1; k <= W; ++k)
+                    if (p + 1 - k >= 0)
+                        stage_tile<TT, TR>(a, tiles + ((p + 1) & 1) * W * TS + (k - 1) * TS, ip, blk(a, p + 1 - k),
+                                           tid, NCOMP);
+                load_dinv<TR>(a.dinv, ip, m, kq, dnext);
+            }
+            cp_async_commit();
+            // band: sum_k op(T)(i, i-k) X_{p-k}
+            double part[NR];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) part[r] = 0.0;
+#pragma unroll
+            for (int k = 1; k <= W; ++k)
+                if (p - k >= 0)
+                    gemv_tile<TT, NR, TR>(tiles + (p & 1) * W * TS + (k - 1) * TS, ring + ((p - k) % (W + 1)) * NR * TH,
+                                          m, kq, part);
+            quad_sum<NR>(part);
+            const int slot = p % NBUF;
+            const bool okb = tc::mbar_wait(&cb->bfull[slot], (p / NBUF) & 1, a.wait_ns, &cb->abort, a.st);
+            if (okb) {
+                const double *bs = bbuf + slot * NR * TH;
+#pragma unroll
+                for (int r = 0; r < NR; ++r)
+                    if ((r & 3) == kq) accs[r * TH + m] = bs[r * TH + m] - part[r];
+            }
+            tc::mbar_arrive(&cb->bempty[slot]);
+            if (!bar_and(1, NCOMP, okb)) return false;
+            // X_p = inv(op T_pp) acc
+            double xs[NR];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) xs[r] = 0.0;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int k = kd<TR>(kq, j);
+#pragma unroll
+                for (int r = 0; r < NR; ++r) xs[r] = fma(dcur[j], accs[r * TH + k], xs[r]);
+            }
+            quad_sum<NR>(xs);
+            const int i = blk(a, p);
+            const int64_t oi = (int64_t)i * TH;
+            const int in_ = blen(a, i);
+            double *xr = ring + (p % (W + 1)) * NR * TH;
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if ((r & 3) == kq) {
+                    xr[r * TH + m] = xs[r];
+                    if (m < in_ && r < a.nrhs) a.B[(oi + m) + (int64_t)r * a.ldb] = xs[r];
+                }
+            okp = true;
+            if (p >= 2) okp = tc::mbar_wait(&cb->xempty[p & 1], ((p >> 1) - 1) & 1, a.wait_ns, &cb->abort, a.st);
+            tc::mbar_arrive(&cb->xfull[p & 1]);
+            return true;
+        };
+        for (int p = 0; p < nb; p += 2) {
+            bool ok = step(p, dA, dB);
+            if (ok && p + 1 < nb) ok = step(p + 1, dB, dA);
+            if (!ok) {
+                cp_async_wait<0>();
+                if (tid == 0) { cb->abort = 1; atomicCAS(&a.st->timeout, 0, 3); a.st->timeout_item = p; }
+                return;
+            }
+        }
+        cp_async_wait<0>();
+        return;
+    }
+
+    // ================= worker CTAs =================
+    TT *wbuf = reinterpret_cast<TT *>(sm_raw);                                     // [2][CW][TS]
+    double *xw = reinterpret_cast<double *>(sm_raw + sizeof(TT) * 2 * CW * TS);    // [CW][NR][64]
+    const int64_t total = 1 + items_before<W, CW>(nb);
+    const int m = tid >> 2, kq = tid & 3;
+    int buf = 0;
+    int row = 0, chunk = 0;
+    if (item < total) {
+        decode<W, CW>(item - 1, nb, row, chunk);
+        const int j0 = chunk * CW, j1 = min(j0 + CW, row - W);
+        for (int jj = j0; jj < j1; ++jj)
+            stage_tile<TT, TR>(a, wbuf + (jj - j0) * TS, blk(a, row), blk(a, jj), tid, NTHR);
+    }
+    cp_async_commit();
+    while (item < total) {
+        __syncthreads();
+        if (tid == 0) s_item = atomicAdd(a.ticket, 1);
+        __syncthreads();
+        const int64_t next = s_item;
+        int nrow = 0, nchunk = 0;
+        if (next < total) {
+            decode<W, CW>(next - 1, nb, nrow, nchunk);
+            const int j0 = nchunk * CW, j1 = min(j0 + CW, nrow - W);
+            for (int jj = j0; jj < j1; ++jj)
+                stage_tile<TT, TR>(a, wbuf + (buf ^ 1) * CW * TS + (jj - j0) * TS, blk(a, nrow), blk(a, jj), tid,
+                                   NTHR);
+        }
+        cp_async_commit();
+        const int j0 = chunk * CW, j1 = min(j0 + CW, row - W);
+        if (tid == 0) {
+            s_ok = wait_geq(&a.ready[j1 - 1], 1, a.wait_ns, a.st);
+            if (!s_ok) { atomicCAS(&a.st->timeout, 0, 6); a.st->timeout_item = (int)item; }
+        }
+        __syncthreads();
+        if (!s_ok) { cp_async_wait<0>(); return; }
+        for (int idx = tid; idx < (j1 - j0) * NR * TH; idx += NTHR) {
+            const int t = idx / (NR * TH), r = (idx / TH) % NR, k = idx % TH;
+            const int j = blk(a, j0 + t);
+            const int64_t oj = (int64_t)j * TH;
+            xw[idx] = (k < blen(a, j) && r < a.nrhs) ? __ldcg(a.B + (oj + k) + (int64_t)r * a.ldb) : 0.0;
+        }
+        cp_async_wait<1>();
+        __syncthreads();
+        if (tid < NCOMP) {
+            double part[NR];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) part[r] = 0.0;
+            for (int jj = j0; jj < j1; ++jj)
+                gemv_tile<TT, NR, TR>(wbuf + buf * CW * TS + (jj - j0) * TS, xw + (jj - j0) * NR * TH, m, kq, part);
+            quad_sum<NR>(part);
+            const int i = blk(a, row);
+            const int64_t oi = (int64_t)i * TH;
+            const int in_ = blen(a, i);
+#pragma unroll
+            for (int r = 0; r < NR; ++r)
+                if ((r & 3) == kq && m < in_ && r < a.nrhs)
+                    atomicAdd(a.B + (oi + m) + (int64_t)r * a.ldb, -part[r]);
+            __threadfence();
+        }
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicAdd(&a.cnt[row], 1);
+        }
+        item = next; row = nrow; chunk = nchunk; buf ^= 1;
+    }
+    cp_async_wait<0>();
+}
+
+template <typename TT, int NR, bool TR>
+constexpr size_t smem_bytes()
+{
+    constexpr int W = Cfg<TT>::W, CW = Cfg<TT>::CW;
+    constexpr size_t TSB = sizeof(TT) * TH * Ld<TT, TR>::v;
+    constexpr size_t chainb = 2 * W * TSB + sizeof(double) * ((W + 1) + NBUF + 1) * NR * TH + sizeof(ChainBars);
+    constexpr size_t workb = 2 * CW * TSB + sizeof(double) * CW * NR * TH;
+    return chainb > workb ? chainb : workb;
+}
+
+template <typename TT, int NR, bool TR>
+int launch(const Args<TT> &a, lnb_stream_t s)
+{
+    constexpr int W = Cfg<TT>::W, CW = Cfg<TT>::CW;
+    constexpr size_t smem = smem_bytes<TT, NR, TR>();
+    static_assert(smem <= 227 * 1024, "chain solve shared memory");
+    cudaError_t e = cudaFuncSetAttribute(k_trsm_chain<TT, NR, TR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // worker items: G(nb - 1 - W)
+    int64_t S = (int64_t)a.nb - 1 - W, witems = 0;
+    if (S > 0) witems = CW * (S / CW) * (S / CW + 1) / 2 + (S % CW) * (S / CW + 1);
+    int64_t grid = 1 + witems;
+    if (grid > sms) grid = sms;
+    k_trsm_chain<TT, NR, TR><<<(unsigned)grid, NTHR, smem, s>>>(a);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+
+template <typename TT>
+int trsm_chain(char uplo, char trans, int64_t n, int64_t nrhs, const TT *T, int64_t ldt, const double *dinv,
+               double *B, int64_t ldb, int *sync, lnb_status_t *st, long long wait_ns, lnb_stream_t s)
+{
+    Args<TT> a;
+    a.T = T; a.ldt = ldt; a.dinv = dinv; a.B = B; a.ldb = ldb; a.n = n; a.nrhs = (int)nrhs;
+    a.nb = (int)((n + TH - 1) / TH);
+    const bool lowerop = (uplo == 'L') == (trans == 'N');
+    a.fwd = lowerop ? 1 : 0;
+    a.vec = ((uintptr_t)T % 16 == 0) && ((ldt * (int64_t)sizeof(TT)) % 16 == 0);
+    a.ticket = sync; a.cnt = sync + 4; a.ready = sync + 4 + a.nb;
+    a.st = st; a.wait_ns = wait_ns;
+    const bool tr = trans == 'T';
+    if (nrhs <= 1) return tr ? launch<TT, 1, true>(a, s) : launch<TT, 1, false>(a, s);
+    if (nrhs <= 2) return tr ? launch<TT, 2, true>(a, s) : launch<TT, 2, false>(a, s);
+    if (nrhs <= 4) return tr ? launch<TT, 4, true>(a, s) : launch<TT, 4, false>(a, s);
+    return tr ? launch<TT, 8, true>(a, s) : launch<TT, 8, false>(a, s);
+}
+
+}  // namespace chain
+}  // namespace lnb
+
+// sync must hold lnb_trsm_sync_ints(n, 64) zeroed ints (ticket first).
+extern "C" int lnb_k_trsm_chain_f64(char uplo, char trans, int64_t n, int64_t nrhs, const double *T, int64_t ldt,
+                                    const double *dinv, double *B, int64_t ldb, int *sync, lnb_status_t *st,
+                                    long long wait_ns, lnb_stream_t s)
+{
+    if (nrhs > 8) return (int)cudaErrorInvalidValue;
+    return lnb::chain::trsm_chain<double>(uplo, trans, n, nrhs, T, ldt, dinv, B, ldb, sync, st, wait_ns, s);
+}
+extern "C" int lnb_k_trsm_chain_f32(char uplo, char trans, int64_t n, int64_t nrhs, const float *T, int64_t ldt,
+                                    const double *dinv, double *B, int64_t ldb, int *sync, lnb_status_t *st,
+                                    long long wait_ns, lnb_stream_t s)
+{
+    if (nrhs > 8) return (int)cudaErrorInvalidValue;
+    return lnb::chain::trsm_chain<float>(uplo, trans, n, nrhs, T, ldt, dinv, B, ldb, sync, st, wait_ns, s);
+}

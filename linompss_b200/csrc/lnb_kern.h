@@ -69,6 +69,16 @@ int lnb_k_trsm_left_f64(char uplo, char trans, int64_t n, int64_t nrhs, double a
                         int64_t ldb, int *sync, lnb_status_t *st, long long wait_ns,
                         int ticket0, lnb_stream_t s);
 
+/* Few right-hand sides (nrhs <= 8): the same solve as one launch built
+ * around the diagonal chain (k_trsv_chain.cu).  sync as above, zeroed by the
+ * caller; alpha already applied. */
+int lnb_k_trsm_chain_f64(char uplo, char trans, int64_t n, int64_t nrhs, const double *T, int64_t ldt,
+                         const double *dinv, double *B, int64_t ldb, int *sync, lnb_status_t *st,
+                         long long wait_ns, lnb_stream_t s);
+int lnb_k_trsm_chain_f32(char uplo, char trans, int64_t n, int64_t nrhs, const float *T, int64_t ldt,
+                         const double *dinv, double *B, int64_t ldb, int *sync, lnb_status_t *st,
+                         long long wait_ns, lnb_stream_t s);
+
 /* ---- FP32-storage factorization kernels (k_chol_f32.cu) ------------------ */
 int lnb_k_potrf_f32(float *A, int64_t lda, int bs, int64_t row0, float *dinv, lnb_status_t *st,
                     lnb_stream_t s);

@@ -51,12 +51,12 @@ int lnb_trsm_f64_run(lnb_ctx *c, char uplo, char trans, char diag, int64_t n, in
 
 int lnb_selftest_wait_timeout(long long wait_us)
 {
-    /* 128 x 128 identity, 1 rhs: two diagonal items and one update item.  The
-     * ticket starts at 1, so diagonal item 0 never runs and both remaining
-     * items wait on a flag that nothing sets. */
+    /* 1024 x 1024 identity, 1 rhs.  The ticket starts at 1, so no CTA walks
+     * the diagonal chain, and the off-band update items wait on solution
+     * blocks that nothing publishes. */
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
-    const int64_t n = 128;
+    const int64_t n = 1024;
     void *ws = lnb_ws(c, lnb_align256(n * n * 8) + lnb_align256(n * 8) + lnb_trsm_f64_ws_bytes(n));
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};

@@ -109,3 +109,25 @@ def test_schol_not_spd(lnb, mode):
     A0[300, 300] = -5.0
     A = np.asfortranarray(A0.copy())
     assert lnb.ompss_schol_rl(n, b, b, A, n) == 301
+
+
+@pytest.mark.parametrize("n,nrhs", [(3001, 1), (3001, 8), (4096, 2)])
+def test_spotrs_chain_matches_fp64_solve(lnb, cuda, n, nrhs):
+    """FP32-stored factor, FP64 right-hand sides and arithmetic: the solve
+    equals an FP64 triangular solve with the same (FP32-valued) factor."""
+    import torch
+    rng = np.random.default_rng(n + nrhs)
+    L = np.tril(rng.uniform(-1, 1, (n, n)) / np.sqrt(n)).astype(np.float32)
+    L[np.diag_indices(n)] = (2.0 + rng.uniform(0, 1, n)).astype(np.float32)
+    B0 = rng.standard_normal((n, nrhs))
+    Lt = torch.tensor(np.ascontiguousarray(L.T), device=cuda)
+    Bt = torch.tensor(np.ascontiguousarray(B0.T).astype(np.float32), device=cuda)
+    lnb.spotrs_dev(Lt, Bt, n, nrhs, "B")
+    torch.cuda.synchronize()
+    L64 = L.astype(np.float64)
+    import scipy.linalg as sl
+    Y = sl.solve_triangular(L64, B0.astype(np.float32).astype(np.float64), lower=True)
+    X = sl.solve_triangular(L64.T, Y, lower=False)
+    got = Bt.cpu().numpy().T.astype(np.float64)
+    # the device result is rounded to FP32 on the way out
+    np.testing.assert_allclose(got, X, rtol=0, atol=2e-7 * np.abs(X).max())

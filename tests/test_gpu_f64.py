@@ -159,6 +159,20 @@ def test_dtrsm_vs_oracle_ragged(lnb, uplo, trans, diag):
     np.testing.assert_allclose(B1, B2, rtol=1e-13, atol=1e-15)
 
 
+@pytest.mark.parametrize("uplo,trans,diag", [("L", "N", "N"), ("L", "T", "N"), ("U", "N", "U"), ("U", "T", "N")])
+@pytest.mark.parametrize("m,n", [(64, 1), (65, 2), (700, 3), (2500, 1), (2500, 8), (1999, 5)])
+def test_dtrsm_few_rhs_vs_oracle(lnb, uplo, trans, diag, m, n):
+    """1..8 right-hand sides take the diagonal-chain launch: every band width
+    and worker-item shape, ragged last block, all four triangle/transpose cases."""
+    rng = np.random.default_rng(m + 7 * n)
+    T = np.asfortranarray(rng.uniform(-1, 1, (m, m)) / np.sqrt(m) + (1.0 if diag == "U" else 3.0) * np.eye(m))
+    B0 = np.asfortranarray(rng.uniform(-1, 1, (m, n)))
+    B1, B2 = B0.copy(order="F"), B0.copy(order="F")
+    lnb.ompss_dtrsm("L", uplo, trans, diag, m, n, 64, 1.0, T, m, B1, m)
+    O.ltrsm(uplo, trans, diag, 64, 1.0, T, B2)
+    np.testing.assert_allclose(B1, B2, rtol=1e-12, atol=1e-13 * np.abs(B2).max())
+
+
 # ---------------------------------------------------------------- tile tasks
 def test_task_potrf_lower_and_upper(lnb):
     n = 150
