@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true", help="skip the plain-FP64 comparison (mixed/bf16)")
+    p.add_argument("--no-batched", action="store_true", help="skip the batched uneven-systems measurement")
+    p.add_argument("--batch-count", type=int, default=10000)
     a = p.parse_args()
     w = dict(WORKLOADS[a.workload])
     for k in ("n", "b", "nrhs"):
@@ -318,6 +320,123 @@ def traffic_from_profiles(kernel, alg_bytes_per_launch):
     return int(ratio * alg_bytes_per_launch)
 
 
+def make_batch(count, seed, device):
+    """`count` systems, n_i ~ U{16..512}, nrhs_i ~ U{1..8}, A_i = G G^T/n_i + 1e-2 I,
+    packed column-major in one flat FP64 buffer (and B_i ~ N(0,1) likewise)."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(16, 513, count)
+    rs = rng.integers(1, 9, count)
+    a_off = np.concatenate([[0], np.cumsum(ns.astype(np.int64) ** 2)[:-1]])
+    b_off = np.concatenate([[0], np.cumsum(ns.astype(np.int64) * rs)[:-1]])
+    A = torch.empty(int((ns.astype(np.int64) ** 2).sum()), dtype=torch.float64, device=device)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    for n in np.unique(ns):
+        idx = np.nonzero(ns == n)[0]
+        G = torch.randn(len(idx), n, n, dtype=torch.float64, device=device, generator=g)
+        Ai = torch.bmm(G, G.transpose(1, 2)).div_(float(n))
+        Ai.diagonal(dim1=1, dim2=2).add_(1e-2)
+        flat = (torch.tensor(a_off[idx], device=device)[:, None] +
+                torch.arange(n * n, device=device)[None, :]).reshape(-1)
+        A.index_copy_(0, flat, Ai.reshape(-1))          # symmetric: row- and column-major agree
+        del G, Ai, flat
+    B = torch.randn(int((ns.astype(np.int64) * rs).sum()), dtype=torch.float64, device=device, generator=g)
+    t = lambda x, dt: torch.tensor(x, dtype=dt, device=device)
+    return (ns, rs, a_off, b_off, t(ns, torch.int32), t(rs, torch.int32), t(a_off, torch.int64),
+            t(b_off, torch.int64), A, B)
+
+
+def batched_arm(args, world, local, peaks):
+    """Batched uneven solves: one persistent launch (autotuned panel width,
+    captured in a CUDA graph) against a loop of per-system plain FP64 solves."""
+    import numpy as np
+    import torch
+
+    import linompss_b200 as lnb
+    dev = torch.device("cuda", local)
+    L = lnb.lib()
+    count = args.batch_count
+    ns, rs, a_off, b_off, nd, rd, ao, bo, dA, dB = make_batch(count, 4321 + local, dev)
+    flops = float(sum(n ** 3 / 3.0 + 2.0 * n * n * r for n, r in zip(ns.astype(float), rs.astype(float))))
+    dX = torch.zeros_like(dB)
+    info = torch.zeros(count, dtype=torch.int32, device=dev)
+    iters = torch.zeros(count, dtype=torch.int32, device=dev)
+    s = torch.cuda.Stream(device=dev)
+    with torch.cuda.stream(s):
+        pw = lnb.batched_autotune(nd, rd, ao, bo, dA, dB, dX, lnb.FACTOR_FP32, 10, stream=s)
+        lnb.batched_posv_dev(nd, rd, ao, bo, dA, dB, dX, lnb.FACTOR_FP32, 10, info, iters, stream=s)
+        torch.cuda.synchronize()
+        gr = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(gr, stream=s):
+            lnb.batched_posv_dev(nd, rd, ao, bo, dA, dB, dX, lnb.FACTOR_FP32, 10, info, iters, stream=s)
+        for _ in range(2):
+            gr.replay()
+        torch.cuda.synchronize()
+        reps = max(3, min(args.steps, 10))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        dX.zero_()
+        e0.record(s)
+        for _ in range(reps):
+            gr.replay()
+        e1.record(s)
+        torch.cuda.synchronize()
+    t_batch = allmax(world, e0.elapsed_time(e1) / reps)
+    assert int((info != 0).sum().item()) == 0, "batched: non-SPD report"
+    # backward error of a sample of systems, FP64 on the device
+    eps = np.finfo(float).eps / 2
+    worst = 0.0
+    for k in np.linspace(0, count - 1, 64).astype(int):
+        n, r = int(ns[k]), int(rs[k])
+        Ak = dA[a_off[k]:a_off[k] + n * n].view(n, n)
+        Xk = dX[b_off[k]:b_off[k] + n * r].view(r, n).t()
+        Bk = dB[b_off[k]:b_off[k] + n * r].view(r, n).t()
+        R = Bk - Ak @ Xk
+        be = (R.abs().max() / (Ak.abs().sum(1).max() * Xk.abs().max() + Bk.abs().max())).item()
+        worst = max(worst, be / (n * eps))
+    assert worst <= 10.0, f"batched backward error {worst} n eps"
+    it = iters.cpu().numpy()
+    del gr
+    # per-system plain FP64 launches on a copy (dposv factors A in place)
+    Aw = dA.clone()
+    Bw = dB.clone()
+    infop = torch.zeros(1, dtype=torch.int32, device=dev)
+    f = L.lnb_dposv_dev
+    f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+    pa, pb, sp = Aw.data_ptr(), Bw.data_ptr(), C.c_void_p(s.cuda_stream)
+    with torch.cuda.stream(s):
+        for k in range(min(count, 50)):     # warm-up: workspace and first-launch costs
+            n, r = int(ns[k]), int(rs[k])
+            f(n, r, 128, C.c_void_p(pa + 8 * int(a_off[k])), n, C.c_void_p(pb + 8 * int(b_off[k])), n,
+              C.c_void_p(infop.data_ptr()), sp)
+        Aw.copy_(dA)
+        Bw.copy_(dB)
+        torch.cuda.synchronize()
+        e0.record(s)
+        for k in range(count):
+            n, r = int(ns[k]), int(rs[k])
+            rc = f(n, r, 128, C.c_void_p(pa + 8 * int(a_off[k])), n, C.c_void_p(pb + 8 * int(b_off[k])), n,
+                   C.c_void_p(infop.data_ptr()), sp)
+            assert rc == 0, lnb.last_error()
+        e1.record(s)
+        torch.cuda.synchronize()
+    t_loop = allmax(world, e0.elapsed_time(e1))
+    del Aw, Bw, dA, dB, dX
+    torch.cuda.empty_cache()
+    tf = world * flops / (t_batch * 1e-3) / 1e12
+    return {"systems": count, "n_range": [16, 512], "nrhs_range": [1, 8], "factor": "fp32 + fp64 refinement",
+            "ms_per_batch": round(t_batch, 3), "value": round(tf, 4), "unit": UNIT,
+            "solves_per_s": round(world * count / (t_batch * 1e-3), 1),
+            "frac_of_fp64_dgemm_peak": round(tf / peaks["fp64"], 4),
+            "frac_of_tf32_peak": round(tf / peaks["tf32"], 4),
+            "per_system_loop_ms": round(t_loop, 3), "speedup_vs_per_system_launches": round(t_loop / t_batch, 2),
+            "per_system_loop": "lnb_dposv_dev (plain FP64, b=128) once per system, same stream",
+            "launch": "one persistent launch in a CUDA graph, replayed", "panel_width": pw,
+            "max_backward_error_over_n_eps_sample64": round(worst, 4),
+            "refinement_iterations": {"min": int(it.min()), "max": int(it.max()), "mean": round(float(it.mean()), 2)}}
+
+
 def ours_arm(args, world, rank, local):
     import numpy as np
     import torch
@@ -448,8 +567,11 @@ def ours_arm(args, world, rank, local):
                 tp.append(e0.elapsed_time(e1))
         plain_ms = allmax(world, statistics.mean(tp))
         bwp = backward_error_dev(A0, Bp, B0)
+        # forward error of the mixed solution against the plain FP64 one
+        fwd = ((X - Bp).abs().max() / Bp.abs().max()).item()
         line["fp64_plain"] = {"ms_per_step": round(plain_ms, 3), "value": round(world * fl / plain_ms / 1e9, 4),
-                              "backward_error": bwp, "speedup_mixed_vs_plain": round(plain_ms / ms_step, 3)}
+                              "backward_error": bwp, "speedup_mixed_vs_plain": round(plain_ms / ms_step, 3),
+                              "forward_error_mixed_vs_plain": fwd}
         del Ap, Bp
         torch.cuda.empty_cache()
 
@@ -499,6 +621,8 @@ def ours_arm(args, world, rank, local):
         line["e2e"] = {"value": round(world * fl / e2e_sec / 1e12, 4), "unit": UNIT, "h2d_bytes_per_step": h2d,
                        "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_sec * 1e3, 3), "api": api}
     line["clocks"] = clk.summary()
+    if not args.no_batched:
+        line["batched"] = batched_arm(args, world, local, peaks)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ns = min(n, 8192)

@@ -4,8 +4,9 @@
 // tasks_trsm.c, tasks_syrk.c, task_gemm.c built with -DSINGLE_PRECISION).
 //
 //   potrf   : leaf diagonal tile in shared memory (k_potrf.cuh)
-//   trsm    : panel solve B <- B L^-T, SIMT, left-looking over 32-column blocks
-//             with the leaf's inverted 32x32 diagonal blocks
+//   trsm    : panel solve B <- B L^-T, SIMT, rows resident in shared memory,
+//             left-looking over 32-column blocks with the leaf's 32x32 inverses;
+//             optionally writes the TF32 operand copies of the result
 //   syrk    : SIMT lower-triangle update (nested diagonal tiles; plain FP32 mode)
 //   prep    : column-major panel -> K-major operand copies for the tensor-core
 //             update: TF32 hi/lo split (x = hi + lo, hi = rna_tf32(x)), or BF16
@@ -19,74 +20,193 @@
 
 namespace lnb {
 
-// ------------------------------------------------------------------------
-// panel solve, FP32 SIMT: CTA = 64 rows, 256 threads (row r = tid%64, column
-// group cg = tid/64 of 8 columns inside each 32-column block)
-// ------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_trsm_rlt_f32(const float *__restrict__ L, int64_t lda,
-                                                      const float *__restrict__ dinv, float *B, int64_t ldb,
-                                                      int64_t m, int bs)
+LNB_DEV float tf32_rna(float x)
 {
-    __shared__ float Xs[64][33];
-    __shared__ float Ls[32][33];
-    __shared__ float Ts[64][33];
-    const int tid = threadIdx.x, r = tid & 63, cg = tid >> 6;
-    const int64_t rbase = (int64_t)blockIdx.x * 64;
-    const int64_t grow = rbase + r;
-    const int nblk = (bs + 31) / 32;
-    for (int jb = 0; jb < nblk; ++jb) {
-        const int jc = jb * 32;
-        float acc[8];
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return __uint_as_float(r);
+}
+
+// ------------------------------------------------------------------------
+// panel solve X = B L^-T, FP32 SIMT.  One CTA owns 32 rows of the panel and
+// keeps them (B, then X) in shared memory for the whole solve; L streams in
+// 32 x 32 blocks by cp.async, double-buffered (all CTAs read the same L, so
+// it is served from L2).  Left-looking over 32-column blocks j:
+//     acc = B_j - sum_{kc<j} X_kc L_{j,kc}^T ;   X_j = acc Dinv_j^T
+// with Dinv_j the leaf's inverse of the j-th 32 x 32 diagonal block.
+// 64 threads, 4 rows x 4 columns of each block per thread (16-byte shared loads).
+// ------------------------------------------------------------------------
+namespace ptrsm {
+constexpr int LDB = 36;   // padded row of the L / Dinv / T staging blocks
+constexpr int NT = 64;    // threads per CTA
+}
+
+LNB_DEV void ptrsm_stage_L(float *dst, const float *L, int64_t lda, int bs, int j, int kc, bool vec, int tid)
+{
+    for (int idx = tid; idx < 32 * 8; idx += ptrsm::NT) {
+        const int k = idx >> 3, c4 = (idx & 7) * 4;   // dst[k][c] = L[32 j + c][32 kc + k]
+        float *d = dst + k * ptrsm::LDB + c4;
+        const int row = 32 * j + c4;
+        const float *g = L + row + (int64_t)(32 * kc + k) * lda;
+        if (vec && row + 4 <= bs) {
+            cp_async16(d, g, true);
+        } else {
 #pragma unroll
-        for (int c = 0; c < 8; ++c) acc[c] = 0.f;
-        for (int kc = 0; kc < jc; kc += 32) {
-            for (int idx = tid; idx < 64 * 32; idx += 256) {
-                const int k = idx >> 6, rr = idx & 63;
-                const int64_t gr = rbase + rr;
-                Xs[rr][k] = gr < m ? __ldcg(&B[gr + (int64_t)(kc + k) * ldb]) : 0.f;
+            for (int e = 0; e < 4; ++e) {
+                if (row + e < bs) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(d + e)),
+                                               "l"(g + e));
+                else d[e] = 0.f;
             }
-            for (int idx = tid; idx < 32 * 32; idx += 256) {
-                const int k = idx >> 5, c = idx & 31;
-                Ls[c][k] = (jc + c < bs) ? L[(jc + c) + (int64_t)(kc + k) * lda] : 0.f;
-            }
-            __syncthreads();
-#pragma unroll 8
-            for (int k = 0; k < 32; ++k) {
-                const float x = Xs[r][k];
-#pragma unroll
-                for (int c = 0; c < 8; ++c) acc[c] = fmaf(x, Ls[cg * 8 + c][k], acc[c]);
-            }
-            __syncthreads();
         }
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int col = jc + cg * 8 + c;
-            float v = 0.f;
-            if (grow < m && col < bs) v = B[grow + (int64_t)col * ldb] - acc[c];
-            Ts[r][cg * 8 + c] = v;
-        }
-        for (int idx = tid; idx < 32 * 32; idx += 256) {
-            const int rr = idx & 31, k = idx >> 5;  // Ls[c][k] = Dinv(c, k)
-            Ls[rr][k] = dinv[(int64_t)jb * 1024 + rr + 32 * k];
-        }
-        __syncthreads();
-        float y[8];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) y[c] = 0.f;
-#pragma unroll 8
-        for (int k = 0; k < 32; ++k) {
-            const float tv = Ts[r][k];
-#pragma unroll
-            for (int c = 0; c < 8; ++c) y[c] = fmaf(tv, Ls[cg * 8 + c][k], y[c]);
-        }
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const int col = jc + cg * 8 + c;
-            if (grow < m && col < bs) B[grow + (int64_t)col * ldb] = y[c];
-        }
-        __threadfence_block();
-        __syncthreads();
     }
+}
+LNB_DEV void ptrsm_stage_D(float *dst, const float *dinv, int j, int tid)
+{
+    for (int idx = tid; idx < 32 * 8; idx += ptrsm::NT) {
+        const int q = idx >> 3, c4 = (idx & 7) * 4;   // dst[q][c] = Dinv_j[c][q] = dinv[j][c + 32 q]
+        cp_async16(dst + q * ptrsm::LDB + c4, dinv + (int64_t)j * 1024 + c4 + 32 * q, true);
+    }
+}
+
+// 4x4 outer-product accumulate of two 16-byte vectors, acc += sgn x l^T
+LNB_DEV void fma4x4(float (&acc)[4][4], const float4 x, const float4 l, float sgn)
+{
+    const float xv[4] = {sgn * x.x, sgn * x.y, sgn * x.z, sgn * x.w};
+    const float lv[4] = {l.x, l.y, l.z, l.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[i][c] = fmaf(xv[i], lv[c], acc[i][c]);
+}
+
+__global__ void __launch_bounds__(64) k_trsm_rlt_f32(const float *__restrict__ L, int64_t lda,
+                                                     const float *__restrict__ dinv, float *B, int64_t ldb,
+                                                     int64_t m, int bs, int vec, float *hi, float *lo, int kpad)
+{
+    extern __shared__ __align__(16) float smf[];
+    using ptrsm::LDB;
+    using ptrsm::NT;
+    const int nj = (bs + 31) / 32;
+    float *Xs = smf;                      // Xs[k * 32 + r]: column k of the CTA's rows (B, then X)
+    float *Lc = Xs + nj * 32 * 32;        // [2][32][LDB]
+    float *Ds = Lc + 2 * 32 * LDB;        // [2][32][LDB]
+    float *Ts = Ds + 2 * 32 * LDB;        // [32][LDB]: Ts[q][r] = acc[r][q]
+    const int tid = threadIdx.x, rq = tid & 7, cg = tid >> 3;   // rows 4rq..4rq+3, columns 4cg..4cg+3
+    const int64_t r0 = (int64_t)blockIdx.x * 32;
+    // the CTA's rows arrive by cp.async (16-byte runs of 4 rows when aligned),
+    // all in flight at once, in the same group as the first inverse block
+    const bool vecB = ((uintptr_t)B % 16 == 0) && (ldb % 4 == 0);
+    for (int idx = tid; idx < nj * 32 * 8; idx += NT) {
+        const int k = idx >> 3, r4 = (idx & 7) * 4;
+        float *d = Xs + k * 32 + r4;
+        const float *g = B + (r0 + r4) + (int64_t)k * ldb;
+        const int64_t nv64 = (k < bs) ? m - (r0 + r4) : 0;
+        const int nv = nv64 < 0 ? 0 : (nv64 > 4 ? 4 : (int)nv64);
+        if (vecB) {
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(d)),
+                         "l"(nv ? g : B), "r"(4 * nv));
+        } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                if (e < nv) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(d + e)),
+                                         "l"(g + e));
+                else d[e] = 0.f;
+            }
+        }
+    }
+    const int S = nj * (nj - 1) / 2;      // chunks (j, kc), kc < j, in j-major order
+    ptrsm_stage_D(Ds, dinv, 0, tid);
+    cp_async_commit();
+    if (S > 0) {
+        ptrsm_stage_L(Lc, L, lda, bs, 1, 0, vec, tid);
+        ptrsm_stage_D(Ds + 32 * LDB, dinv, 1, tid);
+    }
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+
+    float acc[4][4];
+    // X_j = acc Dinv_j^T, written to Xs, to B and (optionally) as TF32 operands
+    auto finish = [&](int j) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            *reinterpret_cast<float4 *>(Ts + (4 * cg + c) * LDB + 4 * rq) =
+                make_float4(acc[0][c], acc[1][c], acc[2][c], acc[3][c]);
+        __syncthreads();
+        const float *D = Ds + (j & 1) * 32 * LDB;
+        float y[4][4] = {};
+#pragma unroll 8
+        for (int q = 0; q < 32; ++q)
+            fma4x4(y, *reinterpret_cast<const float4 *>(Ts + q * LDB + 4 * rq),
+                   *reinterpret_cast<const float4 *>(D + q * LDB + 4 * cg), 1.f);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int col = 32 * j + 4 * cg + c;
+            *reinterpret_cast<float4 *>(Xs + col * 32 + 4 * rq) = make_float4(y[0][c], y[1][c], y[2][c], y[3][c]);
+            if (col < bs)
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (r0 + 4 * rq + i < m) B[(r0 + 4 * rq + i) + (int64_t)col * ldb] = y[i][c];
+        }
+        // fused operand prep for the tensor-core update: K-major TF32 hi (+ lo)
+        const int col0 = 32 * j + 4 * cg;
+        if (hi != nullptr && col0 < kpad) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const int64_t r = r0 + 4 * rq + i;
+                if (r < m) {
+                    float4 vh, vl;
+                    vh.x = tf32_rna(y[i][0]); vh.y = tf32_rna(y[i][1]); vh.z = tf32_rna(y[i][2]); vh.w = tf32_rna(y[i][3]);
+                    *reinterpret_cast<float4 *>(hi + r * kpad + col0) = vh;
+                    if (lo != nullptr) {
+                        vl.x = y[i][0] - vh.x; vl.y = y[i][1] - vh.y; vl.z = y[i][2] - vh.z; vl.w = y[i][3] - vh.w;
+                        *reinterpret_cast<float4 *>(lo + r * kpad + col0) = vl;
+                    }
+                }
+            }
+        }
+    };
+    auto load_b = [&](int j) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float4 v = *reinterpret_cast<const float4 *>(Xs + (32 * j + 4 * cg + c) * 32 + 4 * rq);
+            acc[0][c] = v.x; acc[1][c] = v.y; acc[2][c] = v.z; acc[3][c] = v.w;
+        }
+    };
+    load_b(0);
+    finish(0);
+    int j = 1, kc = 0;
+    for (int s = 0; s < S; ++s) {
+        int jn = j, kn = kc + 1;
+        if (kn == jn) { ++jn; kn = 0; }
+        if (s + 1 < S) {
+            ptrsm_stage_L(Lc + ((s + 1) & 1) * 32 * LDB, L, lda, bs, jn, kn, vec, tid);
+            if (kn == 0) ptrsm_stage_D(Ds + (jn & 1) * 32 * LDB, dinv, jn, tid);
+        }
+        cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        if (kc == 0) load_b(j);
+        const float *Lb = Lc + (s & 1) * 32 * LDB;
+        const float *Xk = Xs + 32 * kc * 32;
+#pragma unroll 8
+        for (int k = 0; k < 32; ++k)
+            fma4x4(acc, *reinterpret_cast<const float4 *>(Xk + k * 32 + 4 * rq),
+                   *reinterpret_cast<const float4 *>(Lb + k * LDB + 4 * cg), -1.f);
+        if (kc == j - 1) finish(j);
+        __syncthreads();
+        j = jn; kc = kn;
+    }
+    // operand columns past the last 32-block are zero padding
+    if (hi != nullptr)
+        for (int idx = tid; idx < 32 * (kpad - 32 * nj); idx += NT) {
+            const int r = idx % 32, k = 32 * nj + idx / 32;
+            if (r0 + r < m) {
+                hi[(r0 + r) * kpad + k] = 0.f;
+                if (lo != nullptr) lo[(r0 + r) * kpad + k] = 0.f;
+            }
+        }
+    cp_async_wait<0>();
 }
 
 // ------------------------------------------------------------------------
@@ -143,13 +263,6 @@ __global__ void __launch_bounds__(256) k_syrk_lower_f32_simt(const float *__rest
 // ------------------------------------------------------------------------
 // panel prep: X (m x kb, column-major FP32) -> K-major operand copies
 // ------------------------------------------------------------------------
-LNB_DEV float tf32_rna(float x)
-{
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return __uint_as_float(r);
-}
-
 // mode 0: hi/lo TF32 split into two fp32 arrays; mode 1: hi only
 __global__ void __launch_bounds__(256) k_prep_tf32(const float *__restrict__ X, int64_t ldx, int64_t m, int kb,
                                                    int kpad, float *hi, float *lo)
@@ -253,7 +366,7 @@ extern "C" int lnb_k_potrf_f32(float *A, int64_t lda, int bs, int64_t row0, floa
 {
     if (bs <= 0) return 0;
     if (bs > LEAF) return (int)cudaErrorInvalidValue;
-    const int smem = (bs * (bs + 1) + 4 * 32 * 33) * (int)sizeof(float);
+    const int smem = (int)leaf_smem_bytes<float>(bs);
     cudaFuncSetAttribute(k_potrf_leaf<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     k_potrf_leaf<float><<<1, 256, smem, s>>>(A, lda, bs, row0, dinv, st);
     lnb_prof_count(1);
@@ -264,7 +377,30 @@ extern "C" int lnb_k_trsm_rlt_f32(const float *L, int64_t lda, const float *dinv
                                   int bs, lnb_stream_t s)
 {
     if (m <= 0 || bs <= 0) return 0;
-    k_trsm_rlt_f32<<<(unsigned)((m + 63) / 64), 256, 0, s>>>(L, lda, dinv, B, ldb, m, bs);
+    const int nj = (bs + 31) / 32;
+    const int smem = (nj * 32 * 32 + 5 * 32 * ptrsm::LDB) * (int)sizeof(float);
+    cudaFuncSetAttribute(k_trsm_rlt_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int vec = ((uintptr_t)L % 16 == 0) && (lda % 4 == 0);
+    k_trsm_rlt_f32<<<(unsigned)((m + 31) / 32), ptrsm::NT, smem, s>>>(L, lda, dinv, B, ldb, m, bs, vec, nullptr,
+                                                                      nullptr, 0);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+
+// the panel solve plus the K-major TF32 operand copies of its result (hi, and
+// lo = x - hi when lo != NULL); kpad >= 32 ceil(bs/32), a multiple of 4, hi/lo
+// 16-byte aligned
+extern "C" int lnb_k_trsm_rlt_prep_f32(const float *L, int64_t lda, const float *dinv, float *B, int64_t ldb,
+                                       int64_t m, int bs, float *hi, float *lo, int kpad, lnb_stream_t s)
+{
+    if (m <= 0 || bs <= 0) return 0;
+    const int nj = (bs + 31) / 32;
+    if (32 * nj > kpad || kpad % 4 || (uintptr_t)hi % 16 || (uintptr_t)lo % 16) return (int)cudaErrorInvalidValue;
+    const int smem = (nj * 32 * 32 + 5 * 32 * ptrsm::LDB) * (int)sizeof(float);
+    cudaFuncSetAttribute(k_trsm_rlt_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int vec = ((uintptr_t)L % 16 == 0) && (lda % 4 == 0);
+    k_trsm_rlt_f32<<<(unsigned)((m + 31) / 32), ptrsm::NT, smem, s>>>(L, lda, dinv, B, ldb, m, bs, vec, hi, lo,
+                                                                      kpad);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }

@@ -366,7 +366,7 @@ extern "C" int lnb_k_potrf_f64(double *A, int64_t lda, int bs, int64_t row0, dou
 {
     if (bs <= 0) return 0;
     if (bs > LEAF) return (int)cudaErrorInvalidValue;
-    const int smem = (bs * (bs + 1) + 4 * 32 * 33) * (int)sizeof(double);
+    const int smem = (int)leaf_smem_bytes<double>(bs);
     cudaFuncSetAttribute(k_potrf_leaf<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     k_potrf_leaf<double><<<1, 256, smem, s>>>(A, lda, bs, row0, dinv, st);
     lnb_prof_count(1);

@@ -3,99 +3,171 @@
 // Semantics of task_dpotrf / LAPACK potrf 'L' (tasks_potrf.c:20-24) on a
 // tile of order bs <= 128, with the info the reference drops reported in
 // the status word.  Larger diagonal tiles are factored by the host-side
-// nested schedule (leaf POTRF + panel TRSM + DMMA update on 128-wide
-// sub-tiles), the structure of the reference's nested variant
-// (chol_nrlmain.c).
+// nested schedule (leaf POTRF + panel TRSM + update on 128-wide sub-tiles),
+// the structure of the reference's nested variant (chol_nrlmain.c).
 //
-// The whole tile lives in shared memory (128 x 129 doubles = 129 KB).  For
-// each 16-column panel, warp 0 factors the 16 x 16 diagonal block in
-// registers with shuffles; then all threads solve the rows below it (one row
-// per thread) and apply the rank-16 update to the trailing lower triangle.  At the
-// end the inverses of the tile's 32x32 diagonal blocks (used by the panel
-// TRSM) are computed from the factor in shared memory.
+// The whole tile lives in shared memory and is factored in 32-column panels:
+//   (1) warp 0 factors the 32 x 32 diagonal block left-looking, column by
+//       column in potf2 order, one row per lane, in rolled loops over shared
+//       memory.  Unrolled register code for this one-warp phase outgrew the
+//       instruction cache and ran at ~30 cycles per instruction.  Columns
+//       are scaled by rsqrt(pivot), the reciprocal LAPACK's potf2 scales by.
+//       The warp then inverts the block by forward substitution, one column
+//       per lane.
+//   (2) the rows below the block become b * inv(L_jj)^T: independent dot
+//       products, 4 threads per row, instead of a substitution chain;
+//   (3) the rank-32 update of the trailing triangle reads a transposed copy
+//       of the panel with vector loads, 4 x 4 outputs per thread.
+// The 32 x 32 inverses are written out (dinv) for the panel TRSM below the
+// tile.  After a failed pivot the columns before it are finished for every
+// row of the tile, the failing diagonal keeps its updated value, and the
+// inverses use the identity past the failure.
 #pragma once
 #include "common.cuh"
 
 namespace lnb {
 
 constexpr int LEAF = 128;   // max order of a leaf tile
-constexpr int LP = 16;      // panel width of the leaf factorization
+constexpr int LP = 32;      // panel width of the leaf factorization
+
+LNB_DEV void leaf_cp_async(float *smem, const float *g)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(smem)), "l"(g));
+}
+LNB_DEV void leaf_cp_async(double *smem, const double *g) { cp_async8(smem, g, true); }
+LNB_DEV float leaf_rsqrt(float x) { return rsqrtf(x); }
+LNB_DEV double leaf_rsqrt(double x) { return rsqrt(x); }
+
+// shared memory layout of the leaf (offsets in elements of T, 16-byte aligned)
+struct LeafLayout {
+    int lds, ldp;
+    size_t s_off, p_off, li_off, rd_off, total;
+};
+template <typename T>
+__host__ __device__ inline LeafLayout leaf_layout(int bs)
+{
+    LeafLayout L;
+    const int v = 16 / (int)sizeof(T);
+    L.lds = bs + 1;
+    L.ldp = ((bs + 3) / 4) * 4 + 4;   // 4-row vector reads may run 3 past bs
+    L.s_off = 0;
+    L.p_off = (((size_t)bs * L.lds + v - 1) / v) * v;
+    L.li_off = L.p_off + (size_t)LP * L.ldp;
+    L.rd_off = L.li_off + ((LP * (LP + 1) + v - 1) / v) * v;
+    L.total = L.rd_off + LP;
+    return L;
+}
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_potrf_leaf(T *A, int64_t lda, int bs, int64_t row0, T *dinv,
                                                     lnb_status_t *st)
 {
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    const int LDS = bs + 1;
-    T *S = reinterpret_cast<T *>(sm_raw);  // S[r * LDS + c] = A[r, c], lower part
+    const LeafLayout LY = leaf_layout<T>(bs);
+    const int LDS = LY.lds, LDP = LY.ldp;
+    T *base = reinterpret_cast<T *>(sm_raw);
+    T *S = base + LY.s_off;     // S[r * LDS + c] = A[r, c], lower part
+    T *Pt = base + LY.p_off;    // Pt[p * LDP + r] = L[r, j0 + p]: the panel below the block, transposed
+    T *Li = base + LY.li_off;   // Li[p * 33 + j] = inv(L_jj)[j][p]
+    T *Rd = base + LY.rd_off;   // Rd[c] = 1 / L[j0 + c, j0 + c]
     __shared__ int fail_col;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) fail_col = bs;
 
+    // the tile arrives by element-wise cp.async, all copies in flight at once
+    // (a plain load loop would pay one memory round trip per iteration)
     for (int idx = tid; idx < bs * bs; idx += blockDim.x) {
         const int c = idx / bs, r = idx - c * bs;
-        if (r >= c) S[r * LDS + c] = A[(int64_t)r + (int64_t)c * lda];
+        if (r >= c) leaf_cp_async(S + r * LDS + c, A + (int64_t)r + (int64_t)c * lda);
     }
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
 
     for (int j0 = 0; j0 < bs; j0 += LP) {
         const int jb = min(LP, bs - j0);
         if (warp == 0) {
-            // (1) the jb x jb diagonal block in registers: lane l holds row j0+l
-            T x[LP];
-#pragma unroll
-            for (int c = 0; c < LP; ++c)
-                x[c] = (lane < jb && c < jb && lane >= c) ? S[(j0 + lane) * LDS + j0 + c] : T(0);
-            int bad = bs;
-#pragma unroll
-            for (int c = 0; c < LP; ++c) {
-                if (c < jb && bad == bs) {
-                    const T d = __shfl_sync(0xffffffffu, x[c], c);
-                    if (!(d > T(0))) {
-                        bad = j0 + c;
-                    } else {
-                        const T dd = sqrt(d);
-                        if (lane == c) x[c] = dd;
-                        else if (lane > c) x[c] = x[c] / dd;
-#pragma unroll
-                        for (int cc = c + 1; cc < LP; ++cc) {
-                            const T l = __shfl_sync(0xffffffffu, x[c], cc);   // L[j0+cc][j0+c]
-                            if (lane >= cc) x[cc] -= x[c] * l;
-                        }
-                    }
+            // ---- (1) factor the jb x jb diagonal block: lane l owns row j0 + l ----
+            const int rl = lane < jb ? lane : 0;                 // rows past jb read row 0, unused
+            T *Ll = S + (j0 + rl) * LDS + j0;
+            int bad = -1;
+            for (int c = 0; c < jb; ++c) {
+                const T *Lc = S + (j0 + c) * LDS + j0;
+                T s0 = Ll[c], s1 = T(0);
+                int p = 0;
+                for (; p + 1 < c; p += 2) {
+                    s0 -= Ll[p] * Lc[p];
+                    s1 -= Ll[p + 1] * Lc[p + 1];
                 }
+                if (p < c) s0 -= Ll[p] * Lc[p];
+                const T sv = s0 + s1;                           // updated A[l][c] for l >= c
+                const T d = __shfl_sync(0xffffffffu, sv, c);
+                if (!(d > T(0))) {
+                    bad = c;                                    // potf2 keeps the updated pivot
+                    if (lane == c) Ll[c] = d;
+                    break;
+                }
+                const T inv = leaf_rsqrt(d);
+                if (lane == c) { Ll[c] = d * inv; Rd[c] = inv; }
+                else if (lane > c && lane < jb) Ll[c] = sv * inv;
+                __syncwarp();
             }
-#pragma unroll
-            for (int c = 0; c < LP; ++c)
-                if (lane < jb && c < jb && lane >= c) S[(j0 + lane) * LDS + j0 + c] = x[c];
-            if (lane == 0 && bad < bs) {
-                fail_col = bad;
-                atomicCAS(&st->info, 0, (int)(row0 + bad + 1));
+            const int fc = bad >= 0 ? bad : jb;   // finished columns of the block
+            if (lane == 0 && bad >= 0) {
+                fail_col = j0 + bad;
+                atomicCAS(&st->info, 0, (int)(row0 + j0 + bad + 1));
+            }
+            __syncwarp();
+            // ---- inverse of the block (identity past fc): lane c builds column c
+            //      in Li[c][*] = inv[*][c] by forward substitution ----
+            T *Xc = Li + lane * (LP + 1);
+            for (int r = 0; r < LP; ++r) {
+                T v0 = (r == lane) ? T(1) : T(0), v1 = T(0);
+                if (r < fc) {
+                    const T *Lr = S + (j0 + r) * LDS + j0;
+                    int p = 0;
+                    for (; p + 1 < r; p += 2) {
+                        v0 -= Lr[p] * Xc[p];
+                        v1 -= Lr[p + 1] * Xc[p + 1];
+                    }
+                    if (p < r) v0 -= Lr[p] * Xc[p];
+                }
+                Xc[r] = (v0 + v1) * (r < fc ? Rd[r] : T(1));
+            }
+            if (dinv != nullptr) {
+                T *D = dinv + (int64_t)(j0 / LP) * LP * LP;
+                for (int r = 0; r < LP; ++r) D[r + LP * lane] = Xc[r];
             }
         }
         __syncthreads();
-        // after a failed pivot only the columns before it are finished, for
-        // every row of the tile (as LAPACK's column-by-column potf2 leaves them)
+        // columns of this panel that are final for the rows below
         const int jv = fail_col < bs ? fail_col - j0 : jb;
-        // (2) rows below the diagonal block: X = B L^-T, one row per thread,
-        //     L read from shared memory (the same element by all threads)
-        for (int r = j0 + jb + tid; r < bs; r += blockDim.x) {
-            T x[LP];
+        // ---- (2) rows below the block: x_r = b_r inv(L_jj)^T, 4 threads per row ----
+        const int t0 = j0 + jb;
+        const int g = tid & 3;
+        for (int rb = t0; rb < bs; rb += 64) {
+            const int r = rb + (tid >> 2);
+            const bool act = r < bs;
+            T b[LP];
 #pragma unroll
-            for (int c = 0; c < LP; ++c) {
-                if (c < jv) {
-                    T v = S[r * LDS + j0 + c];
+            for (int p = 0; p < LP; ++p) b[p] = (act && p < jb) ? S[r * LDS + j0 + p] : T(0);
+            __syncwarp();
 #pragma unroll
-                    for (int p = 0; p < c; ++p) v -= x[p] * S[(j0 + c) * LDS + j0 + p];
-                    x[c] = v / S[(j0 + c) * LDS + j0 + c];
-                    S[r * LDS + j0 + c] = x[c];
+            for (int s = 0; s < LP / 4; ++s) {
+                const int j = g + 4 * s;
+                T acc = T(0);
+#pragma unroll
+                for (int p = 0; p < LP; ++p) acc = fma(b[p], Li[p * (LP + 1) + j], acc);
+                if (act && j < jv) {
+                    S[r * LDS + j0 + j] = acc;
+                    Pt[j * LDP + r] = acc;
                 }
             }
         }
         __syncthreads();
         if (fail_col < bs) break;
-        // rank-jb update of the trailing lower triangle, 4x4 blocks per thread
-        const int t0 = j0 + jb, tr = bs - t0;
+        // ---- (3) rank-jb update of the trailing lower triangle, 4x4 per thread ----
+        const int tr = bs - t0;
         if (tr > 0) {
             const int nb4 = (tr + 3) / 4, nblk = nb4 * (nb4 + 1) / 2;
             for (int id = tid; id < nblk; id += blockDim.x) {
@@ -103,70 +175,64 @@ __global__ void __launch_bounds__(256) k_potrf_leaf(T *A, int64_t lda, int bs, i
                 while (bi * (bi + 1) / 2 > id) --bi;
                 while ((bi + 1) * (bi + 2) / 2 <= id) ++bi;
                 const int bj = id - bi * (bi + 1) / 2;
-                const int ra = t0 + 4 * bi, rb = t0 + 4 * bj;
+                const int ra = t0 + 4 * bi, rc = t0 + 4 * bj;
                 T acc[4][4];
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
                     for (int j = 0; j < 4; ++j) acc[i][j] = T(0);
                 for (int p = 0; p < jb; ++p) {
-                    T a[4], b[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        a[i] = (ra + i < bs) ? S[(ra + i) * LDS + j0 + p] : T(0);
-                        b[i] = (rb + i < bs) ? S[(rb + i) * LDS + j0 + p] : T(0);
+                    T a[4], c[4];
+                    if constexpr (sizeof(T) == 4) {
+                        const float4 va = *reinterpret_cast<const float4 *>(Pt + p * LDP + ra);
+                        const float4 vc = *reinterpret_cast<const float4 *>(Pt + p * LDP + rc);
+                        a[0] = va.x; a[1] = va.y; a[2] = va.z; a[3] = va.w;
+                        c[0] = vc.x; c[1] = vc.y; c[2] = vc.z; c[3] = vc.w;
+                    } else {
+                        const double2 va0 = *reinterpret_cast<const double2 *>(Pt + p * LDP + ra);
+                        const double2 va1 = *reinterpret_cast<const double2 *>(Pt + p * LDP + ra + 2);
+                        const double2 vc0 = *reinterpret_cast<const double2 *>(Pt + p * LDP + rc);
+                        const double2 vc1 = *reinterpret_cast<const double2 *>(Pt + p * LDP + rc + 2);
+                        a[0] = va0.x; a[1] = va0.y; a[2] = va1.x; a[3] = va1.y;
+                        c[0] = vc0.x; c[1] = vc0.y; c[2] = vc1.x; c[3] = vc1.y;
                     }
 #pragma unroll
                     for (int i = 0; i < 4; ++i)
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], c[j], acc[i][j]);
                 }
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
-                        const int r = ra + i, c = rb + j;
-                        if (r < bs && c < bs && r >= c) S[r * LDS + c] -= acc[i][j];
+                        const int r = ra + i, cc = rc + j;
+                        if (r < bs && cc < bs && r >= cc) S[r * LDS + cc] -= acc[i][j];
                     }
             }
         }
         __syncthreads();
     }
     __syncthreads();
-    const int lim = fail_col;
-    // write the factored lower triangle back (columns < lim are the factor;
-    // past a failed pivot the partial state is written like LAPACK does)
+    // write the lower triangle back (past a failed pivot, the partial state)
     for (int idx = tid; idx < bs * bs; idx += blockDim.x) {
         const int c = idx / bs, r = idx - c * bs;
         if (r >= c) A[(int64_t)r + (int64_t)c * lda] = S[r * LDS + c];
     }
-    // inverses of the 32x32 diagonal blocks (identity past a failed pivot):
-    // warp q inverts block q, lane c builds column c in shared scratch
+    // blocks of the tile after a failed panel: identity inverses
     if (dinv != nullptr) {
-        T *X = S + bs * LDS;                        // 4 x [32][33] scratch after the tile
-        const int nq = (bs + 31) / 32;
-        for (int q = warp; q < nq; q += blockDim.x / 32) {
-            const int qn = max(0, min(32, lim - q * 32));
-            T *Xq = X + (q & 3) * 32 * 33;
-            const int c = lane, o = q * 32;
-            for (int r = 0; r < 32; ++r) {
-                T v;
-                if (c >= qn) v = (r == c) ? T(1) : T(0);
-                else if (r < c || r >= qn) v = T(0);
-                else if (r == c) v = T(1) / S[(o + c) * LDS + o + c];
-                else {
-                    T s = T(0);
-                    for (int p = c; p < r; ++p) s += S[(o + r) * LDS + o + p] * Xq[p * 33 + c];
-                    v = -s / S[(o + r) * LDS + o + r];
-                }
-                Xq[r * 33 + c] = v;
-            }
-            __syncwarp();
-            T *D = dinv + (int64_t)q * 1024;
-            for (int r = 0; r < 32; ++r) D[r + 32 * c] = Xq[r * 33 + c];
-            __syncwarp();
+        const int nq = (bs + LP - 1) / LP;
+        const int q0 = fail_col < bs ? fail_col / LP + 1 : nq;
+        for (int idx = tid; idx < (nq - q0) * LP * LP; idx += blockDim.x) {
+            const int q = q0 + idx / (LP * LP), e = idx % (LP * LP);
+            dinv[(int64_t)q * LP * LP + e] = (e % LP == e / LP) ? T(1) : T(0);
         }
     }
+}
+
+template <typename T>
+inline size_t leaf_smem_bytes(int bs)
+{
+    return leaf_layout<T>(bs).total * sizeof(T);
 }
 
 }  // namespace lnb

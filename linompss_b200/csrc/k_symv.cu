@@ -5,81 +5,112 @@
 // product reads only the lower triangle (4 n^2 bytes): each stored element
 // A[r,c] (r > c) contributes A[r,c] x[c] to y[r] and A[r,c] x[r] to y[c].
 //
-// Layout of the walk: a CTA owns a strip of W columns and a segment of rows
-// below the strip's diagonal; thread t owns one row at a time, reads the W
-// elements of its row in the strip (consecutive threads -> consecutive rows,
-// so every column is read as contiguous 2 KB runs), accumulates y[r] for its
-// row and keeps W per-column partials for the transposed contribution, which
-// are reduced across the CTA once at the end.  Accumulation into y uses
-// double atomics (summation order is not fixed).
+// Layout of the walk: a CTA owns a group of column strips and a segment of
+// rows below the group's diagonal; thread t owns RPT rows, reads the strip
+// elements of each (consecutive threads -> consecutive rows, so every column
+// is read as contiguous runs), accumulates y[r] for its rows across the whole
+// group and keeps per-column partials for the transposed contribution, which
+// are reduced across the CTA once per strip.  Accumulation into y uses double
+// atomics (summation order is not fixed).
 #include "common.cuh"
 
 namespace lnb {
 
 constexpr int SV_THREADS = 256;
-constexpr int SV_SEG = 2048;       // rows per CTA segment
+
+// Work item: SEG rows (from the item's diagonal down) x G strips of WS columns.
+// Each thread owns RPT rows; their sums over the item's G*WS columns build up
+// in shared memory (one atomic per row per item), and the column sums of the
+// current strip build up in registers over the thread's rows (one CTA
+// reduction + WS atomics per strip).  At ~128 registers two CTAs fit per SM
+// and the loads of two rows per thread are in flight at once.
+template <int NR>
+struct SvCfg {
+    static constexpr int WS = NR >= 8 ? 2 : 16 / NR;
+    static constexpr int G = 4;
+    static constexpr int IW = WS * G;
+    static constexpr int RPT = NR >= 8 ? 2 : NR >= 4 ? 4 : 8;
+    static constexpr int SEG = SV_THREADS * RPT;
+};
 
 template <int NR>
-__global__ void __launch_bounds__(SV_THREADS) k_symv_lower(int64_t n, const double *__restrict__ A, int64_t lda,
-                                                           const double *__restrict__ X, double *Y, int absval)
+__global__ void __launch_bounds__(SV_THREADS, 2) k_symv_lower(int64_t n, const double *__restrict__ A, int64_t lda,
+                                                              const double *__restrict__ X, double *Y, int absval)
 {
-    constexpr int W = 64 / NR;
-    __shared__ double xs[W][NR];
-    __shared__ double red[SV_THREADS / 32][W * NR];
-    const int64_t cj = (int64_t)blockIdx.y * W;
-    const int64_t r0 = cj + (int64_t)blockIdx.x * SV_SEG;
+    using Cf = SvCfg<NR>;
+    constexpr int WS = Cf::WS, IW = Cf::IW, RPT = Cf::RPT;
+    __shared__ double xs[IW][NR];
+    __shared__ double red[SV_THREADS / 32][WS * NR];
+    __shared__ double v1s[RPT * NR][SV_THREADS];     // row sums, each thread its own column
+    const int64_t cj = (int64_t)blockIdx.y * IW;
+    const int64_t r0 = cj + (int64_t)blockIdx.x * Cf::SEG;
     if (cj >= n || r0 >= n) return;
-    const int wcols = (int)((n - cj) < W ? (n - cj) : W);
-    for (int i = threadIdx.x; i < W * NR; i += SV_THREADS) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wcols = (int)((n - cj) < IW ? (n - cj) : IW);
+    for (int i = tid; i < IW * NR; i += SV_THREADS) {
         const int c = i / NR, q = i % NR;
         xs[c][q] = (c < wcols) ? X[(cj + c) + (int64_t)q * n] : 0.0;
     }
+    for (int i = 0; i < RPT * NR; ++i) v1s[i][tid] = 0.0;
     __syncthreads();
-    double v2[W][NR];
+#pragma unroll 1
+    for (int g = 0; g < Cf::G; ++g) {
+        const int64_t cg = cj + g * WS;
+        const int wg = wcols - g * WS;               // valid columns of this strip (may be <= 0)
+        double v2[WS][NR];
 #pragma unroll
-    for (int c = 0; c < W; ++c)
+        for (int c = 0; c < WS; ++c)
 #pragma unroll
-        for (int q = 0; q < NR; ++q) v2[c][q] = 0.0;
-
-    const int64_t r1 = (r0 + SV_SEG) < n ? (r0 + SV_SEG) : n;
-    for (int64_t r = r0 + threadIdx.x; r < r1; r += SV_THREADS) {
-        double xr[NR], v1[NR];
+            for (int q = 0; q < NR; ++q) v2[c][q] = 0.0;
+#pragma unroll 2
+        for (int i = 0; i < RPT; ++i) {
+            const int64_t r = r0 + tid + (int64_t)SV_THREADS * i;
+            const double *arow = A + r + cg * lda;
+            double av[WS], xr[NR], s1[NR];
 #pragma unroll
-        for (int q = 0; q < NR; ++q) { xr[q] = X[r + (int64_t)q * n]; v1[q] = 0.0; }
-        const double *arow = A + r + cj * lda;
-        double a[W];
-#pragma unroll
-        for (int c = 0; c < W; ++c) a[c] = (c < wcols && r >= cj + c) ? __ldcs(arow + (int64_t)c * lda) : 0.0;
-#pragma unroll
-        for (int c = 0; c < W; ++c) {
-            double av = absval ? fabs(a[c]) : a[c];
-            const bool strict = r > cj + c;
+            for (int c = 0; c < WS; ++c)
+                av[c] = (r < n && c < wg && r >= cg + c) ? __ldcs(arow + (int64_t)c * lda) : 0.0;
 #pragma unroll
             for (int q = 0; q < NR; ++q) {
-                v1[q] = fma(av, xs[c][q], v1[q]);
-                if (strict) v2[c][q] = fma(av, xr[q], v2[c][q]);
+                xr[q] = r < n ? __ldg(X + r + (int64_t)q * n) : 0.0;
+                s1[q] = 0.0;
             }
-        }
 #pragma unroll
-        for (int q = 0; q < NR; ++q) atomicAdd(&Y[r + (int64_t)q * n], v1[q]);
+            for (int c = 0; c < WS; ++c) {
+                const double v = absval ? fabs(av[c]) : av[c];
+                const bool strict = r > cg + c;
+#pragma unroll
+                for (int q = 0; q < NR; ++q) {
+                    s1[q] = fma(v, xs[g * WS + c][q], s1[q]);
+                    if (strict) v2[c][q] = fma(v, xr[q], v2[c][q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NR; ++q) v1s[i * NR + q][tid] += s1[q];
+        }
+        // column sums of the strip over the CTA's rows
+#pragma unroll
+        for (int c = 0; c < WS; ++c)
+#pragma unroll
+            for (int q = 0; q < NR; ++q) {
+                double v = v2[c][q];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0) red[warp][c * NR + q] = v;
+            }
+        __syncthreads();
+        for (int i = tid; i < WS * NR; i += SV_THREADS) {
+            double v = 0.0;
+            for (int w = 0; w < SV_THREADS / 32; ++w) v += red[w][i];
+            const int c = i / NR, q = i % NR;
+            if (c < wg && v != 0.0) atomicAdd(&Y[(cg + c) + (int64_t)q * n], v);
+        }
+        __syncthreads();
     }
-    // reduce the transposed partials over the CTA
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int c = 0; c < W; ++c)
-#pragma unroll
-        for (int q = 0; q < NR; ++q) {
-            double v = v2[c][q];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if (lane == 0) red[warp][c * NR + q] = v;
-        }
-    __syncthreads();
-    for (int i = threadIdx.x; i < W * NR; i += SV_THREADS) {
-        double v = 0.0;
-        for (int w = 0; w < SV_THREADS / 32; ++w) v += red[w][i];
-        const int c = i / NR, q = i % NR;
-        if (c < wcols && v != 0.0) atomicAdd(&Y[(cj + c) + (int64_t)q * n], v);
+    for (int i = 0; i < RPT; ++i) {
+        const int64_t r = r0 + tid + (int64_t)SV_THREADS * i;
+        if (r < n)
+            for (int q = 0; q < NR; ++q) atomicAdd(&Y[r + (int64_t)q * n], v1s[i * NR + q][tid]);
     }
 }
 
@@ -167,8 +198,8 @@ template <int NR>
 static void launch_symv(int64_t n, const double *A, int64_t lda, const double *X, double *Y, int absval,
                         lnb_stream_t s)
 {
-    constexpr int W = 64 / NR;
-    dim3 grid((unsigned)((n + SV_SEG - 1) / SV_SEG), (unsigned)((n + W - 1) / W));
+    using Cf = SvCfg<NR>;
+    dim3 grid((unsigned)((n + Cf::SEG - 1) / Cf::SEG), (unsigned)((n + Cf::IW - 1) / Cf::IW));
     k_symv_lower<NR><<<grid, SV_THREADS, 0, s>>>(n, A, lda, X, Y, absval);
     lnb_prof_count(1);
 }

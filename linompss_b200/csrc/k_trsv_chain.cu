@@ -11,13 +11,16 @@
 //     warps keep the last W solution blocks in shared memory and apply the W
 //     sub-diagonal tiles of each block row themselves, so no global-memory
 //     round trip sits between two chain steps.  The W band tiles of the next
-//     step stream in by cp.async while the current step computes, and the
-//     inverse of the next diagonal block streams into registers.
-//   * a loader warp of the same CTA waits until the far-off-diagonal updates
-//     of upcoming block rows are complete and stages those right-hand-side
-//     rows into shared memory ahead of the compute warps;
-//   * a publisher warp makes each finished solution block visible to the
-//     whole GPU (fence + release flag) off the compute warps' path;
+//     step stream in by cp.async while the current step computes (from L2:
+//     they and the diagonal inverses are bulk-prefetched PF steps ahead), and
+//     the inverse of the next diagonal block streams into registers.
+//   * a loader warp of the same CTA (4 lane groups, one upcoming block row
+//     each) waits until the far-off-diagonal updates of a row are complete
+//     and stages its right-hand sides into shared memory with cp.async ahead
+//     of the compute warps;
+//   * a publisher warp makes finished solution blocks visible to the whole
+//     GPU (one fence for all blocks finished so far, then their flags) off
+//     the compute warps' path;
 //   * every other CTA takes work items (row i, a chunk of CW tiles j <=
 //     i-W-1) from an atomic ticket in row order.  An item streams its tiles
 //     (double-buffered across items) before it waits for its solution blocks,
@@ -34,7 +37,9 @@ namespace chain {
 constexpr int TH = 64;              // block size
 constexpr int NCOMP = 256;          // compute threads: m = t>>2, kq = t&3
 constexpr int NTHR = NCOMP + 64;    // + publisher warp + loader warp
-constexpr int NBUF = 4;             // right-hand-side slots staged ahead
+constexpr int NBUF = 4;             // right-hand-side slots = loader lane groups
+constexpr int XR = 4;               // finished-block slots between compute and publisher
+constexpr int PF = 4;               // L2 prefetch distance of the chain, in steps
 
 // band width W handled by the chain CTA, worker chunk CW (tiles per item)
 template <typename TT> struct Cfg;
@@ -66,6 +71,27 @@ LNB_DEV void cp_async4(void *smem, const void *gmem)
 }
 LNB_DEV void cp_async_el(float *d, const float *g) { cp_async4(d, g); }
 LNB_DEV void cp_async_el(double *d, const double *g) { cp_async8(d, g, true); }
+
+// 16-byte cp.async from L2 (.cg) copying src_bytes (0, 8 or 16) and zero-filling the rest
+LNB_DEV void cp_async16_n(void *smem, const void *gmem, int src_bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem)), "l"(gmem),
+                 "r"(src_bytes));
+}
+// arrive on `bar` once this thread's earlier cp.async copies have landed
+LNB_DEV void cp_async_mbar_arrive(uint64_t *bar)
+{
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// hint: bring `bytes` (a multiple of 16, 16-byte aligned) into L2
+LNB_DEV void prefetch_l2(const void *p, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+LNB_DEV void st_relaxed(int *p, int v)
+{
+    asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 
 // named barrier over `count` threads that also ANDs a predicate
 LNB_DEV bool bar_and(int id, int count, bool pred)
@@ -119,6 +145,16 @@ LNB_DEV void stage_tile(const Args<TT> &a, TT *S, int i, int j, int tid, int nth
             }
         }
     }
+}
+
+// L2 prefetch of column `col` of the stored block holding op(T)(i, j)
+template <typename TT, bool TR>
+LNB_DEV void prefetch_tile_col(const Args<TT> &a, int i, int j, int col)
+{
+    const int rb = TR ? j : i, cb = TR ? i : j;
+    if (col >= blen(a, cb)) return;
+    const uint32_t bytes = (uint32_t)(blen(a, rb) * (int)sizeof(TT)) & ~15u;
+    if (bytes) prefetch_l2(a.T + (int64_t)rb * TH + ((int64_t)cb * TH + col) * a.ldt, bytes);
 }
 
 // part[r] += sum over this lane's 16 k of op[m][k] * X[r * 64 + k]
@@ -215,7 +251,7 @@ LNB_DEV void decode(int64_t q, int nb, int &row, int &chunk)
 }
 
 struct ChainBars {
-    uint64_t bfull[NBUF], bempty[NBUF], xfull[2], xempty[2];
+    uint64_t bfull[NBUF], bempty[NBUF], xfull[XR], xempty[XR];
     int abort;
 };
 
@@ -243,8 +279,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
         double *accs = bbuf + NBUF * NR * TH;                                         // [NR][64]
         ChainBars *cb = reinterpret_cast<ChainBars *>(accs + NR * TH);
         if (tid == 0) {
-            for (int q = 0; q < NBUF; ++q) { tc::mbar_init(&cb->bfull[q], 32); tc::mbar_init(&cb->bempty[q], NCOMP); }
-            for (int q = 0; q < 2; ++q) { tc::mbar_init(&cb->xfull[q], NCOMP); tc::mbar_init(&cb->xempty[q], 1); }
+            for (int q = 0; q < NBUF; ++q) { tc::mbar_init(&cb->bfull[q], 8); tc::mbar_init(&cb->bempty[q], NCOMP); }
+            for (int q = 0; q < XR; ++q) { tc::mbar_init(&cb->xfull[q], NCOMP); tc::mbar_init(&cb->xempty[q], 1); }
             cb->abort = 0;
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
@@ -252,50 +288,72 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
         const int warp = tid >> 5, lane = tid & 31;
 
         if (warp == 8) {
-            // ---- publisher: X_p visible GPU-wide, then ready[p] ----
-            for (int p = 0; p < nb; ++p) {
-                bool ok = true;
-                if (lane == 0) ok = tc::mbar_wait(&cb->xfull[p & 1], (p >> 1) & 1, a.wait_ns, &cb->abort, a.st);
-                ok = __shfl_sync(0xffffffffu, ok, 0);
-                if (!ok) {
-                    if (lane == 0) { cb->abort = 1; atomicCAS(&a.st->timeout, 0, 4); a.st->timeout_item = p; }
-                    return;
-                }
-                if (lane == 0) {
+            // ---- publisher: X_p visible GPU-wide, then ready[p].  One fence covers
+            //      every block the compute warps have finished by then. ----
+            if (lane == 0) {
+                int p = 0;
+                while (p < nb) {
+                    if (!tc::mbar_wait(&cb->xfull[p % XR], (p / XR) & 1, a.wait_ns, &cb->abort, a.st)) {
+                        cb->abort = 1;
+                        atomicCAS(&a.st->timeout, 0, 4);
+                        a.st->timeout_item = p;
+                        break;
+                    }
+                    int q = p + 1;
+                    while (q < nb && q < p + XR && tc::mbar_try_wait(&cb->xfull[q % XR], (q / XR) & 1)) ++q;
                     __threadfence();
-                    st_release(&a.ready[p], 1);
-                    tc::mbar_arrive(&cb->xempty[p & 1]);
+                    for (int t = p; t < q; ++t) {
+                        st_relaxed(&a.ready[t], 1);
+                        tc::mbar_arrive(&cb->xempty[t % XR]);
+                    }
+                    p = q;
                 }
             }
             return;
         }
         if (warp == 9) {
-            // ---- loader: B rows of chain position p once its items are done ----
-            for (int p = 0; p < nb; ++p) {
-                const int slot = p % NBUF;
+            // ---- loader: 4 groups of 8 lanes; group g stages the B rows of chain
+            //      positions p = g (mod 4) into slot g once the row's items are done.
+            //      16-byte copies from L2 land asynchronously and complete the slot's
+            //      mbarrier, so a group polls its next row while copies are in flight. ----
+            const int g = lane >> 3, gl = lane & 7;
+            const unsigned gmask = 0xffu << (8 * g);
+            const bool vecB = ((uintptr_t)a.B % 16 == 0) && (a.ldb % 2 == 0);
+            for (int p = g; p < nb; p += NBUF) {
                 bool ok = true;
-                if (lane == 0) {
+                if (gl == 0) {
                     if (p >= NBUF)
-                        ok = tc::mbar_wait(&cb->bempty[slot], ((p / NBUF) - 1) & 1, a.wait_ns, &cb->abort, a.st);
+                        ok = tc::mbar_wait(&cb->bempty[g], ((p / NBUF) - 1) & 1, a.wait_ns, &cb->abort, a.st);
                     if (ok) ok = wait_geq(&a.cnt[p], need_of<W, CW>(p), a.wait_ns, a.st);
                 }
-                ok = __shfl_sync(0xffffffffu, ok, 0);
+                ok = __shfl_sync(gmask, ok, 8 * g);
                 if (!ok) {
-                    if (lane == 0) { cb->abort = 1; atomicCAS(&a.st->timeout, 0, 5); a.st->timeout_item = p; }
-                    return;
+                    if (gl == 0) { cb->abort = 1; atomicCAS(&a.st->timeout, 0, 5); a.st->timeout_item = p; }
+                    break;
                 }
                 const int i = blk(a, p);
                 const int64_t oi = (int64_t)i * TH;
                 const int in_ = blen(a, i);
-                double *dst = bbuf + slot * NR * TH;
+                double *dst = bbuf + g * NR * TH;
+                if (vecB) {
 #pragma unroll
-                for (int q = 0; q < 2 * NR; ++q) {
-                    const int idx = lane + 32 * q, r = idx / TH, mm = idx % TH;
-                    dst[idx] = (mm < in_ && r < a.nrhs) ? __ldcg(a.B + (oi + mm) + (int64_t)r * a.ldb) : 0.0;
+                    for (int q = 0; q < 4 * NR; ++q) {
+                        const int pr = gl + 8 * q, r = pr / 32, mm = 2 * (pr % 32);
+                        const int nv = (r < a.nrhs) ? max(0, min(2, in_ - mm)) : 0;
+                        cp_async16_n(dst + r * TH + mm, nv ? a.B + (oi + mm) + (int64_t)r * a.ldb : a.B, 8 * nv);
+                    }
+                    cp_async_mbar_arrive(&cb->bfull[g]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 8 * NR; ++q) {
+                        const int idx = gl + 8 * q, r = idx / TH, mm = idx % TH;
+                        dst[idx] = (mm < in_ && r < a.nrhs) ? __ldcg(a.B + (oi + mm) + (int64_t)r * a.ldb) : 0.0;
+                    }
+                    __syncwarp(gmask);
+                    tc::mbar_arrive(&cb->bfull[g]);
                 }
-                __syncwarp();
-                tc::mbar_arrive(&cb->bfull[slot]);
             }
+            cp_async_wait<0>();
             return;
         }
 
@@ -319,6 +377,14 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
                 load_dinv<TR>(a.dinv, ip, m, kq, dnext);
             }
             cp_async_commit();
+            // L2 prefetch PF steps ahead (band tiles, one column per thread, and the
+            // diagonal inverse), so the cp.async of the next step is served from L2
+            if (a.vec && p + PF < nb) {
+                const int k = 1 + (tid >> 6);
+                if (k <= W && p + PF - k >= 0)
+                    prefetch_tile_col<TT, TR>(a, blk(a, p + PF), blk(a, p + PF - k), tid & 63);
+                if (tid == 255) prefetch_l2(a.dinv + (int64_t)blk(a, p + PF) * TH * TH, TH * TH * sizeof(double));
+            }
             // band: sum_k op(T)(i, i-k) X_{p-k}
             double part[NR];
 #pragma unroll
@@ -361,8 +427,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
                     if (m < in_ && r < a.nrhs) a.B[(oi + m) + (int64_t)r * a.ldb] = xs[r];
                 }
             okp = true;
-            if (p >= 2) okp = tc::mbar_wait(&cb->xempty[p & 1], ((p >> 1) - 1) & 1, a.wait_ns, &cb->abort, a.st);
-            tc::mbar_arrive(&cb->xfull[p & 1]);
+            if (p >= XR) okp = tc::mbar_wait(&cb->xempty[p % XR], ((p / XR) - 1) & 1, a.wait_ns, &cb->abort, a.st);
+            tc::mbar_arrive(&cb->xfull[p % XR]);
             return true;
         };
         for (int p = 0; p < nb; p += 2) {

@@ -205,13 +205,17 @@ int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode,
             }
         }
         if (mrem > 0) {
-            CK(lnb_k_trsm_rlt_f32(Akk, lda, dinv, Akk + bs, lda, mrem, bs, crit), "trsm f32");
-            if (mode == LNB_FACTOR_TF32X3 || mode == LNB_FACTOR_TF32)
-                CK(lnb_k_prep_tf32(Akk + bs, lda, mrem, bs, (int)pb.kpad, (float *)pb.hi[slot],
-                                   mode == LNB_FACTOR_TF32X3 ? (float *)pb.lo[slot] : NULL, crit), "prep tf32");
-            else if (mode == LNB_FACTOR_BF16)
-                CK(lnb_k_prep_bf16(Akk + bs, lda, mrem, bs, (int)pb.kpad, pb.scale[slot], pb.hi[slot], crit),
-                   "prep bf16");
+            if (mode == LNB_FACTOR_TF32X3 || mode == LNB_FACTOR_TF32) {
+                /* panel solve with the K-major operand copies written by the same launch */
+                CK(lnb_k_trsm_rlt_prep_f32(Akk, lda, dinv, Akk + bs, lda, mrem, bs, (float *)pb.hi[slot],
+                                           mode == LNB_FACTOR_TF32X3 ? (float *)pb.lo[slot] : NULL, (int)pb.kpad,
+                                           crit), "trsm+prep f32");
+            } else {
+                CK(lnb_k_trsm_rlt_f32(Akk, lda, dinv, Akk + bs, lda, mrem, bs, crit), "trsm f32");
+                if (mode == LNB_FACTOR_BF16)
+                    CK(lnb_k_prep_bf16(Akk + bs, lda, mrem, bs, (int)pb.kpad, pb.scale[slot], pb.hi[slot], crit),
+                       "prep bf16");
+            }
         }
         CK(cudaEventRecord(ev_trsm, crit), "event");
         if (mrem <= 0) break;

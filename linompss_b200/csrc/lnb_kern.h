@@ -84,6 +84,10 @@ int lnb_k_potrf_f32(float *A, int64_t lda, int bs, int64_t row0, float *dinv, ln
                     lnb_stream_t s);
 int lnb_k_trsm_rlt_f32(const float *L, int64_t lda, const float *dinv, float *B, int64_t ldb, int64_t m,
                        int bs, lnb_stream_t s);
+/* the same solve, also writing the K-major TF32 operand copies of the result
+ * (hi = rna_tf32(x); lo = x - hi when lo != NULL), rows of kpad elements */
+int lnb_k_trsm_rlt_prep_f32(const float *L, int64_t lda, const float *dinv, float *B, int64_t ldb, int64_t m,
+                            int bs, float *hi, float *lo, int kpad, lnb_stream_t s);
 int lnb_k_syrk_lower_f32_simt(const float *P, int64_t ldp, float *C, int64_t ldc, int64_t nrows,
                               int64_t c0, int64_t c1, int kdim, lnb_stream_t s);
 /* K-major operand copies of a solved panel X (m x kb, ld ldx): TF32 hi (and

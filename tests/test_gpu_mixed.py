@@ -38,7 +38,10 @@ def test_ir_well_conditioned(lnb, factor):
     B0 = np.asfortranarray(np.random.default_rng(1).standard_normal((n, 1)))
     X, res = check(lnb, A0, B0, b, getattr(lnb, factor))
     Xref = np.linalg.solve(A0, B0)
-    assert np.abs(X - Xref).max() / np.abs(Xref).max() <= 1e-10
+    # refinement stops at an inf-norm normwise backward error <= 10 n eps, so
+    # the forward error is bounded by cond_inf(A) times that (2x margin)
+    bound = 2 * np.linalg.cond(A0, np.inf) * 10 * n * EPS
+    assert np.abs(X - Xref).max() / np.abs(Xref).max() <= bound
     if factor in ("FACTOR_TF32X3", "FACTOR_FP32"):
         assert res["iterations"] <= 4 and not res["used_pcg"]
 
