@@ -432,7 +432,7 @@ def batched_arm(args, world, local, peaks):
             "frac_of_tf32_peak": round(tf / peaks["tf32"], 4),
             "per_system_loop_ms": round(t_loop, 3), "speedup_vs_per_system_launches": round(t_loop / t_batch, 2),
             "per_system_loop": "lnb_dposv_dev (plain FP64, b=128) once per system, same stream",
-            "launch": "one persistent launch in a CUDA graph, replayed", "panel_width": pw,
+            "launch": "one persistent launch in a CUDA graph, replayed", "cta_threads": pw,
             "max_backward_error_over_n_eps_sample64": round(worst, 4),
             "refinement_iterations": {"min": int(it.min()), "max": int(it.max()), "mean": round(float(it.mean()), 2)}}
 

@@ -326,6 +326,8 @@ def batched_posv_dev(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode=FAC
 
 def batched_autotune(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode=FACTOR_FP32, max_iter=10,
                      stream=None) -> int:
+    """Times the solver's CTA sizes on this batch, keeps the fastest for later
+    calls in this process and returns it (256 or 512 threads)."""
     args = _batched_args(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode, max_iter)
     return _chk(lib().lnb_batched_autotune(*args, _stream(stream)))
 

@@ -77,7 +77,7 @@ LNB_DEV bool wait_geq(const int *flag, int target, long long wait_ns, const lnb_
         if (ld_acquire(&st->timeout) != 0) return false;
         if ((long long)(globaltimer() - t0) > wait_ns) return false;
         __nanosleep(ns);
-        if (ns < 1024) ns <<= 1;
+        if (ns < 256) ns <<= 1;   // short cap: these waits sit on dependency chains
     }
 }
 

@@ -7,21 +7,28 @@
 // order (largest first), so the uneven sizes balance over the SMs; the whole
 // batch is one launch and can be captured in a CUDA graph.
 //
-// Per system (n <= 512, nrhs <= 8), in one CTA of BT threads:
-//   1. the lower triangle of A (FP64) is copied into the CTA's scratch factor
-//      F (type TF = float or double, ld n; L2-resident)
-//   2. right-looking Cholesky with PW-wide panels: the panel is staged in
-//      shared memory, warp 0 factors its diagonal block with shuffles, all
-//      threads solve the rows below and apply the rank-PW update to F
-//   3. x = 0, r = b; repeat: z = F^-T F^-1 r (blocked by PW rows), x += z,
-//      r = b - A x in FP64 from the original A; stop at backward error
+// Per system (n <= 512, nrhs <= 8), in one CTA of NT threads:
+//   1. the lower triangle of A (FP64) goes to the CTA's scratch factor F
+//      (type TF = float or double, 16-byte-aligned columns, L2-resident); the
+//      same pass forms ||A||_inf from the column sums of the lower part
+//   2. right-looking Cholesky in 32-column panels: the panel is staged in
+//      shared memory by cp.async, one warp factors its diagonal block
+//      left-looking and inverts it, the rows below become dot products with
+//      that inverse, and the trailing update runs 4 x 4 tiles per thread with
+//      16-byte loads, the C tile fetched before the products so its latency
+//      is hidden
+//   3. x = 0, r = b; repeat: z = F^-T F^-1 r (32-row blocks: coalesced partial
+//      sums over all warps, then the stored block inverse), x += z,
+//      r = b - A x in FP64 from the original A (rows x column groups, several
+//      loads in flight per thread); stop at backward error
 //      ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol, at most max_iter
-//      times (one pass, no refinement, when TF = double)
+//      times (one direct solve when TF = double)
 #include "common.cuh"
 
 namespace lnb {
 
-constexpr int BMAXN = 512, BMAXR = 8;
+constexpr int BMAXN = 512, BMAXR = 8, BP = 32;
+constexpr int BLDP = BMAXN + 4;           // stride of a staged panel column in shared memory
 
 struct BatchArgs {
     int count;
@@ -29,7 +36,7 @@ struct BatchArgs {
     const int64_t *a_off, *b_off;
     const double *A, *B;
     double *X;
-    void *scratch;            // per-CTA factor scratch: BMAXN * BMAXN elements each
+    void *scratch;            // per CTA: factor F (BMAXN x BMAXN) then BMAXN/32 inverse blocks (32 x 32)
     const int *order;         // processing order (cost-sorted)
     int *ticket;
     int *info, *iters;
@@ -37,211 +44,385 @@ struct BatchArgs {
     double tol_eps;           // tol = tol_eps * n
 };
 
-template <typename TF, int PW>
-__device__ int factor_one(TF *F, int n, const double *A, TF *Ps)
+template <typename TF>
+__host__ __device__ constexpr int64_t bscratch_elems() { return (int64_t)BMAXN * BMAXN + (int64_t)(BMAXN / BP) * BP * BP; }
+
+// shared-memory layout of one CTA (bytes)
+template <typename TF, int NT>
+struct BSmem {
+    static constexpr size_t P = sizeof(TF) * BP * BLDP;              // panel, P[c][r]
+    static constexpr size_t LI = sizeof(TF) * BP * (BP + 1);         // block inverse, Li[p][j] = inv[j][p]
+    static constexpr size_t RD = sizeof(TF) * BP;                     // 1 / diagonal
+    static constexpr size_t CS = sizeof(float) * BMAXN;               // column sums of |A|
+    static constexpr size_t XS = sizeof(double) * BMAXR * BMAXN;      // x
+    static constexpr size_t RS = sizeof(double) * BMAXR * BMAXN;      // r, z
+    static constexpr size_t RED = sizeof(double) * (NT / 32) * BP * BMAXR;
+    static constexpr size_t total = P + LI + RD + CS + XS + RS + RED;
+};
+
+// 16-byte cp.async from L2 copying `bytes` (0..16) and zero-filling the rest
+LNB_DEV void bcp16(void *smem, const void *gmem, int bytes)
 {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
-    __shared__ int fail;
-    if (tid == 0) fail = 0;
-    // lower triangle of A into F
-    for (int idx = tid; idx < n * n; idx += nt) {
-        const int c = idx / n, r = idx - c * n;
-        if (r >= c) F[r + c * n] = (TF)A[r + (int64_t)c * n];
-    }
-    __syncthreads();
-    constexpr int LDP = PW + 1;
-    for (int j0 = 0; j0 < n; j0 += PW) {
-        const int jb = min(PW, n - j0), mr = n - j0;
-        // stage the panel rows j0..n, cols j0..j0+jb
-        for (int idx = tid; idx < mr * jb; idx += nt) {
-            const int c = idx / mr, r = idx - c * mr;
-            Ps[r * LDP + c] = F[(j0 + r) + (j0 + c) * n];
-        }
-        __syncthreads();
-        if (warp == 0) {
-            TF x[PW];
-#pragma unroll
-            for (int c = 0; c < PW; ++c) x[c] = (lane < jb && c < jb && lane >= c) ? Ps[lane * LDP + c] : TF(0);
-            int bad = 0;
-#pragma unroll
-            for (int c = 0; c < PW; ++c) {
-                if (c < jb && !bad) {
-                    const TF d = __shfl_sync(0xffffffffu, x[c], c);
-                    if (!(d > TF(0))) {
-                        bad = j0 + c + 1;
-                    } else {
-                        const TF dd = sqrt(d);
-                        if (lane == c) x[c] = dd;
-                        else if (lane > c) x[c] = x[c] / dd;
-#pragma unroll
-                        for (int cc = c + 1; cc < PW; ++cc) {
-                            const TF l = __shfl_sync(0xffffffffu, x[c], cc);
-                            if (lane >= cc) x[cc] -= x[c] * l;
-                        }
-                    }
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < PW; ++c)
-                if (lane < jb && c < jb && lane >= c) Ps[lane * LDP + c] = x[c];
-            if (lane == 0 && bad) fail = bad;
-        }
-        __syncthreads();
-        if (fail) break;
-        for (int r = jb + tid; r < mr; r += nt) {
-            TF x[PW];
-#pragma unroll
-            for (int c = 0; c < PW; ++c) {
-                if (c < jb) {
-                    TF v = Ps[r * LDP + c];
-#pragma unroll
-                    for (int p = 0; p < c; ++p) v -= x[p] * Ps[c * LDP + p];
-                    x[c] = v / Ps[c * LDP + c];
-                    Ps[r * LDP + c] = x[c];
-                }
-            }
-        }
-        __syncthreads();
-        for (int idx = tid; idx < mr * jb; idx += nt) {
-            const int c = idx / mr, r = idx - c * mr;
-            if (r >= c) F[(j0 + r) + (j0 + c) * n] = Ps[r * LDP + c];
-        }
-        // trailing update of F (lower), 4x4 blocks per thread; loads before stores
-        const int t0 = jb, tr = mr - jb;
-        if (tr > 0) {
-            const int nb4 = (tr + 3) / 4, nblk = nb4 * (nb4 + 1) / 2;
-            for (int id = tid; id < nblk; id += nt) {
-                int bi = (int)((sqrtf(8.0f * id + 1.0f) - 1.0f) * 0.5f);
-                while (bi * (bi + 1) / 2 > id) --bi;
-                while ((bi + 1) * (bi + 2) / 2 <= id) ++bi;
-                const int bj = id - bi * (bi + 1) / 2;
-                const int ra = t0 + 4 * bi, rb = t0 + 4 * bj;
-                TF acc[4][4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] = TF(0);
-                for (int p = 0; p < jb; ++p) {
-                    TF a[4], bb[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) {
-                        a[i] = (ra + i < mr) ? Ps[(ra + i) * LDP + p] : TF(0);
-                        bb[i] = (rb + i < mr) ? Ps[(rb + i) * LDP + p] : TF(0);
-                    }
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
-                }
-                TF cv[4][4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int r = ra + i, c = rb + j;
-                        cv[i][j] = (r < mr && c < mr && r >= c) ? F[(j0 + r) + (j0 + c) * n] : TF(0);
-                    }
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int r = ra + i, c = rb + j;
-                        if (r < mr && c < mr && r >= c) F[(j0 + r) + (j0 + c) * n] = cv[i][j] - acc[i][j];
-                    }
-            }
-        }
-        __syncthreads();
-    }
-    __syncthreads();
-    return fail;   // block-uniform: every thread reads the shared flag after the barrier
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(smem)), "l"(gmem), "r"(bytes));
 }
 
-// z <- F^-T F^-1 z in place (z: n x nr doubles in shared memory, ld BMAXN).
-// Blocked by PW rows: the off-diagonal part of each block row is a sum split
-// over all threads (reduced in shared memory), the PW x PW triangle is one
-// thread per right-hand side.
-template <typename TF, int PW>
-__device__ void solve_one(const TF *F, int n, int nr, double *z, double *red)
+// sum_{p<len} a[p*sa] b[p*sb] with 8 loads of each operand in flight per step
+template <typename T>
+LNB_DEV T bdot(const T *a, int sa, const T *b, int sb, int len)
 {
-    const int tid = threadIdx.x, nt = blockDim.x, nparts = nt / PW;
-    for (int k0 = 0; k0 < n; k0 += PW) {              // forward: z_k -= L_k,0:k z_0:k
-        const int kb = min(PW, n - k0);
-        for (int q = 0; q < nr; ++q) {
-            const int i = tid % PW, part = tid / PW;
-            double s = 0.0;
-            if (i < kb)
-                for (int j = part; j < k0; j += nparts) s += (double)F[(k0 + i) + j * n] * z[j + q * BMAXN];
-            red[part * PW + i] = s;
-            __syncthreads();
-            if (tid < kb) {
-                double t = 0.0;
-                for (int p = 0; p < nparts; ++p) t += red[p * PW + tid];
-                z[(k0 + tid) + q * BMAXN] -= t;
-            }
-            __syncthreads();
-        }
-        if (tid < nr) {
-            const int q = tid;
-            for (int i = 0; i < kb; ++i) {
-                double s = z[(k0 + i) + q * BMAXN];
-                for (int j = 0; j < i; ++j) s -= (double)F[(k0 + i) + (k0 + j) * n] * z[(k0 + j) + q * BMAXN];
-                z[(k0 + i) + q * BMAXN] = s / (double)F[(k0 + i) + (k0 + i) * n];
-            }
-        }
-        __syncthreads();
+    T s0 = T(0), s1 = T(0), s2 = T(0), s3 = T(0);
+    int p = 0;
+    for (; p + 8 <= len; p += 8) {
+        T x[8], y[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) { x[e] = a[(p + e) * sa]; y[e] = b[(p + e) * sb]; }
+        s0 = fma(x[0], y[0], s0); s1 = fma(x[1], y[1], s1); s2 = fma(x[2], y[2], s2); s3 = fma(x[3], y[3], s3);
+        s0 = fma(x[4], y[4], s0); s1 = fma(x[5], y[5], s1); s2 = fma(x[6], y[6], s2); s3 = fma(x[7], y[7], s3);
     }
-    for (int k0 = ((n - 1) / PW) * PW; k0 >= 0; k0 -= PW) {   // backward: z_k -= L_{k+1:,k}^T z_{k+1:}
-        const int kb = min(PW, n - k0);
-        for (int q = 0; q < nr; ++q) {
-            const int part = tid % nparts, i = tid / nparts;   // consecutive threads -> consecutive j
-            double s = 0.0;
-            if (i < kb)
-                for (int j = k0 + kb + part; j < n; j += nparts) s += (double)F[j + (k0 + i) * n] * z[j + q * BMAXN];
-            red[part * PW + i] = s;
-            __syncthreads();
-            if (tid < kb) {
-                double t = 0.0;
-                for (int p = 0; p < nparts; ++p) t += red[p * PW + tid];
-                z[(k0 + tid) + q * BMAXN] -= t;
-            }
-            __syncthreads();
-        }
-        if (tid < nr) {
-            const int q = tid;
-            for (int i = kb - 1; i >= 0; --i) {
-                double s = z[(k0 + i) + q * BMAXN];
-                for (int j = i + 1; j < kb; ++j) s -= (double)F[(k0 + j) + (k0 + i) * n] * z[(k0 + j) + q * BMAXN];
-                z[(k0 + i) + q * BMAXN] = s / (double)F[(k0 + i) + (k0 + i) * n];
-            }
-        }
-        __syncthreads();
-    }
+    for (; p < len; ++p) s0 = fma(a[p * sa], b[p * sb], s0);
+    return (s0 + s1) + (s2 + s3);
 }
+LNB_DEV float brsqrt(float x) { return rsqrtf(x); }
+LNB_DEV double brsqrt(double x) { return rsqrt(x); }
 
-LNB_DEV double block_max(double v, double *red)
+template <int NT>
+LNB_DEV double bmax_block(double v, double *red)
 {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
     __syncthreads();
     if (lane == 0) red[warp] = v;
     __syncthreads();
     double m = 0.0;
-    for (int w = 0; w < nw; ++w) m = fmax(m, red[w]);
+    for (int w = 0; w < NT / 32; ++w) m = fmax(m, red[w]);
     __syncthreads();
     return m;
 }
 
-template <typename TF, int PW>
-__global__ void __launch_bounds__(256) k_batched_posv(BatchArgs a)
+// 4-element vector load/store of TF from 16-byte-aligned memory (FP32: one
+// float4; FP64: two double2)
+LNB_DEV void ld4(const float *p, float (&v)[4])
 {
+    const float4 q = *reinterpret_cast<const float4 *>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+LNB_DEV void ld4(const double *p, double (&v)[4])
+{
+    const double2 q0 = *reinterpret_cast<const double2 *>(p), q1 = *reinterpret_cast<const double2 *>(p + 2);
+    v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
+}
+LNB_DEV void ld4cg(const float *p, float (&v)[4])
+{
+    const float4 q = __ldcg(reinterpret_cast<const float4 *>(p));
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+}
+LNB_DEV void ld4cg(const double *p, double (&v)[4])
+{
+    const double2 q0 = __ldcg(reinterpret_cast<const double2 *>(p)), q1 = __ldcg(reinterpret_cast<const double2 *>(p + 2));
+    v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
+}
+
+// Right-looking Cholesky of the n x n system in F (lower, ld ldF, 16-byte
+// aligned columns), 32-column panels staged in shared memory.  Writes the
+// 32 x 32 inverses of the diagonal blocks to Dv (Dk[j*32+p] = inv[j][p]).
+// Returns info (0 or the 1-based first bad pivot), the same in every thread.
+template <typename TF, int NT>
+__device__ int bfactor(TF *F, int ldF, int n, TF *Dv, TF *P, TF *Li, TF *Rd, int *s_fail)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int V = 16 / (int)sizeof(TF);              // elements per 16-byte copy
+    if (tid == 0) *s_fail = 0;
+    for (int j0 = 0; j0 < n; j0 += BP) {
+        const int jb = min(BP, n - j0), mr = n - j0;
+        // stage P[c][r] = F[(j0 + r) + (j0 + c) ldF], r < mr, c < jb
+        const int nch = (mr + V - 1) / V;
+        for (int idx = tid; idx < jb * nch; idx += NT) {
+            const int c = idx / nch, r = (idx - c * nch) * V;
+            const int nv = min(V, mr - r);
+            bcp16(P + c * BLDP + r, F + (j0 + r) + (int64_t)(j0 + c) * ldF, nv * (int)sizeof(TF));
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        if (warp == 0) {
+            // diagonal block, left-looking (potf2 order); lane l owns row l
+            const int rl = lane < jb ? lane : 0;
+            int bad = -1;
+            for (int c = 0; c < jb; ++c) {
+                const TF sv = P[c * BLDP + rl] - bdot(P + rl, BLDP, P + c, BLDP, c);
+                const TF d = __shfl_sync(0xffffffffu, sv, c);
+                if (!(d > TF(0))) { bad = c; break; }
+                const TF inv = brsqrt(d);
+                if (lane == c) { P[c * BLDP + c] = d * inv; Rd[c] = inv; }
+                else if (lane > c && lane < jb) P[c * BLDP + lane] = sv * inv;
+                __syncwarp();
+            }
+            if (lane == 0 && bad >= 0) *s_fail = j0 + bad + 1;
+            if (bad < 0) {
+                // inverse of the block: lane c builds column c, Li[c][*] = inv[*][c]
+                TF *Xc = Li + lane * (BP + 1);
+                for (int r = 0; r < BP; ++r) {
+                    TF v = (r == lane) ? TF(1) : TF(0);
+                    if (r < jb) v = (v - bdot(P + r, BLDP, Xc, 1, r)) * Rd[r];
+                    Xc[r] = v;
+                }
+                __syncwarp();
+                TF *Dk = Dv + (int64_t)(j0 / BP) * BP * BP;
+                for (int r = 0; r < BP; ++r) Dk[r * BP + lane] = Li[lane * (BP + 1) + r];
+            }
+        }
+        __syncthreads();
+        if (*s_fail) break;
+        // rows below the block: x_r = b_r inv^T, 4 threads per row
+        const int g = tid & 3;
+        for (int rb = jb; rb < mr; rb += NT / 4) {
+            const int r = rb + (tid >> 2);
+            const bool act = r < mr;
+            TF bv[BP];
+#pragma unroll
+            for (int p = 0; p < BP; ++p) bv[p] = (act && p < jb) ? P[p * BLDP + r] : TF(0);
+            __syncwarp();
+#pragma unroll
+            for (int s = 0; s < BP / 4; ++s) {
+                const int j = g + 4 * s;
+                TF acc = TF(0);
+#pragma unroll
+                for (int p = 0; p < BP; ++p) acc = fma(bv[p], Li[p * (BP + 1) + j], acc);
+                if (act && j < jb) P[j * BLDP + r] = acc;
+            }
+        }
+        __syncthreads();
+        // the finished panel back to F (16-byte runs; rows above the diagonal get
+        // unused values)
+        for (int idx = tid; idx < jb * nch; idx += NT) {
+            const int c = idx / nch, r = (idx - c * nch) * V;
+            TF *dst = F + (j0 + r) + (int64_t)(j0 + c) * ldF;
+            if (r + V <= mr) {
+                if constexpr (V == 4) *reinterpret_cast<float4 *>(dst) = *reinterpret_cast<const float4 *>(P + c * BLDP + r);
+                else *reinterpret_cast<double2 *>(dst) = *reinterpret_cast<const double2 *>(P + c * BLDP + r);
+            } else {
+                for (int e = 0; r + e < mr; ++e) dst[e] = P[c * BLDP + r + e];
+            }
+        }
+        // trailing update F[r][c] -= sum_p P[p][r] P[p][c], jb <= c <= r < mr (relative), 4x4 per thread
+        const int tr = mr - jb;
+        if (tr > 0) {
+            const int nb4 = (tr + 3) / 4, nblk = nb4 * (nb4 + 1) / 2;
+            for (int id = tid; id < nblk; id += NT) {
+                int bi = (int)((sqrtf(8.0f * id + 1.0f) - 1.0f) * 0.5f);
+                while (bi * (bi + 1) / 2 > id) --bi;
+                while ((bi + 1) * (bi + 2) / 2 <= id) ++bi;
+                const int bj = id - bi * (bi + 1) / 2;
+                const int ra = jb + 4 * bi, rc = jb + 4 * bj;
+                // C tile first (its loads overlap the products below)
+                TF cv[4][4];
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) {
+                    if (rc + jj < mr) ld4cg(F + (j0 + ra) + (int64_t)(j0 + rc + jj) * ldF, cv[jj]);
+                    else cv[jj][0] = cv[jj][1] = cv[jj][2] = cv[jj][3] = TF(0);
+                }
+                TF acc[4][4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int jj = 0; jj < 4; ++jj) acc[i][jj] = TF(0);
+#pragma unroll 8
+                for (int p = 0; p < BP; ++p) {
+                    TF av[4], cvv[4];
+                    ld4(P + p * BLDP + ra, av);
+                    ld4(P + p * BLDP + rc, cvv);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int jj = 0; jj < 4; ++jj) acc[i][jj] = fma(av[i], cvv[jj], acc[i][jj]);
+                }
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) {
+                    const int c = rc + jj;
+                    if (c >= mr) continue;
+                    TF *col = F + (j0 + ra) + (int64_t)(j0 + c) * ldF;
+                    if (bi != bj && ra + 4 <= mr) {
+                        TF o[4];
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) o[i] = cv[jj][i] - acc[i][jj];
+                        if constexpr (V == 4) *reinterpret_cast<float4 *>(col) = make_float4(o[0], o[1], o[2], o[3]);
+                        else {
+                            *reinterpret_cast<double2 *>(col) = make_double2(o[0], o[1]);
+                            *reinterpret_cast<double2 *>(col + 2) = make_double2(o[2], o[3]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                            if (ra + i < mr && ra + i >= c) col[i] = cv[jj][i] - acc[i][jj];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    return *s_fail;
+}
+
+// z <- inv(L) z, then z <- inv(L^T) z, for nr columns of z in shared memory
+// (z[q * BMAXN + i]); L in F, the block inverses in Dv.
+template <typename TF, int NT>
+__device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double *z, double *red)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = NT / 32;
+    static_assert(BMAXR <= NW, "one warp per right-hand side in the block-inverse steps");
+    const int nblk = (n + BP - 1) / BP;
+    // forward
+    for (int kb = 0; kb < nblk; ++kb) {
+        const int k0 = kb * BP, kn = min(BP, n - k0);
+        if (k0 > 0) {
+            double acc[BMAXR];
+#pragma unroll
+            for (int q = 0; q < BMAXR; ++q) acc[q] = 0.0;
+            if (lane < kn) {
+#pragma unroll 4
+                for (int c = warp; c < k0; c += NW) {
+                    const double f = (double)__ldcg(F + (k0 + lane) + (int64_t)c * ldF);
+#pragma unroll
+                    for (int q = 0; q < BMAXR; ++q)
+                        if (q < nr) acc[q] = fma(f, z[q * BMAXN + c], acc[q]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < BMAXR; ++q) red[(warp * BP + lane) * BMAXR + q] = acc[q];
+            __syncthreads();
+            for (int t = tid; t < kn * nr; t += NT) {
+                const int i = t / nr, q = t - i * nr;
+                double s = 0.0;
+                for (int w = 0; w < NW; ++w) s += red[(w * BP + i) * BMAXR + q];
+                z[q * BMAXN + k0 + i] -= s;
+            }
+            __syncthreads();
+        }
+        // z_blk = inv(L_kk) z_blk: thread (j, q), j = row of the block, q = rhs
+        const TF *Dk = Dv + (int64_t)kb * BP * BP;
+        const int j = tid & 31, q = tid >> 5;
+        const bool act = j < kn && q < nr;
+        double v = 0.0;
+        if (act)
+            for (int p = 0; p <= j; ++p) v = fma((double)__ldcg(Dk + j * BP + p), z[q * BMAXN + k0 + p], v);
+        __syncthreads();
+        if (act) z[q * BMAXN + k0 + j] = v;
+        __syncthreads();
+    }
+    // backward
+    for (int kb = nblk - 1; kb >= 0; --kb) {
+        const int k0 = kb * BP, kn = min(BP, n - k0), r0 = k0 + kn;
+        if (r0 < n) {
+            for (int jc = warp; jc < kn; jc += NW) {
+                double acc[BMAXR];
+#pragma unroll
+                for (int q = 0; q < BMAXR; ++q) acc[q] = 0.0;
+                const TF *col = F + (int64_t)(k0 + jc) * ldF;
+#pragma unroll 4
+                for (int r = r0 + lane; r < n; r += 32) {
+                    const double f = (double)__ldcg(col + r);
+#pragma unroll
+                    for (int q = 0; q < BMAXR; ++q)
+                        if (q < nr) acc[q] = fma(f, z[q * BMAXN + r], acc[q]);
+                }
+#pragma unroll
+                for (int q = 0; q < BMAXR; ++q) {
+                    double v = acc[q];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+                    if (lane == 0) red[jc * BMAXR + q] = v;
+                }
+            }
+            __syncthreads();
+            for (int t = tid; t < kn * nr; t += NT) {
+                const int i = t / nr, q = t - i * nr;
+                z[q * BMAXN + k0 + i] -= red[i * BMAXR + q];
+            }
+            __syncthreads();
+        }
+        // z_blk = inv(L_kk)^T z_blk
+        const TF *Dk = Dv + (int64_t)kb * BP * BP;
+        const int j = tid & 31, q = tid >> 5;
+        const bool act = j < kn && q < nr;
+        double v = 0.0;
+        if (act)
+            for (int p = j; p < kn; ++p) v = fma((double)__ldcg(Dk + p * BP + j), z[q * BMAXN + k0 + p], v);
+        __syncthreads();
+        if (act) z[q * BMAXN + k0 + j] = v;
+        __syncthreads();
+    }
+}
+
+// r = b - A x (A full symmetric n x n, FP64) for nr columns; returns the max
+// over columns of ||r||_inf / (anorm ||x||_inf + ||b||_inf), same in every thread
+template <int NT>
+__device__ double bresidual(const double *A, int n, int nr, const double *B, const double *x, double *r,
+                            double anorm, double *red)
+{
+    const int tid = threadIdx.x;
+    constexpr int CG = NT / 64;            // column groups
+    const int i0 = tid & 63, cg = tid >> 6;
+    for (int rb = 0; rb < n; rb += 64) {
+        const int i = rb + i0;
+        double acc[BMAXR];
+#pragma unroll
+        for (int q = 0; q < BMAXR; ++q) acc[q] = 0.0;
+        if (i < n) {
+#pragma unroll 4
+            for (int c = cg; c < n; c += CG) {
+                const double a = __ldg(A + i + (int64_t)c * n);
+#pragma unroll
+                for (int q = 0; q < BMAXR; ++q)
+                    if (q < nr) acc[q] = fma(a, x[q * BMAXN + c], acc[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < BMAXR; ++q) red[(cg * 64 + i0) * BMAXR + q] = acc[q];
+        __syncthreads();
+        for (int t = tid; t < 64 * nr; t += NT) {
+            const int ii = t / nr, q = t - ii * nr;
+            if (rb + ii < n) {
+                double s = 0.0;
+                for (int g = 0; g < CG; ++g) s += red[(g * 64 + ii) * BMAXR + q];
+                r[q * BMAXN + rb + ii] = B[(rb + ii) + (int64_t)q * n] - s;
+            }
+        }
+        __syncthreads();
+    }
+    double worst = 0.0;
+    for (int q = 0; q < nr; ++q) {
+        double rm = 0.0, xm = 0.0, bm = 0.0;
+        for (int i = tid; i < n; i += NT) {
+            rm = fmax(rm, fabs(r[q * BMAXN + i]));
+            xm = fmax(xm, fabs(x[q * BMAXN + i]));
+            bm = fmax(bm, fabs(B[i + (int64_t)q * n]));
+        }
+        rm = bmax_block<NT>(rm, red);
+        xm = bmax_block<NT>(xm, red);
+        bm = bmax_block<NT>(bm, red);
+        const double den = anorm * xm + bm;
+        worst = fmax(worst, den > 0.0 ? rm / den : 0.0);
+    }
+    return worst;
+}
+
+template <typename TF, int NT>
+__global__ void __launch_bounds__(NT) k_batched_posv(BatchArgs a)
+{
+    using SM = BSmem<TF, NT>;
     extern __shared__ __align__(16) unsigned char smb[];
-    double *x = (double *)smb;                     // [BMAXR][BMAXN]
-    double *r = x + BMAXR * BMAXN;                 // [BMAXR][BMAXN]
-    TF *Ps = (TF *)(r + BMAXR * BMAXN);            // panel [BMAXN][PW+1]
-    __shared__ double red[256];
-    __shared__ int s_item;
-    TF *F = (TF *)a.scratch + (int64_t)blockIdx.x * BMAXN * BMAXN;
-    const int tid = threadIdx.x, nt = blockDim.x;
+    TF *P = (TF *)smb;
+    TF *Li = (TF *)(smb + SM::P);
+    TF *Rd = (TF *)(smb + SM::P + SM::LI);
+    float *colsum = (float *)(smb + SM::P + SM::LI + SM::RD);
+    double *xs = (double *)(smb + SM::P + SM::LI + SM::RD + SM::CS);
+    double *rs = (double *)((unsigned char *)xs + SM::XS);
+    double *red = (double *)((unsigned char *)rs + SM::RS);
+    __shared__ int s_item, s_fail;
+    TF *F = (TF *)a.scratch + (int64_t)blockIdx.x * bscratch_elems<TF>();
+    TF *Dv = F + (int64_t)BMAXN * BMAXN;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     while (true) {
         if (tid == 0) s_item = atomicAdd(a.ticket, 1);
         __syncthreads();
@@ -261,58 +442,54 @@ __global__ void __launch_bounds__(256) k_batched_posv(BatchArgs a)
         const double *A = a.A + a.a_off[sys];
         const double *B = a.B + a.b_off[sys];
         double *Xo = a.X + a.b_off[sys];
-        const int info = factor_one<TF, PW>(F, n, A, Ps);   // same value in every thread
+        const int ldF = (n + 3) & ~3;
+        // F = lower(A) in TF, and the column sums of |A| (= row sums) from the lower part
+        for (int i = tid; i < n; i += NT) colsum[i] = 0.f;
         __syncthreads();
+        for (int c = warp; c < n; c += NT / 32) {
+            float sc = 0.f;
+#pragma unroll 4
+            for (int r = c + lane; r < n; r += 32) {
+                const double v = __ldg(A + r + (int64_t)c * n);
+                F[r + (int64_t)c * ldF] = (TF)v;
+                const float av = (float)fabs(v);
+                sc += av;
+                if (r > c) atomicAdd(&colsum[r], av);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) sc += __shfl_down_sync(0xffffffffu, sc, o);
+            if (lane == 0) atomicAdd(&colsum[c], sc);
+        }
+        __syncthreads();
+        const int info = bfactor<TF, NT>(F, ldF, n, Dv, P, Li, Rd, &s_fail);
         int it = 0;
         if (info == 0) {
-            // ||A||_inf (full symmetric storage) and ||b||_inf per rhs
-            double amax = 0.0;
-            for (int i = tid; i < n; i += nt) {
-                double s = 0.0;
-                for (int j = 0; j < n; ++j) s += fabs(A[i + (int64_t)j * n]);
-                amax = fmax(amax, s);
-            }
-            const double anorm = block_max(amax, red);
-            for (int idx = tid; idx < BMAXR * BMAXN; idx += nt) x[idx] = 0.0;
-            for (int idx = tid; idx < n * nr; idx += nt) {
-                const int i = idx % n, q = idx / n;
-                r[i + q * BMAXN] = B[i + (int64_t)q * n];
+            double am = 0.0;
+            for (int i = tid; i < n; i += NT) am = fmax(am, (double)colsum[i]);
+            const double anorm = bmax_block<NT>(am, red);
+            for (int t = tid; t < BMAXR * BMAXN; t += NT) xs[t] = 0.0;
+            for (int t = tid; t < n * nr; t += NT) {
+                const int i = t % n, q = t / n;
+                rs[q * BMAXN + i] = B[i + (int64_t)q * n];
             }
             __syncthreads();
             const double tol = a.tol_eps * n;
             const int maxit = (sizeof(TF) == 8) ? 1 : a.max_iter;
             for (it = 1; it <= maxit; ++it) {
-                solve_one<TF, PW>(F, n, nr, r, red);                  // r <- M^-1 r
-                for (int idx = tid; idx < n * nr; idx += nt) {
-                    const int i = idx % n, q = idx / n;
-                    x[i + q * BMAXN] += r[i + q * BMAXN];
+                bsolve<TF, NT>(F, ldF, Dv, n, nr, rs, red);           // r <- M^-1 r
+                for (int t = tid; t < n * nr; t += NT) {
+                    const int i = t % n, q = t / n;
+                    xs[q * BMAXN + i] += rs[q * BMAXN + i];
                 }
                 __syncthreads();
-                // r = b - A x  (FP64), with ||r||, ||x||, ||b|| per rhs
-                double worst = 0.0;
-                for (int q = 0; q < nr; ++q) {
-                    double rm = 0.0, xm = 0.0, bm = 0.0;
-                    for (int i = tid; i < n; i += nt) {
-                        double s = B[i + (int64_t)q * n];
-                        bm = fmax(bm, fabs(s));
-                        for (int j = 0; j < n; ++j) s -= A[i + (int64_t)j * n] * x[j + q * BMAXN];
-                        r[i + q * BMAXN] = s;
-                        rm = fmax(rm, fabs(s));
-                        xm = fmax(xm, fabs(x[i + q * BMAXN]));
-                    }
-                    rm = block_max(rm, red);
-                    xm = block_max(xm, red);
-                    bm = block_max(bm, red);
-                    const double den = anorm * xm + bm;
-                    const double be = den > 0.0 ? rm / den : 0.0;
-                    worst = fmax(worst, be);
-                }
+                if (it == maxit && sizeof(TF) == 8) break;             // FP64 factor: one direct solve
+                const double worst = bresidual<NT>(A, n, nr, B, xs, rs, anorm, red);
                 if (worst <= tol) break;
             }
             if (it > maxit) it = maxit;
-            for (int idx = tid; idx < n * nr; idx += nt) {
-                const int i = idx % n, q = idx / n;
-                Xo[i + (int64_t)q * n] = x[i + q * BMAXN];
+            for (int t = tid; t < n * nr; t += NT) {
+                const int i = t % n, q = t / n;
+                Xo[i + (int64_t)q * n] = xs[q * BMAXN + i];
             }
         }
         if (tid == 0) {
@@ -364,42 +541,33 @@ extern "C" int lnb_k_batch_order(int count, const int *n, int *order, lnb_stream
 
 extern "C" size_t lnb_batched_scratch_bytes(int grid, int fp64)
 {
-    return (size_t)grid * BMAXN * BMAXN * (fp64 ? 8 : 4);
+    return (size_t)grid * (fp64 ? bscratch_elems<double>() * 8 : bscratch_elems<float>() * 4);
 }
 
+template <typename TF, int NT>
+static void launch_batched(const BatchArgs &a, int grid, lnb_stream_t s)
+{
+    const int smem = (int)BSmem<TF, NT>::total;
+    cudaFuncSetAttribute(k_batched_posv<TF, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_batched_posv<TF, NT><<<grid, NT, smem, s>>>(a);
+}
+
+// variant: CTA size, 256 or 512 threads (512 in FP32 mode only)
 extern "C" int lnb_k_batched_posv(int count, const int *n, const int *nrhs, const int64_t *a_off,
                                   const int64_t *b_off, const double *A, const double *B, double *X, void *scratch,
                                   int grid, const int *order, int *ticket, int *info, int *iters, int max_iter,
-                                  int fp64, int pw, lnb_stream_t s)
+                                  int fp64, int variant, lnb_stream_t s)
 {
     BatchArgs a;
     a.count = count; a.n = n; a.nrhs = nrhs; a.a_off = a_off; a.b_off = b_off; a.A = A; a.B = B; a.X = X;
     a.scratch = scratch; a.order = order; a.ticket = ticket; a.info = info; a.iters = iters;
     a.max_iter = max_iter; a.tol_eps = 10.0 * 1.1102230246251565e-16;
+    if ((uintptr_t)scratch % 16) return (int)cudaErrorMisalignedAddress;
     cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(int), s);
     if (e != cudaSuccess) return (int)e;
-    const size_t vec = 2 * BMAXR * BMAXN * sizeof(double);
-    if (fp64) {
-        if (pw == 32) {
-            const int smem = (int)(vec + BMAXN * 33 * sizeof(double));
-            cudaFuncSetAttribute(k_batched_posv<double, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            k_batched_posv<double, 32><<<grid, 256, smem, s>>>(a);
-        } else {
-            const int smem = (int)(vec + BMAXN * 17 * sizeof(double));
-            cudaFuncSetAttribute(k_batched_posv<double, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            k_batched_posv<double, 16><<<grid, 256, smem, s>>>(a);
-        }
-    } else {
-        if (pw == 32) {
-            const int smem = (int)(vec + BMAXN * 33 * sizeof(float));
-            cudaFuncSetAttribute(k_batched_posv<float, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            k_batched_posv<float, 32><<<grid, 256, smem, s>>>(a);
-        } else {
-            const int smem = (int)(vec + BMAXN * 17 * sizeof(float));
-            cudaFuncSetAttribute(k_batched_posv<float, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-            k_batched_posv<float, 16><<<grid, 256, smem, s>>>(a);
-        }
-    }
+    if (fp64) launch_batched<double, 256>(a, grid, s);
+    else if (variant == 512) launch_batched<float, 512>(a, grid, s);
+    else launch_batched<float, 256>(a, grid, s);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }

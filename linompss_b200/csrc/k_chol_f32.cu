@@ -28,23 +28,26 @@ LNB_DEV float tf32_rna(float x)
 }
 
 // ------------------------------------------------------------------------
-// panel solve X = B L^-T, FP32 SIMT.  One CTA owns 32 rows of the panel and
-// keeps them (B, then X) in shared memory for the whole solve; L streams in
-// 32 x 32 blocks by cp.async, double-buffered (all CTAs read the same L, so
-// it is served from L2).  Left-looking over 32-column blocks j:
+// panel solve X = B L^-T, FP32 SIMT.  A CTA owns 32 rows of the panel and
+// walks its 32-column blocks left-looking:
 //     acc = B_j - sum_{kc<j} X_kc L_{j,kc}^T ;   X_j = acc Dinv_j^T
-// with Dinv_j the leaf's inverse of the j-th 32 x 32 diagonal block.
-// 64 threads, 4 rows x 4 columns of each block per thread (16-byte shared loads).
+// with Dinv_j the leaf's inverse of the j-th 32 x 32 diagonal block.  Each
+// (j, kc) chunk stages the L block and the CTA's finished X block (written
+// back to B, read again from L2) by cp.async, double-buffered; block starts
+// also stage B_j and Dinv_j.  Keeping only the chunk in shared memory (not
+// all of X) lets several CTAs share an SM.  64 threads, 4 rows x 4 columns of
+// each block per thread, operands by 16-byte shared loads.
 // ------------------------------------------------------------------------
 namespace ptrsm {
-constexpr int LDB = 36;   // padded row of the L / Dinv / T staging blocks
+constexpr int LDB = 36;   // padded row of the staged L / Dinv / T blocks
 constexpr int NT = 64;    // threads per CTA
 }
 
+// dst[k][c] = L[32 j + c][32 kc + k]
 LNB_DEV void ptrsm_stage_L(float *dst, const float *L, int64_t lda, int bs, int j, int kc, bool vec, int tid)
 {
     for (int idx = tid; idx < 32 * 8; idx += ptrsm::NT) {
-        const int k = idx >> 3, c4 = (idx & 7) * 4;   // dst[k][c] = L[32 j + c][32 kc + k]
+        const int k = idx >> 3, c4 = (idx & 7) * 4;
         float *d = dst + k * ptrsm::LDB + c4;
         const int row = 32 * j + c4;
         const float *g = L + row + (int64_t)(32 * kc + k) * lda;
@@ -60,11 +63,32 @@ LNB_DEV void ptrsm_stage_L(float *dst, const float *L, int64_t lda, int bs, int 
         }
     }
 }
+// dst[q][c] = Dinv_j[c][q] = dinv[j][c + 32 q]
 LNB_DEV void ptrsm_stage_D(float *dst, const float *dinv, int j, int tid)
 {
     for (int idx = tid; idx < 32 * 8; idx += ptrsm::NT) {
-        const int q = idx >> 3, c4 = (idx & 7) * 4;   // dst[q][c] = Dinv_j[c][q] = dinv[j][c + 32 q]
+        const int q = idx >> 3, c4 = (idx & 7) * 4;
         cp_async16(dst + q * ptrsm::LDB + c4, dinv + (int64_t)j * 1024 + c4 + 32 * q, true);
+    }
+}
+// dst[k][r] = B[r0 + r][32 kb + k] (rows past m and columns past bs read as 0).
+// From L2 (.cg) when 16-byte aligned; otherwise synchronous L2 loads.
+LNB_DEV void ptrsm_stage_B(float *dst, const float *B, int64_t ldb, int64_t m, int bs, int64_t r0, int kb,
+                           bool vecB, int tid)
+{
+    for (int idx = tid; idx < 32 * 8; idx += ptrsm::NT) {
+        const int k = idx >> 3, r4 = (idx & 7) * 4;
+        float *d = dst + k * 32 + r4;
+        const float *g = B + (r0 + r4) + (int64_t)(32 * kb + k) * ldb;
+        const int64_t nv64 = (32 * kb + k < bs) ? m - (r0 + r4) : 0;
+        const int nv = nv64 < 0 ? 0 : (nv64 > 4 ? 4 : (int)nv64);
+        if (vecB) {
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(d)), "l"(nv ? g : B),
+                         "r"(4 * nv));
+        } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) d[e] = e < nv ? __ldcg(g + e) : 0.f;
+        }
     }
 }
 
@@ -83,57 +107,27 @@ __global__ void __launch_bounds__(64) k_trsm_rlt_f32(const float *__restrict__ L
                                                      const float *__restrict__ dinv, float *B, int64_t ldb,
                                                      int64_t m, int bs, int vec, float *hi, float *lo, int kpad)
 {
-    extern __shared__ __align__(16) float smf[];
+    __shared__ __align__(16) float Xc[2][32 * 32];          // staged X_kc, [k][r]
+    __shared__ __align__(16) float Lc[2][32 * ptrsm::LDB];  // staged L_{j,kc}, [k][c]
+    __shared__ __align__(16) float Ds[2][32 * ptrsm::LDB];  // Dinv_j, [q][c]
+    __shared__ __align__(16) float Bs[2][32 * 32];          // B_j, [k][r]
+    __shared__ __align__(16) float Ts[32 * ptrsm::LDB];     // acc transposed, [q][r]
     using ptrsm::LDB;
     using ptrsm::NT;
     const int nj = (bs + 31) / 32;
-    float *Xs = smf;                      // Xs[k * 32 + r]: column k of the CTA's rows (B, then X)
-    float *Lc = Xs + nj * 32 * 32;        // [2][32][LDB]
-    float *Ds = Lc + 2 * 32 * LDB;        // [2][32][LDB]
-    float *Ts = Ds + 2 * 32 * LDB;        // [32][LDB]: Ts[q][r] = acc[r][q]
     const int tid = threadIdx.x, rq = tid & 7, cg = tid >> 3;   // rows 4rq..4rq+3, columns 4cg..4cg+3
     const int64_t r0 = (int64_t)blockIdx.x * 32;
-    // the CTA's rows arrive by cp.async (16-byte runs of 4 rows when aligned),
-    // all in flight at once, in the same group as the first inverse block
     const bool vecB = ((uintptr_t)B % 16 == 0) && (ldb % 4 == 0);
-    for (int idx = tid; idx < nj * 32 * 8; idx += NT) {
-        const int k = idx >> 3, r4 = (idx & 7) * 4;
-        float *d = Xs + k * 32 + r4;
-        const float *g = B + (r0 + r4) + (int64_t)k * ldb;
-        const int64_t nv64 = (k < bs) ? m - (r0 + r4) : 0;
-        const int nv = nv64 < 0 ? 0 : (nv64 > 4 ? 4 : (int)nv64);
-        if (vecB) {
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(d)),
-                         "l"(nv ? g : B), "r"(4 * nv));
-        } else {
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                if (e < nv) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(d + e)),
-                                         "l"(g + e));
-                else d[e] = 0.f;
-            }
-        }
-    }
-    const int S = nj * (nj - 1) / 2;      // chunks (j, kc), kc < j, in j-major order
-    ptrsm_stage_D(Ds, dinv, 0, tid);
-    cp_async_commit();
-    if (S > 0) {
-        ptrsm_stage_L(Lc, L, lda, bs, 1, 0, vec, tid);
-        ptrsm_stage_D(Ds + 32 * LDB, dinv, 1, tid);
-    }
-    cp_async_commit();
-    cp_async_wait<1>();
-    __syncthreads();
 
     float acc[4][4];
-    // X_j = acc Dinv_j^T, written to Xs, to B and (optionally) as TF32 operands
+    // X_j = acc Dinv_j^T, written to B and (optionally) as TF32 operands
     auto finish = [&](int j) {
 #pragma unroll
         for (int c = 0; c < 4; ++c)
             *reinterpret_cast<float4 *>(Ts + (4 * cg + c) * LDB + 4 * rq) =
                 make_float4(acc[0][c], acc[1][c], acc[2][c], acc[3][c]);
         __syncthreads();
-        const float *D = Ds + (j & 1) * 32 * LDB;
+        const float *D = Ds[j & 1];
         float y[4][4] = {};
 #pragma unroll 8
         for (int q = 0; q < 32; ++q)
@@ -142,13 +136,11 @@ __global__ void __launch_bounds__(64) k_trsm_rlt_f32(const float *__restrict__ L
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int col = 32 * j + 4 * cg + c;
-            *reinterpret_cast<float4 *>(Xs + col * 32 + 4 * rq) = make_float4(y[0][c], y[1][c], y[2][c], y[3][c]);
             if (col < bs)
 #pragma unroll
                 for (int i = 0; i < 4; ++i)
                     if (r0 + 4 * rq + i < m) B[(r0 + 4 * rq + i) + (int64_t)col * ldb] = y[i][c];
         }
-        // fused operand prep for the tensor-core update: K-major TF32 hi (+ lo)
         const int col0 = 32 * j + 4 * cg;
         if (hi != nullptr && col0 < kpad) {
 #pragma unroll
@@ -169,26 +161,45 @@ __global__ void __launch_bounds__(64) k_trsm_rlt_f32(const float *__restrict__ L
     auto load_b = [&](int j) {
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-            const float4 v = *reinterpret_cast<const float4 *>(Xs + (32 * j + 4 * cg + c) * 32 + 4 * rq);
+            const float4 v = *reinterpret_cast<const float4 *>(Bs[j & 1] + (4 * cg + c) * 32 + 4 * rq);
             acc[0][c] = v.x; acc[1][c] = v.y; acc[2][c] = v.z; acc[3][c] = v.w;
         }
     };
+    // chunk (j, kc): the L block and X_kc; a block's first chunk also brings B_j and Dinv_j
+    auto stage_chunk = [&](int buf, int j, int kc) {
+        ptrsm_stage_L(Lc[buf], L, lda, bs, j, kc, vec, tid);
+        ptrsm_stage_B(Xc[buf], B, ldb, m, bs, r0, kc, vecB, tid);
+        if (kc == 0) {
+            ptrsm_stage_B(Bs[j & 1], B, ldb, m, bs, r0, j, vecB, tid);
+            ptrsm_stage_D(Ds[j & 1], dinv, j, tid);
+        }
+    };
+
+    // block 0: B_0 and Dinv_0, then X_0
+    ptrsm_stage_B(Bs[0], B, ldb, m, bs, r0, 0, vecB, tid);
+    ptrsm_stage_D(Ds[0], dinv, 0, tid);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
     load_b(0);
     finish(0);
+    __syncthreads();                      // X_0 is in B before chunk (1, 0) reads it back
+    const int S = nj * (nj - 1) / 2;      // chunks (j, kc), kc < j, in j-major order
+    if (S > 0) stage_chunk(0, 1, 0);
+    cp_async_commit();
     int j = 1, kc = 0;
     for (int s = 0; s < S; ++s) {
         int jn = j, kn = kc + 1;
         if (kn == jn) { ++jn; kn = 0; }
-        if (s + 1 < S) {
-            ptrsm_stage_L(Lc + ((s + 1) & 1) * 32 * LDB, L, lda, bs, jn, kn, vec, tid);
-            if (kn == 0) ptrsm_stage_D(Ds + (jn & 1) * 32 * LDB, dinv, jn, tid);
-        }
+        // the next chunk's X block is finished: chunk (j', j'-1) is first staged one
+        // chunk after block j'-1's finish (for j' >= 2), and (1, 0) above
+        if (s + 1 < S) stage_chunk((s + 1) & 1, jn, kn);
         cp_async_commit();
         cp_async_wait<1>();
         __syncthreads();
         if (kc == 0) load_b(j);
-        const float *Lb = Lc + (s & 1) * 32 * LDB;
-        const float *Xk = Xs + 32 * kc * 32;
+        const float *Lb = Lc[s & 1];
+        const float *Xk = Xc[s & 1];
 #pragma unroll 8
         for (int k = 0; k < 32; ++k)
             fma4x4(acc, *reinterpret_cast<const float4 *>(Xk + k * 32 + 4 * rq),
@@ -217,32 +228,60 @@ __global__ void __launch_bounds__(256) k_syrk_lower_f32_simt(const float *__rest
                                                              int64_t ldc, int64_t nrows, int64_t c0, int64_t c1,
                                                              int kdim)
 {
-    __shared__ float As[16][68], Bs[16][68];
+    // K in chunks of 32, staged by cp.async and double-buffered
+    __shared__ __align__(16) float As[2][32][68], Bs[2][32][68];
     const int64_t rbase = c0 + (int64_t)blockIdx.y * 64, cbase = c0 + (int64_t)blockIdx.x * 64;
     if (rbase + 64 <= cbase || rbase >= nrows || cbase >= c1) return;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    float acc[4][4] = {};
-    for (int k0 = 0; k0 < kdim; k0 += 16) {
-        for (int idx = threadIdx.x; idx < 16 * 64; idx += 256) {
-            const int kk = idx >> 6, mm = idx & 63;
+    const bool vec = ((uintptr_t)P % 16 == 0) && (ldp % 4 == 0) && (rbase % 4 == 0) && (cbase % 4 == 0);
+    auto stage = [&](int buf, int k0) {
+        for (int idx = threadIdx.x; idx < 32 * 16; idx += 256) {
+            const int kk = idx >> 4, m4 = (idx & 15) * 4;
             const bool kin = k0 + kk < kdim;
-            const int64_t ra = rbase + mm, rb = cbase + mm;
-            As[kk][mm] = (kin && ra < nrows) ? P[ra + (int64_t)(k0 + kk) * ldp] : 0.f;
-            Bs[kk][mm] = (kin && rb < nrows) ? P[rb + (int64_t)(k0 + kk) * ldp] : 0.f;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int64_t r = (h ? cbase : rbase) + m4;
+                float *d = h ? &Bs[buf][kk][m4] : &As[buf][kk][m4];
+                const float *g = P + r + (int64_t)(k0 + kk) * ldp;
+                const int64_t nv64 = kin ? nrows - r : 0;
+                const int nv = nv64 < 0 ? 0 : (nv64 > 4 ? 4 : (int)nv64);
+                if (vec) {
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(d)),
+                                 "l"(nv ? g : P), "r"(4 * nv));
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        if (e < nv) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(d + e)),
+                                                 "l"(g + e));
+                        else d[e] = 0.f;
+                    }
+                }
+            }
         }
+    };
+    float acc[4][4] = {};
+    const int nk = (kdim + 31) / 32;
+    stage(0, 0);
+    cp_async_commit();
+    for (int kt = 0; kt < nk; ++kt) {
+        if (kt + 1 < nk) stage((kt + 1) & 1, (kt + 1) * 32);
+        cp_async_commit();
+        cp_async_wait<1>();
         __syncthreads();
+        const int b = kt & 1;
+#pragma unroll 8
+        for (int kk = 0; kk < 32; ++kk) {
+            float a[4], bb[4];
 #pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-            float a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) { a[i] = As[kk][ty + 16 * i]; b[i] = Bs[kk][tx + 16 * i]; }
+            for (int i = 0; i < 4; ++i) { a[i] = As[b][kk][ty + 16 * i]; bb[i] = Bs[b][kk][tx + 16 * i]; }
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], bb[j], acc[i][j]);
         }
         __syncthreads();
     }
+    cp_async_wait<0>();
     float cv[4][4];   // loads first, then stores (avoids serialized read-modify-writes)
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -377,12 +416,9 @@ extern "C" int lnb_k_trsm_rlt_f32(const float *L, int64_t lda, const float *dinv
                                   int bs, lnb_stream_t s)
 {
     if (m <= 0 || bs <= 0) return 0;
-    const int nj = (bs + 31) / 32;
-    const int smem = (nj * 32 * 32 + 5 * 32 * ptrsm::LDB) * (int)sizeof(float);
-    cudaFuncSetAttribute(k_trsm_rlt_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const int vec = ((uintptr_t)L % 16 == 0) && (lda % 4 == 0);
-    k_trsm_rlt_f32<<<(unsigned)((m + 31) / 32), ptrsm::NT, smem, s>>>(L, lda, dinv, B, ldb, m, bs, vec, nullptr,
-                                                                      nullptr, 0);
+    k_trsm_rlt_f32<<<(unsigned)((m + 31) / 32), ptrsm::NT, 0, s>>>(L, lda, dinv, B, ldb, m, bs, vec, nullptr,
+                                                                    nullptr, 0);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }
@@ -396,11 +432,8 @@ extern "C" int lnb_k_trsm_rlt_prep_f32(const float *L, int64_t lda, const float 
     if (m <= 0 || bs <= 0) return 0;
     const int nj = (bs + 31) / 32;
     if (32 * nj > kpad || kpad % 4 || (uintptr_t)hi % 16 || (uintptr_t)lo % 16) return (int)cudaErrorInvalidValue;
-    const int smem = (nj * 32 * 32 + 5 * 32 * ptrsm::LDB) * (int)sizeof(float);
-    cudaFuncSetAttribute(k_trsm_rlt_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const int vec = ((uintptr_t)L % 16 == 0) && (lda % 4 == 0);
-    k_trsm_rlt_f32<<<(unsigned)((m + 31) / 32), ptrsm::NT, smem, s>>>(L, lda, dinv, B, ldb, m, bs, vec, hi, lo,
-                                                                      kpad);
+    k_trsm_rlt_f32<<<(unsigned)((m + 31) / 32), ptrsm::NT, 0, s>>>(L, lda, dinv, B, ldb, m, bs, vec, hi, lo, kpad);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }

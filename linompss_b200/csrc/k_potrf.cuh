@@ -7,13 +7,10 @@
 // the structure of the reference's nested variant (chol_nrlmain.c).
 //
 // The whole tile lives in shared memory and is factored in 32-column panels:
-//   (1) warp 0 factors the 32 x 32 diagonal block left-looking, column by
-//       column in potf2 order, one row per lane, in rolled loops over shared
-//       memory.  Unrolled register code for this one-warp phase outgrew the
-//       instruction cache and ran at ~30 cycles per instruction.  Columns
-//       are scaled by rsqrt(pivot), the reciprocal LAPACK's potf2 scales by.
-//       The warp then inverts the block by forward substitution, one column
-//       per lane.
+//   (1) all threads factor the 32 x 32 diagonal block right-looking and build
+//       its inverse in the same sweep, one barrier per column (one-warp
+//       versions of both were the leaf's serial bottleneck); columns are
+//       scaled by rsqrt(pivot), the reciprocal LAPACK's potf2 scales by.
 //   (2) the rows below the block become b * inv(L_jj)^T: independent dot
 //       products, 4 threads per row, instead of a substitution chain;
 //   (3) the rank-32 update of the trailing triangle reads a transposed copy
@@ -54,7 +51,7 @@ __host__ __device__ inline LeafLayout leaf_layout(int bs)
     L.p_off = (((size_t)bs * L.lds + v - 1) / v) * v;
     L.li_off = L.p_off + (size_t)LP * L.ldp;
     L.rd_off = L.li_off + ((LP * (LP + 1) + v - 1) / v) * v;
-    L.total = L.rd_off + LP;
+    L.total = L.rd_off + 2 * LP;
     return L;
 }
 
@@ -69,9 +66,9 @@ __global__ void __launch_bounds__(256) k_potrf_leaf(T *A, int64_t lda, int bs, i
     T *S = base + LY.s_off;     // S[r * LDS + c] = A[r, c], lower part
     T *Pt = base + LY.p_off;    // Pt[p * LDP + r] = L[r, j0 + p]: the panel below the block, transposed
     T *Li = base + LY.li_off;   // Li[p * 33 + j] = inv(L_jj)[j][p]
-    T *Rd = base + LY.rd_off;   // Rd[c] = 1 / L[j0 + c, j0 + c]
+    T *Rd = base + LY.rd_off;   // Rd[c] = rsqrt(pivot c) = 1 / L[c][c]; Rd[LP + c] = pivot c
     __shared__ int fail_col;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
     if (tid == 0) fail_col = bs;
 
     // the tile arrives by element-wise cp.async, all copies in flight at once
@@ -86,57 +83,65 @@ __global__ void __launch_bounds__(256) k_potrf_leaf(T *A, int64_t lda, int bs, i
 
     for (int j0 = 0; j0 < bs; j0 += LP) {
         const int jb = min(LP, bs - j0);
-        if (warp == 0) {
-            // ---- (1) factor the jb x jb diagonal block: lane l owns row j0 + l ----
-            const int rl = lane < jb ? lane : 0;                 // rows past jb read row 0, unused
-            T *Ll = S + (j0 + rl) * LDS + j0;
-            int bad = -1;
+        // ---- (1) factor the jb x jb diagonal block right-looking with all threads,
+        //      one barrier per column, and build its inverse X = inv(L_jj) in the
+        //      same sweep (X = I; for each column c: X[r][:] -= L[r][c] X[c][:] / L[c][c]
+        //      for r > c).  Both use the unscaled column over the pivot, e.g.
+        //      S[r][cc] -= S[r][c] S[cc][c] / d_c; the scaling of L's column c and of
+        //      X's row c by rsqrt(d_c) (the reciprocal potf2 uses) waits for one pass
+        //      at the end.  X lives in Li (Li[q][r] = X[r][q]). ----
+        {
+            const int ty = tid >> 5, tx = lane;
+            for (int idx = tid; idx < LP * (LP + 1); idx += blockDim.x) {
+                const int q = idx / (LP + 1), r = idx - q * (LP + 1);
+                Li[idx] = (r == q) ? T(1) : T(0);
+            }
+            __syncthreads();
+            int fc = jb;
             for (int c = 0; c < jb; ++c) {
-                const T *Lc = S + (j0 + c) * LDS + j0;
-                T s0 = Ll[c], s1 = T(0);
-                int p = 0;
-                for (; p + 1 < c; p += 2) {
-                    s0 -= Ll[p] * Lc[p];
-                    s1 -= Ll[p + 1] * Lc[p + 1];
-                }
-                if (p < c) s0 -= Ll[p] * Lc[p];
-                const T sv = s0 + s1;                           // updated A[l][c] for l >= c
-                const T d = __shfl_sync(0xffffffffu, sv, c);
-                if (!(d > T(0))) {
-                    bad = c;                                    // potf2 keeps the updated pivot
-                    if (lane == c) Ll[c] = d;
-                    break;
-                }
+                const T d = S[(j0 + c) * LDS + j0 + c];       // every thread reads the same pivot
+                if (!(d > T(0))) { fc = c; break; }            // potf2 keeps the updated pivot
                 const T inv = leaf_rsqrt(d);
-                if (lane == c) { Ll[c] = d * inv; Rd[c] = inv; }
-                else if (lane > c && lane < jb) Ll[c] = sv * inv;
-                __syncwarp();
-            }
-            const int fc = bad >= 0 ? bad : jb;   // finished columns of the block
-            if (lane == 0 && bad >= 0) {
-                fail_col = j0 + bad;
-                atomicCAS(&st->info, 0, (int)(row0 + j0 + bad + 1));
-            }
-            __syncwarp();
-            // ---- inverse of the block (identity past fc): lane c builds column c
-            //      in Li[c][*] = inv[*][c] by forward substitution ----
-            T *Xc = Li + lane * (LP + 1);
-            for (int r = 0; r < LP; ++r) {
-                T v0 = (r == lane) ? T(1) : T(0), v1 = T(0);
-                if (r < fc) {
-                    const T *Lr = S + (j0 + r) * LDS + j0;
-                    int p = 0;
-                    for (; p + 1 < r; p += 2) {
-                        v0 -= Lr[p] * Xc[p];
-                        v1 -= Lr[p + 1] * Xc[p + 1];
-                    }
-                    if (p < r) v0 -= Lr[p] * Xc[p];
+                const T invd = inv * inv;
+                if (tid == 0) { Rd[c] = inv; Rd[LP + c] = d; }
+                const int cc = c + 1 + tx;
+                if (cc < jb) {
+                    const T lcc = S[(j0 + cc) * LDS + j0 + c] * invd;
+                    for (int r = cc + ty; r < jb; r += 8)
+                        S[(j0 + r) * LDS + j0 + cc] -= S[(j0 + r) * LDS + j0 + c] * lcc;
                 }
-                Xc[r] = (v0 + v1) * (r < fc ? Rd[r] : T(1));
+                // X rows r > c, columns q <= c: X[r][q] -= S[r][c] X[c][q] / d_c
+                for (int e = tid; e < (jb - 1 - c) * (c + 1); e += blockDim.x) {
+                    const int r = c + 1 + e / (c + 1), q = e - (r - c - 1) * (c + 1);
+                    Li[q * (LP + 1) + r] -= S[(j0 + r) * LDS + j0 + c] * invd * Li[q * (LP + 1) + c];
+                }
+                __syncthreads();
             }
+            if (tid == 0 && fc < jb) {
+                fail_col = j0 + fc;
+                atomicCAS(&st->info, 0, (int)(row0 + j0 + fc + 1));
+            }
+            // scale L's columns and X's rows (X = identity past a failed pivot)
+            for (int idx = tid; idx < jb * jb; idx += blockDim.x) {
+                const int r = idx / jb, c = idx - r * jb;
+                if (c < fc && r >= c) {
+                    T &v = S[(j0 + r) * LDS + j0 + c];
+                    v = (r == c) ? Rd[LP + c] * Rd[c] : v * Rd[c];
+                }
+            }
+            for (int idx = tid; idx < LP * LP; idx += blockDim.x) {
+                const int r = idx / LP, q = idx - r * LP;      // X[r][q]
+                T &x = Li[q * (LP + 1) + r];
+                if (r < fc) x *= Rd[r];
+                else x = (r == q) ? T(1) : T(0);
+            }
+            __syncthreads();
             if (dinv != nullptr) {
                 T *D = dinv + (int64_t)(j0 / LP) * LP * LP;
-                for (int r = 0; r < LP; ++r) D[r + LP * lane] = Xc[r];
+                for (int idx = tid; idx < LP * LP; idx += blockDim.x) {
+                    const int c = idx / LP, r = idx - c * LP;
+                    D[r + LP * c] = Li[c * (LP + 1) + r];
+                }
             }
         }
         __syncthreads();
@@ -152,15 +157,19 @@ __global__ void __launch_bounds__(256) k_potrf_leaf(T *A, int64_t lda, int bs, i
 #pragma unroll
             for (int p = 0; p < LP; ++p) b[p] = (act && p < jb) ? S[r * LDS + j0 + p] : T(0);
             __syncwarp();
+            T acc[LP / 4];
+#pragma unroll
+            for (int s = 0; s < LP / 4; ++s) acc[s] = T(0);
+#pragma unroll
+            for (int p = 0; p < LP; ++p)
+#pragma unroll
+                for (int s = 0; s < LP / 4; ++s) acc[s] = fma(b[p], Li[p * (LP + 1) + g + 4 * s], acc[s]);
 #pragma unroll
             for (int s = 0; s < LP / 4; ++s) {
                 const int j = g + 4 * s;
-                T acc = T(0);
-#pragma unroll
-                for (int p = 0; p < LP; ++p) acc = fma(b[p], Li[p * (LP + 1) + j], acc);
                 if (act && j < jv) {
-                    S[r * LDS + j0 + j] = acc;
-                    Pt[j * LDP + r] = acc;
+                    S[r * LDS + j0 + j] = acc[s];
+                    Pt[j * LDP + r] = acc[s];
                 }
             }
         }

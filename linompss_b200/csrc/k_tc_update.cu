@@ -11,7 +11,7 @@
 //                 128-row block; one kind::f16 MMA, epilogue multiplies by
 //                 s_i * s_j
 // Output tiles 128 x 128, K staged 128 bytes at a time by TMA (128B swizzle,
-// no multicast), one persistent CTA per SM walking the launch's tile list,
+// no multicast), persistent CTAs (one per SM, at most 16 tiles each) walking the launch's tile list,
 // two TMEM accumulators (2 x 128 columns) so the epilogue of one tile
 // overlaps the mainloop of the next.  Warp roles: warp 0 lane 0 issues TMA,
 // warp 1 lane 0 issues tcgen05.mma, warps 2..5 run the epilogue (tcgen05.ld
@@ -24,6 +24,7 @@
 namespace lnb {
 
 enum { MODE_TF32X3 = 0, MODE_TF32 = 1, MODE_BF16 = 2 };
+constexpr int64_t TC_MAX_TILES = 16;   // tiles one CTA walks at most (see the launcher)
 
 template <int MODE>
 struct TcCfg {
@@ -308,7 +309,13 @@ extern "C" int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    dim3 grid((unsigned)(tl.count < sms ? tl.count : sms));
+    // persistent, but a CTA walks at most TC_MAX_TILES tiles: long updates then
+    // retire CTAs every few hundred microseconds, which lets the high-priority
+    // stream's panel kernels (POTRF, TRSM) take SMs in the middle of an update
+    int64_t g = tl.count < sms ? tl.count : sms;
+    const int64_t gcap = (tl.count + TC_MAX_TILES - 1) / TC_MAX_TILES;
+    if (gcap > g) g = gcap;
+    dim3 grid((unsigned)g);
     switch (mode) {
     case MODE_TF32X3:
         cudaFuncSetAttribute(k_tc_syrk_lower<MODE_TF32X3>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -30,9 +30,10 @@ constexpr int NRC = 64;         // rhs columns per pass
 // ------------------------------------------------------------------------
 // inverses of the diagonal blocks
 // ------------------------------------------------------------------------
+// the inverses are computed in FP64 and stored in the precision of T
 template <typename TT>
 __global__ void __launch_bounds__(TH) k_trtri_blocks(const TT *T, int64_t ldt, int64_t n, char uplo, int unit,
-                                                     double *dinv)
+                                                     TT *dinv)
 {
     extern __shared__ double smx[];
     double (*X)[TH + 1] = reinterpret_cast<double (*)[TH + 1]>(smx);              // X[r][c], column c owned by thread c
@@ -67,8 +68,8 @@ __global__ void __launch_bounds__(TH) k_trtri_blocks(const TT *T, int64_t ldt, i
         }
     }
     __syncthreads();
-    double *D = dinv + (int64_t)q * TH * TH;
-    for (int r = 0; r < TH; ++r) D[r + TH * c] = X[r][c];
+    TT *D = dinv + (int64_t)q * TH * TH;
+    for (int r = 0; r < TH; ++r) D[r + TH * c] = (TT)X[r][c];
 }
 
 // ------------------------------------------------------------------------
@@ -76,7 +77,7 @@ __global__ void __launch_bounds__(TH) k_trtri_blocks(const TT *T, int64_t ldt, i
 // ------------------------------------------------------------------------
 template <typename TT>
 struct TrsmArgs {
-    const TT *T; int64_t ldt; const double *dinv;
+    const TT *T; int64_t ldt; const TT *dinv;
     double *B; int64_t ldb; int64_t n, nrhs;
     int nb; int fwd; int tT;   // tT: op(T) = T^T
     int *ticket, *cnt, *ready;
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(128) k_trsm_dag(TrsmArgs<TT> a)
 
         if (row_item) {
             // ---- R(ii): X_i = inv(op T_ii) (B_i - op(T)_{i,p} X_p),  p = previous block ----
-            const double *D = a.dinv + (int64_t)i * TH * TH;
+            const TT *D = a.dinv + (int64_t)i * TH * TH;
             for (int idx = tid; idx < TH * TH; idx += 128) {
                 const int k = idx / TH, m = idx % TH;   // Ds[k][m] = inv(op T_ii)[m][k]
                 Ds[k * TLD + m] = a.tT ? D[k + TH * m] : D[m + TH * k];
@@ -279,7 +280,7 @@ extern "C" int64_t lnb_trsm_sync_ints(int64_t n, int h)
 }
 
 template <typename TT>
-static int trtri_blocks(const TT *T, int64_t ldt, int64_t n, int h, char uplo, int unit, double *dinv, lnb_stream_t s)
+static int trtri_blocks(const TT *T, int64_t ldt, int64_t n, int h, char uplo, int unit, TT *dinv, lnb_stream_t s)
 {
     if (h != TH) return (int)cudaErrorInvalidValue;
     if (n <= 0) return 0;
@@ -293,7 +294,7 @@ static int trtri_blocks(const TT *T, int64_t ldt, int64_t n, int h, char uplo, i
 
 template <typename TT>
 static int trsm_left(char uplo, char trans, int64_t n, int64_t nrhs, double alpha, const TT *T, int64_t ldt,
-                     const double *dinv, int h, double *B, int64_t ldb, int *sync, lnb_status_t *st,
+                     const TT *dinv, int h, double *B, int64_t ldb, int *sync, lnb_status_t *st,
                      long long wait_ns, int ticket0, lnb_stream_t s)
 {
     if (h != TH) return (int)cudaErrorInvalidValue;
@@ -313,11 +314,11 @@ static int trsm_left(char uplo, char trans, int64_t n, int64_t nrhs, double alph
     }
     if (nrhs <= 8) {
         if constexpr (sizeof(TT) == 8)
-            return lnb_k_trsm_chain_f64(uplo, trans, n, nrhs, (const double *)T, ldt, dinv, B, ldb, sync, st,
-                                        wait_ns, s);
+            return lnb_k_trsm_chain_f64(uplo, trans, n, nrhs, (const double *)T, ldt, (const double *)dinv, B, ldb,
+                                        sync, st, wait_ns, s);
         else
-            return lnb_k_trsm_chain_f32(uplo, trans, n, nrhs, (const float *)T, ldt, dinv, B, ldb, sync, st,
-                                        wait_ns, s);
+            return lnb_k_trsm_chain_f32(uplo, trans, n, nrhs, (const float *)T, ldt, (const float *)dinv, B, ldb,
+                                        sync, st, wait_ns, s);
     }
     TrsmArgs<TT> a;
     a.T = T; a.ldt = ldt; a.dinv = dinv; a.B = B; a.ldb = ldb; a.n = n; a.nrhs = nrhs;
@@ -346,7 +347,7 @@ extern "C" int lnb_k_trtri_blocks_f64(const double *T, int64_t ldt, int64_t n, i
     return trtri_blocks<double>(T, ldt, n, h, uplo, unit, dinv, s);
 }
 extern "C" int lnb_k_trtri_blocks_f32(const float *T, int64_t ldt, int64_t n, int h, char uplo, int unit,
-                                      double *dinv, lnb_stream_t s)
+                                      float *dinv, lnb_stream_t s)
 {
     return trtri_blocks<float>(T, ldt, n, h, uplo, unit, dinv, s);
 }
@@ -357,7 +358,7 @@ extern "C" int lnb_k_trsm_left_f64(char uplo, char trans, int64_t n, int64_t nrh
     return trsm_left<double>(uplo, trans, n, nrhs, alpha, T, ldt, dinv, h, B, ldb, sync, st, wait_ns, ticket0, s);
 }
 extern "C" int lnb_k_trsm_left_f32(char uplo, char trans, int64_t n, int64_t nrhs, double alpha, const float *T,
-                                   int64_t ldt, const double *dinv, int h, double *B, int64_t ldb, int *sync,
+                                   int64_t ldt, const float *dinv, int h, double *B, int64_t ldb, int *sync,
                                    lnb_status_t *st, long long wait_ns, int ticket0, lnb_stream_t s)
 {
     return trsm_left<float>(uplo, trans, n, nrhs, alpha, T, ldt, dinv, h, B, ldb, sync, st, wait_ns, ticket0, s);

@@ -19,8 +19,8 @@
 //     and stages its right-hand sides into shared memory with cp.async ahead
 //     of the compute warps;
 //   * a publisher warp makes finished solution blocks visible to the whole
-//     GPU (one fence for all blocks finished so far, then their flags) off
-//     the compute warps' path;
+//     GPU (one release fence for all blocks finished so far, then their
+//     flags) off the compute warps' path;
 //   * every other CTA takes work items (row i, a chunk of CW tiles j <=
 //     i-W-1) from an atomic ticket in row order.  An item streams its tiles
 //     (double-buffered across items) before it waits for its solution blocks,
@@ -58,7 +58,7 @@ template <> struct Ld<double, false> { static constexpr int v = 68; };
 
 template <typename TT>
 struct Args {
-    const TT *T; int64_t ldt; const double *dinv;
+    const TT *T; int64_t ldt; const TT *dinv;   // inverses stored in the precision of T
     double *B; int64_t ldb; int64_t n; int nrhs;
     int nb, fwd, vec;           // vec: T and ldt allow 16-byte copies
     int *ticket, *cnt, *ready;  // cnt/ready indexed by chain position
@@ -88,6 +88,9 @@ LNB_DEV void prefetch_l2(const void *p, uint32_t bytes)
 {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
+// release fence at GPU scope: orders this thread's earlier writes, and those it
+// has observed through a barrier, before its later writes (cumulative)
+LNB_DEV void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
 LNB_DEV void st_relaxed(int *p, int v)
 {
     asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
@@ -197,20 +200,26 @@ template <bool TR>
 LNB_DEV int kd(int kq, int j) { return TR ? 2 * (kq + 4 * (j >> 1)) + (j & 1) : kq + 4 * j; }
 
 // inverse of op(T) on diagonal block i, this lane's 16 entries of row m
-template <bool TR>
-LNB_DEV void load_dinv(const double *dinv, int i, int m, int kq, double (&dv)[16])
+// (stored in the precision of T, held in FP64)
+template <bool TR, typename DT>
+LNB_DEV void load_dinv(const DT *dinv, int i, int m, int kq, double (&dv)[16])
 {
-    const double *D = dinv + (int64_t)i * TH * TH;   // inv(T_ii), column-major
+    const DT *D = dinv + (int64_t)i * TH * TH;   // inv(T_ii), column-major
     if constexpr (TR) {
-        // inv(T_ii^T)[m][k] = D[k + 64 m]
+        // inv(T_ii^T)[m][k] = D[k + 64 m], pairs of consecutive k
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-            const double2 q = __ldg(reinterpret_cast<const double2 *>(D + TH * m + 2 * (kq + 4 * u)));
-            dv[2 * u] = q.x; dv[2 * u + 1] = q.y;
+            if constexpr (sizeof(DT) == 8) {
+                const double2 q = __ldg(reinterpret_cast<const double2 *>(D + TH * m + 2 * (kq + 4 * u)));
+                dv[2 * u] = q.x; dv[2 * u + 1] = q.y;
+            } else {
+                const float2 q = __ldg(reinterpret_cast<const float2 *>(D + TH * m + 2 * (kq + 4 * u)));
+                dv[2 * u] = q.x; dv[2 * u + 1] = q.y;
+            }
         }
     } else {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) dv[j] = __ldg(D + m + TH * kd<false>(kq, j));
+        for (int j = 0; j < 16; ++j) dv[j] = (double)__ldg(D + m + TH * kd<false>(kq, j));
     }
 }
 
@@ -301,7 +310,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
                     }
                     int q = p + 1;
                     while (q < nb && q < p + XR && tc::mbar_try_wait(&cb->xfull[q % XR], (q / XR) & 1)) ++q;
-                    __threadfence();
+                    fence_acq_rel_gpu();
                     for (int t = p; t < q; ++t) {
                         st_relaxed(&a.ready[t], 1);
                         tc::mbar_arrive(&cb->xempty[t % XR]);
@@ -360,7 +369,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
         // ---- compute warps ----
         const int m = tid >> 2, kq = tid & 3;
         double dA[16], dB[16];
-        load_dinv<TR>(a.dinv, blk(a, 0), m, kq, dA);
+        load_dinv<TR, TT>(a.dinv, blk(a, 0), m, kq, dA);
         bool okp = true;
         // one chain step at position p; dcur holds inv(op T_pp), dnext receives the next one
         auto step = [&](int p, double (&dcur)[16], double (&dnext)[16]) -> bool {
@@ -374,7 +383,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
                     if (p + 1 - k >= 0)
                         stage_tile<TT, TR>(a, tiles + ((p + 1) & 1) * W * TS + (k - 1) * TS, ip, blk(a, p + 1 - k),
                                            tid, NCOMP);
-                load_dinv<TR>(a.dinv, ip, m, kq, dnext);
+                load_dinv<TR, TT>(a.dinv, ip, m, kq, dnext);
             }
             cp_async_commit();
             // L2 prefetch PF steps ahead (band tiles, one column per thread, and the
@@ -383,7 +392,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
                 const int k = 1 + (tid >> 6);
                 if (k <= W && p + PF - k >= 0)
                     prefetch_tile_col<TT, TR>(a, blk(a, p + PF), blk(a, p + PF - k), tid & 63);
-                if (tid == 255) prefetch_l2(a.dinv + (int64_t)blk(a, p + PF) * TH * TH, TH * TH * sizeof(double));
+                if (tid == 255) prefetch_l2(a.dinv + (int64_t)blk(a, p + PF) * TH * TH, TH * TH * sizeof(TT));
             }
             // band: sum_k op(T)(i, i-k) X_{p-k}
             double part[NR];
@@ -501,11 +510,11 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
             for (int r = 0; r < NR; ++r)
                 if ((r & 3) == kq && m < in_ && r < a.nrhs)
                     atomicAdd(a.B + (oi + m) + (int64_t)r * a.ldb, -part[r]);
-            __threadfence();
+            fence_acq_rel_gpu();
         }
         __syncthreads();
         if (tid == 0) {
-            __threadfence();
+            fence_acq_rel_gpu();
             atomicAdd(&a.cnt[row], 1);
         }
         item = next; row = nrow; chunk = nchunk; buf ^= 1;
@@ -546,7 +555,7 @@ int launch(const Args<TT> &a, lnb_stream_t s)
 }
 
 template <typename TT>
-int trsm_chain(char uplo, char trans, int64_t n, int64_t nrhs, const TT *T, int64_t ldt, const double *dinv,
+int trsm_chain(char uplo, char trans, int64_t n, int64_t nrhs, const TT *T, int64_t ldt, const TT *dinv,
                double *B, int64_t ldb, int *sync, lnb_status_t *st, long long wait_ns, lnb_stream_t s)
 {
     Args<TT> a;
@@ -576,7 +585,7 @@ extern "C" int lnb_k_trsm_chain_f64(char uplo, char trans, int64_t n, int64_t nr
     return lnb::chain::trsm_chain<double>(uplo, trans, n, nrhs, T, ldt, dinv, B, ldb, sync, st, wait_ns, s);
 }
 extern "C" int lnb_k_trsm_chain_f32(char uplo, char trans, int64_t n, int64_t nrhs, const float *T, int64_t ldt,
-                                    const double *dinv, double *B, int64_t ldb, int *sync, lnb_status_t *st,
+                                    const float *dinv, double *B, int64_t ldb, int *sync, lnb_status_t *st,
                                     long long wait_ns, lnb_stream_t s)
 {
     if (nrhs > 8) return (int)cudaErrorInvalidValue;

@@ -7,9 +7,10 @@
  * captured in a CUDA graph once the workspace exists (any earlier call, or
  * lnb_batched_autotune, creates it).
  *
- * Autotuning: the panel width of the per-system factorization (16 or 32) is
- * chosen per mode by lnb_batched_autotune, which times both variants on the
- * caller's own batch and keeps the faster one for the rest of the process.
+ * Autotuning: the CTA size of the persistent solver (256 or 512 threads; 256
+ * only in FP64 mode, whose shared-memory layout fills the SM) is chosen by
+ * lnb_batched_autotune, which times the candidates on the caller's own batch
+ * and keeps the faster one for the rest of the process.
  */
 #include <string.h>
 
@@ -18,7 +19,7 @@
 size_t lnb_batched_scratch_bytes(int grid, int fp64);
 int lnb_k_batched_posv(int count, const int *n, const int *nrhs, const int64_t *a_off, const int64_t *b_off,
                        const double *A, const double *B, double *X, void *scratch, int grid, const int *order,
-                       int *ticket, int *info, int *iters, int max_iter, int fp64, int pw, cudaStream_t s);
+                       int *ticket, int *info, int *iters, int max_iter, int fp64, int variant, cudaStream_t s);
 int lnb_k_batch_order(int count, const int *n, int *order, cudaStream_t s);
 
 #define CK(call, where)                                            \
@@ -27,7 +28,7 @@ int lnb_k_batch_order(int count, const int *n, int *order, cudaStream_t s);
         if (_e != 0) return lnb_cuda_error(_e, where);             \
     } while (0)
 
-static int g_pw[2] = {32, 32};   /* tuned panel width: [fp32 mode, fp64 mode] */
+static int g_pw[2] = {256, 256};   /* tuned CTA size: [fp32 mode, fp64 mode] */
 
 static int batched_run(int count, const int *n, const int *nrhs, const int64_t *a_off, const int64_t *b_off,
                        const double *dA, const double *dB, double *dX, int mode, int max_iter, int *info,
@@ -71,10 +72,11 @@ int lnb_batched_autotune(int count, const int *n_dev, const int *nrhs_dev, const
     cudaStream_t s = (cudaStream_t)stream;
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
-    const int cand[2] = {16, 32};
+    const int cand[2] = {256, 512};
+    const int ncand = mode == LNB_FACTOR_FP64 ? 1 : 2;
     float best = 1e30f;
-    int pick = 32;
-    for (int k = 0; k < 2; ++k) {
+    int pick = 256;
+    for (int k = 0; k < ncand; ++k) {
         for (int rep = 0; rep < 2; ++rep) {   /* first run warms up */
             CK(cudaEventRecord(c->t0, s), "event");
             int e = batched_run(count, n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode, max_iter, NULL,

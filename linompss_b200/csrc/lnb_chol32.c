@@ -339,7 +339,7 @@ static int spotrs_run(lnb_ctx *c, int64_t n, int64_t nrhs, const float *dL, int6
                       char which, lnb_arena *ar, cudaStream_t s)
 {
     const int64_t nb = (n + TRSV_H - 1) / TRSV_H;
-    double *dinv = lnb_arena_take(ar, (size_t)nb * TRSV_H * TRSV_H * 8);
+    float *dinv = lnb_arena_take(ar, (size_t)nb * TRSV_H * TRSV_H * sizeof(float));
     double *Z = lnb_arena_take(ar, (size_t)n * nrhs * 8);
     int *sync = lnb_arena_take(ar, (size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4);
     if (!sync) return lnb_set_error(LNB_ENOMEM, "spotrs workspace");

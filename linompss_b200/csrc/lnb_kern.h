@@ -76,7 +76,7 @@ int lnb_k_trsm_chain_f64(char uplo, char trans, int64_t n, int64_t nrhs, const d
                          const double *dinv, double *B, int64_t ldb, int *sync, lnb_status_t *st,
                          long long wait_ns, lnb_stream_t s);
 int lnb_k_trsm_chain_f32(char uplo, char trans, int64_t n, int64_t nrhs, const float *T, int64_t ldt,
-                         const double *dinv, double *B, int64_t ldb, int *sync, lnb_status_t *st,
+                         const float *dinv, double *B, int64_t ldb, int *sync, lnb_status_t *st,
                          long long wait_ns, lnb_stream_t s);
 
 /* ---- FP32-storage factorization kernels (k_chol_f32.cu) ------------------ */
@@ -105,11 +105,12 @@ int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int kpad, int6
                         int64_t ldc, int64_t nrows, int64_t c0, int64_t c1, int kdim, const float *scale,
                         lnb_status_t *st, long long wait_ns, lnb_stream_t s);
 
-/* FP32-stored triangular factor, FP64 right-hand sides and arithmetic */
-int lnb_k_trtri_blocks_f32(const float *T, int64_t ldt, int64_t n, int h, char uplo, int unit, double *dinv,
+/* FP32-stored triangular factor, FP64 right-hand sides and arithmetic; the block
+ * inverses are stored in FP32 (computed in FP64) */
+int lnb_k_trtri_blocks_f32(const float *T, int64_t ldt, int64_t n, int h, char uplo, int unit, float *dinv,
                            lnb_stream_t s);
 int lnb_k_trsm_left_f32(char uplo, char trans, int64_t n, int64_t nrhs, double alpha, const float *T,
-                        int64_t ldt, const double *dinv, int h, double *B, int64_t ldb, int *sync,
+                        int64_t ldt, const float *dinv, int h, double *B, int64_t ldb, int *sync,
                         lnb_status_t *st, long long wait_ns, int ticket0, lnb_stream_t s);
 
 /* ---- symmetric products and refinement vectors (k_symv.cu) --------------- */

@@ -73,9 +73,9 @@ static size_t ir_ws_bytes(int64_t n, int64_t nrhs, int b, int mode)
 static int precond(lnb_ctx *c, const irws *w, cudaStream_t s)
 {
     CK(lnb_k_scale_rows_f64(w->n, w->nrhs, w->S, w->R, w->Z, s), "scale");
-    CK(lnb_k_trsm_left_f32('L', 'N', w->n, w->nrhs, 1.0, w->A32, w->ld32, w->dinv, TRSV_H, w->Z, w->n, w->sync,
+    CK(lnb_k_trsm_left_f32('L', 'N', w->n, w->nrhs, 1.0, w->A32, w->ld32, (const float *)w->dinv, TRSV_H, w->Z, w->n, w->sync,
                            c->st, lnb_wait_ns(), 0, s), "forward solve");
-    CK(lnb_k_trsm_left_f32('L', 'T', w->n, w->nrhs, 1.0, w->A32, w->ld32, w->dinv, TRSV_H, w->Z, w->n, w->sync,
+    CK(lnb_k_trsm_left_f32('L', 'T', w->n, w->nrhs, 1.0, w->A32, w->ld32, (const float *)w->dinv, TRSV_H, w->Z, w->n, w->sync,
                            c->st, lnb_wait_ns(), 0, s), "backward solve");
     CK(lnb_k_scale_rows_f64(w->n, w->nrhs, w->S, w->Z, w->Z, s), "scale");
     return 0;
@@ -156,7 +156,7 @@ int lnb_dsposv_ir_dev(int n, int nrhs, int b, const double *dA, int lda, const d
         if (e > 0 && res) { rr.info = e; *res = rr; }
         return e > 0 ? lnb_set_error(e, "low-precision factor: tile at row %d could not be refactored", e) : e;
     }
-    CK(lnb_k_trtri_blocks_f32(w.A32, w.ld32, n, TRSV_H, 'L', 0, w.dinv, s), "trtri");
+    CK(lnb_k_trtri_blocks_f32(w.A32, w.ld32, n, TRSV_H, 'L', 0, (float *)w.dinv, s), "trtri");
     CK(cudaEventRecord(c->t1, s), "event");
     int info = lnb_status_read(c, s);
     if (info < 0) return info;
