@@ -104,16 +104,26 @@ __global__ void __launch_bounds__(256) k_potrf_leaf(T *A, int64_t lda, int bs, i
                 const T inv = leaf_rsqrt(d);
                 const T invd = inv * inv;
                 if (tid == 0) { Rd[c] = inv; Rd[LP + c] = d; }
+                // thread (ty, tx): rows r = c+1+ty+8u (u < 4) of column cc = c+1+tx of L,
+                // and of column q = tx of X; all loads issued before the updates
                 const int cc = c + 1 + tx;
-                if (cc < jb) {
-                    const T lcc = S[(j0 + cc) * LDS + j0 + c] * invd;
-                    for (int r = cc + ty; r < jb; r += 8)
-                        S[(j0 + r) * LDS + j0 + cc] -= S[(j0 + r) * LDS + j0 + c] * lcc;
+                T lr[4], sv[4], xv[4];
+                const T lcc = cc < jb ? S[(j0 + cc) * LDS + j0 + c] * invd : T(0);
+                const T xcq = tx <= c ? Li[tx * (LP + 1) + c] * invd : T(0);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int r = c + 1 + ty + 8 * u;
+                    const bool in = r < jb;
+                    lr[u] = in ? S[(j0 + r) * LDS + j0 + c] : T(0);
+                    sv[u] = (in && cc < jb && r >= cc) ? S[(j0 + r) * LDS + j0 + cc] : T(0);
+                    xv[u] = (in && tx <= c) ? Li[tx * (LP + 1) + r] : T(0);
                 }
-                // X rows r > c, columns q <= c: X[r][q] -= S[r][c] X[c][q] / d_c
-                for (int e = tid; e < (jb - 1 - c) * (c + 1); e += blockDim.x) {
-                    const int r = c + 1 + e / (c + 1), q = e - (r - c - 1) * (c + 1);
-                    Li[q * (LP + 1) + r] -= S[(j0 + r) * LDS + j0 + c] * invd * Li[q * (LP + 1) + c];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int r = c + 1 + ty + 8 * u;
+                    if (r < jb && cc < jb && r >= cc) S[(j0 + r) * LDS + j0 + cc] = sv[u] - lr[u] * lcc;
+                    // X rows r > c, column q = tx <= c: X[r][q] -= S[r][c] X[c][q] / d_c
+                    if (r < jb && tx <= c) Li[tx * (LP + 1) + r] = xv[u] - lr[u] * xcq;
                 }
                 __syncthreads();
             }

@@ -18,13 +18,25 @@
 // -> registers -> C).  Every mbarrier wait is bounded; on expiry the CTA
 // records a timeout, drains what it issued and frees TMEM.
 #include <cuda.h>
+#include <stdlib.h>
 
 #include "tc_sm100.cuh"
 
 namespace lnb {
 
 enum { MODE_TF32X3 = 0, MODE_TF32 = 1, MODE_BF16 = 2 };
-constexpr int64_t TC_MAX_TILES = 16;   // tiles one CTA walks at most (see the launcher)
+constexpr int64_t TC_MAX_TILES = 16;   // default tiles one CTA walks at most (see the launcher)
+
+// LNB_TC_MAX_TILES overrides the cap (read once)
+static int64_t tc_max_tiles()
+{
+    static int64_t v = -1;
+    if (v < 0) {
+        const char *e = getenv("LNB_TC_MAX_TILES");
+        v = (e && atoi(e) > 0) ? atoi(e) : TC_MAX_TILES;
+    }
+    return v;
+}
 
 template <int MODE>
 struct TcCfg {
@@ -313,7 +325,8 @@ extern "C" int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int
     // retire CTAs every few hundred microseconds, which lets the high-priority
     // stream's panel kernels (POTRF, TRSM) take SMs in the middle of an update
     int64_t g = tl.count < sms ? tl.count : sms;
-    const int64_t gcap = (tl.count + TC_MAX_TILES - 1) / TC_MAX_TILES;
+    const int64_t mt = tc_max_tiles();
+    const int64_t gcap = (tl.count + mt - 1) / mt;
     if (gcap > g) g = gcap;
     dim3 grid((unsigned)g);
     switch (mode) {
