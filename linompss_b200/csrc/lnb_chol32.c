@@ -14,6 +14,7 @@
  * copy only starts after that update (the crit stream waits on it).
  */
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -48,12 +49,22 @@ size_t lnb_chol_f32_ws_bytes(int n, int b, int mode)
     return bytes + 4096;
 }
 
-/* one diagonal tile: leaf (<= 128) or a nested 128-wide pass with SIMT
- * inner updates; dinv receives the tile's 32x32 block inverses */
+/* one diagonal tile: a cluster launch (whole 32-blocks, up to 512), a leaf
+ * (<= 128), or a nested 128-wide pass with SIMT inner updates; dinv receives
+ * the tile's 32x32 block inverses */
+int lnb_k_potrf_cluster_f32(float *A, int64_t lda, int bs, int64_t row0, float *dinv, lnb_status_t *st,
+                            cudaStream_t s);
+
 int lnb_potrf_tile_f32(float *Akk, int64_t lda, int bs, int64_t row0, float *dinv, lnb_status_t *st,
                        cudaStream_t s)
 {
     const int LEAF_N = 128;
+    /* whole 32-blocks, 16-byte aligned: one cluster launch */
+    if (bs >= 64 && bs <= 512 && bs % 32 == 0 && (uintptr_t)Akk % 16 == 0 && lda % 4 == 0 &&
+        (uintptr_t)dinv % 16 == 0) {
+        CK(lnb_k_potrf_cluster_f32(Akk, lda, bs, row0, dinv, st, s), "potrf tile f32");
+        return 0;
+    }
     for (int j = 0; j < bs; j += LEAF_N) {
         const int jb = bs - j < LEAF_N ? bs - j : LEAF_N;
         float *Ajj = Akk + j + (int64_t)j * lda;

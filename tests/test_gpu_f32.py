@@ -102,13 +102,19 @@ def test_schol_hypermatrix(lnb):
 
 
 @pytest.mark.parametrize("mode", ["fp32", "tf32x3"])
-def test_schol_not_spd(lnb, mode):
+@pytest.mark.parametrize("n,b,bad", [(400, 128, 300), (1200, 512, 700), (1200, 512, 520), (1200, 512, 1100),
+                                       (1000, 200, 450), (256, 256, 0)])
+def test_schol_not_spd(lnb, mode, n, b, bad):
+    """A negative pivot is reported 1-based from every diagonal-tile path: the
+    cluster factor (whole 32-blocks: b = 512, 256), the leaf (b <= 128, the
+    ragged last tile) and the nested path (lda % 4 != 0)."""
     lnb.set_factor_mode(MODES[mode])
-    n, b = 400, 128
+    lda = n + 1 if b == 200 else n
     A0 = O.spd_diag_dominant(n, seed=2).astype(np.float32)
-    A0[300, 300] = -5.0
-    A = np.asfortranarray(A0.copy())
-    assert lnb.ompss_schol_rl(n, b, b, A, n) == 301
+    A0[bad, bad] = -5.0
+    A = np.zeros((lda, n), dtype=np.float32, order="F")
+    A[:n] = A0
+    assert lnb.ompss_schol_rl(n, b, b, A, lda) == bad + 1
 
 
 @pytest.mark.parametrize("n,nrhs", [(3001, 1), (3001, 8), (4096, 2)])
