@@ -235,6 +235,10 @@ def _stream(stream):
 
 
 def _ld(t) -> int:
+    # a (cols, rows) row-major tensor holds a column-major rows x cols matrix;
+    # torch reports stride 1 for a size-1 leading dimension, whose ld is rows
+    if t.dim() > 1 and t.size(0) == 1:
+        return max(int(t.size(1)), 1)
     return int(t.stride(0))
 
 

@@ -208,15 +208,8 @@ __global__ void __launch_bounds__(64) k_trsm_rlt_f32(const float *__restrict__ L
         __syncthreads();
         j = jn; kc = kn;
     }
-    // operand columns past the last 32-block are zero padding
-    if (hi != nullptr)
-        for (int idx = tid; idx < 32 * (kpad - 32 * nj); idx += NT) {
-            const int r = idx % 32, k = 32 * nj + idx / 32;
-            if (r0 + r < m) {
-                hi[(r0 + r) * kpad + k] = 0.f;
-                if (lo != nullptr) lo[(r0 + r) * kpad + k] = 0.f;
-            }
-        }
+    // operand columns past bs are not written: the update's tensor map ends at
+    // K = bs and reads zeros beyond it (kpad may be the stride of a wider array)
     cp_async_wait<0>();
 }
 
@@ -396,9 +389,40 @@ __global__ void k_lower_to_f32(const double *__restrict__ A, int64_t lda, int64_
     }
 }
 
+// columns [c0, c1) of the lower triangle of S A S in FP32; column c0 + blockIdx.y
+__global__ void k_lower_to_f32_cols(const double *__restrict__ A, int64_t lda, int64_t n, int64_t c0, int64_t c1,
+                                    const double *__restrict__ s, float *A32, int64_t ld32)
+{
+    for (int64_t j = c0 + blockIdx.y; j < c1; j += gridDim.y) {
+        const double sj = s[j];
+        for (int64_t i = j + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+             i += (int64_t)gridDim.x * blockDim.x)
+            A32[i + j * ld32] = (float)(A[i + j * lda] * s[i] * sj);
+    }
+}
+
 }  // namespace lnb
 
 using namespace lnb;
+
+extern "C" int lnb_k_lower_to_f32_cols(const double *A, int64_t lda, int64_t n, int64_t c0, int64_t c1,
+                                       const double *S, float *A32, int64_t ld32, lnb_stream_t s)
+{
+    if (c1 <= c0 || c0 >= n) return 0;
+    const int64_t rows = n - c0;
+    dim3 grid((unsigned)((rows + 255) / 256 < 32 ? (rows + 255) / 256 : 32), (unsigned)(c1 - c0 < 65535 ? c1 - c0 : 65535));
+    k_lower_to_f32_cols<<<grid, 256, 0, s>>>(A, lda, n, c0, c1, S, A32, ld32);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+
+extern "C" int lnb_k_equil_scale_vec(const double *a, int64_t n, int on, double *s_out, lnb_stream_t s)
+{
+    if (n <= 0) return 0;
+    k_equil_scale<<<(unsigned)((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024), 256, 0, s>>>(a, 0, n, on, s_out);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
 
 extern "C" int lnb_k_potrf_f32(float *A, int64_t lda, int bs, int64_t row0, float *dinv, lnb_status_t *st,
                                lnb_stream_t s)
@@ -424,8 +448,9 @@ extern "C" int lnb_k_trsm_rlt_f32(const float *L, int64_t lda, const float *dinv
 }
 
 // the panel solve plus the K-major TF32 operand copies of its result (hi, and
-// lo = x - hi when lo != NULL); kpad >= 32 ceil(bs/32), a multiple of 4, hi/lo
-// 16-byte aligned
+// lo = x - hi when lo != NULL), row stride kpad >= 32 ceil(bs/32), a multiple
+// of 4, hi/lo 16-byte aligned; K columns [0, 32 ceil(bs/32)) of each row are
+// written, nothing beyond
 extern "C" int lnb_k_trsm_rlt_prep_f32(const float *L, int64_t lda, const float *dinv, float *B, int64_t ldb,
                                        int64_t m, int bs, float *hi, float *lo, int kpad, lnb_stream_t s)
 {

@@ -278,14 +278,15 @@ static EncodeTiledFn encode_fn()
     return fn;
 }
 
-// K-major operand copy: rows x kpad elements (row stride kpad), box 128 rows x 128 bytes
-static int make_map(CUtensorMap *m, const void *base, int64_t rows, int kpad, bool bf16)
+// K-major operand copy: rows x kext elements, row stride kstride elements, box
+// 128 rows x 128 bytes; K beyond kext reads as zero
+static int make_map(CUtensorMap *m, const void *base, int64_t rows, int kext, int64_t kstride, bool bf16)
 {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return (int)cudaErrorNotSupported;
     const int esz = bf16 ? 2 : 4;
-    cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)kpad * esz};
+    cuuint64_t dims[2] = {(cuuint64_t)kext, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)kstride * esz};
     cuuint32_t box[2] = {(cuuint32_t)(128 / esz), 128};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = fn(m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
@@ -299,16 +300,18 @@ static int make_map(CUtensorMap *m, const void *base, int64_t rows, int kpad, bo
 
 using namespace lnb;
 
-// mode: 0 = TF32x3 (hi, lo), 1 = TF32 (hi), 2 = BF16 (hi = bf16 copy, scale)
-extern "C" int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int kpad, int64_t prow, float *C,
+// mode: 0 = TF32x3 (hi, lo), 1 = TF32 (hi), 2 = BF16 (hi = bf16 copy, scale).
+// The operands are K-major with row stride kstride (elements, a multiple of
+// 16 bytes); the first kdim K columns are used.
+extern "C" int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int64_t kstride, int64_t prow, float *C,
                                    int64_t ldc, int64_t nrows, int64_t c0, int64_t c1, int kdim, const float *scale,
                                    lnb_status_t *st, long long wait_ns, lnb_stream_t s)
 {
     if (nrows <= c0 || c1 <= c0 || kdim <= 0) return 0;
     if ((uintptr_t)hi % 16 || (lo && (uintptr_t)lo % 16)) return (int)cudaErrorMisalignedAddress;
     CUtensorMap ta, tb;
-    int e = make_map(&ta, hi, prow, kpad, mode == MODE_BF16);
-    if (!e) e = make_map(&tb, mode == MODE_TF32X3 ? lo : hi, prow, kpad, mode == MODE_BF16);
+    int e = make_map(&ta, hi, prow, kdim, kstride, mode == MODE_BF16);
+    if (!e) e = make_map(&tb, mode == MODE_TF32X3 ? lo : hi, prow, kdim, kstride, mode == MODE_BF16);
     if (e) return e;
     TileList tl;
     tl.tiles_c = (int)((c1 - c0 + 127) / 128);
@@ -325,7 +328,9 @@ extern "C" int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int
     // retire CTAs every few hundred microseconds, which lets the high-priority
     // stream's panel kernels (POTRF, TRSM) take SMs in the middle of an update
     int64_t g = tl.count < sms ? tl.count : sms;
-    const int64_t mt = tc_max_tiles();
+    // the cap counts 512-deep tiles: a CTA of a long-K update walks fewer
+    int64_t mt = tc_max_tiles() * 512 / kdim;
+    if (mt < 1) mt = 1;
     const int64_t gcap = (tl.count + mt - 1) / mt;
     if (gcap > g) g = gcap;
     dim3 grid((unsigned)g);

@@ -163,7 +163,7 @@ static int upd32(const panelbuf *pb, int slot, const float *P, int64_t ldp, floa
         e = lnb_k_syrk_lower_f32_simt(P, ldp, C, ldc, nrows, c0, c1, k, s);
     } else {
         const int m = pb->mode == LNB_FACTOR_TF32X3 ? 0 : pb->mode == LNB_FACTOR_TF32 ? 1 : 2;
-        e = lnb_k_tc_syrk_lower(m, pb->hi[slot], pb->lo[slot], (int)pb->kpad, nrows, C, ldc, nrows, c0, c1, k,
+        e = lnb_k_tc_syrk_lower(m, pb->hi[slot], pb->lo[slot], pb->kpad, nrows, C, ldc, nrows, c0, c1, k,
                                 pb->scale[slot], st, lnb_wait_ns(), s);
     }
     const double opb = pb->mode == LNB_FACTOR_BF16 ? 2.0 : pb->mode == LNB_FACTOR_TF32X3 ? 8.0 : 4.0;
@@ -239,6 +239,144 @@ int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode,
         if (nb2 > nb1) CK(upd32(&pb, slot, P, lda, Ct, lda, mrem, nb1, nb2, bs, c->st, s), "update panel k+2");
         CK(cudaEventRecord(ev_next, s), "event");
         if (mrem > nb2) CK(upd32(&pb, slot, P, lda, Ct, lda, mrem, nb2, mrem, bs, c->st, s), "update rest");
+        CK(cudaStreamWaitEvent(crit, ev_next, 0), "event wait");
+    }
+    CK(cudaEventRecord(ev_done, crit), "event");
+    CK(cudaStreamWaitEvent(s, ev_done, 0), "event wait");
+    return 0;
+}
+
+/* ---- streamed input ----------------------------------------------------------
+ * The matrix arrives over PCIe block column by block column while the
+ * factorization runs.  The K-major operand copies of every panel are kept (one
+ * n x ldk array each for hi and lo; panel k fills K columns [k b, k b + b) of
+ * the rows below it), so a block column that arrives after some panels are
+ * done is brought up to date by one long-K update with all of them (a
+ * left-looking "catch-up") and from then on takes the right-looking updates.
+ * A column joins as soon as its data is there -- the host checks the arrival
+ * events every step, and the per-step status read keeps it within a step of
+ * the device -- and at the latest when the next panels need it, in which case
+ * the device waits for its arrival event. */
+
+static inline int64_t ldk_of(int n) { return ((int64_t)n + 31) & ~(int64_t)31; }
+
+/* LNB_STREAM_AHEAD caps how many block columns beyond the next two may join
+ * early (unset: no cap); 0 makes every column join by a catch-up update just
+ * before it is needed */
+static int stream_ahead(void)
+{
+    const char *e = getenv("LNB_STREAM_AHEAD");
+    return (e && *e) ? atoi(e) : 1 << 30;
+}
+
+int lnb_chol_f32_stream_ok(int n, int b, int mode)
+{
+    return (mode == LNB_FACTOR_TF32X3 || mode == LNB_FACTOR_TF32) && b % 32 == 0 && n > b;
+}
+
+size_t lnb_chol_f32_stream_ws_bytes(int n, int b, int mode)
+{
+    size_t bytes = lnb_align256((size_t)((b + 31) / 32) * 1024 * sizeof(float)) + 256;
+    bytes += (mode == LNB_FACTOR_TF32X3 ? 2 : 1) * lnb_align256((size_t)n * ldk_of(n) * 4);
+    return bytes + 4096;
+}
+
+static int upd_tc(int mode, const float *hi, const float *lo, int64_t kstride, float *C, int64_t ldc, int64_t nrows,
+                  int64_t c0, int64_t c1, int k, lnb_status_t *st, cudaStream_t s)
+{
+    if (nrows <= c0 || c1 <= c0) return 0;
+    const double w = (double)(c1 - c0);
+    const double pairs = w * (double)nrows - (double)(c0 + c1 - 1) * w / 2.0;
+    const int prof = lnb_prof_begin(s);
+    const int e = lnb_k_tc_syrk_lower(mode == LNB_FACTOR_TF32X3 ? 0 : 1, hi, lo, kstride, nrows, C, ldc, nrows, c0,
+                                      c1, k, NULL, st, lnb_wait_ns(), s);
+    const double opb = mode == LNB_FACTOR_TF32X3 ? 8.0 : 4.0;
+    lnb_prof_end(prof, s, 2.0 * k * pairs, opb * (double)k * ((double)(nrows - c0) + w) + 8.0 * pairs);
+    return e;
+}
+
+/* block columns j0..j1 of the working matrix from the arrived FP64 data, then
+ * the update with panels 0..kdone-1 (K = kdone b) */
+static int join_cols(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, const lnb_stream_in *in,
+                     const float *HA, const float *LA, int64_t ldk, int j0, int j1, int kdone, cudaStream_t s)
+{
+    const int64_t c0 = (int64_t)j0 * b, c1 = ((int64_t)j1 + 1) * b < n ? ((int64_t)j1 + 1) * b : n;
+    for (int j = j0; j <= j1; ++j) CK(cudaStreamWaitEvent(s, in->arr[j], 0), "arrival wait");
+    CK(lnb_k_lower_to_f32_cols(in->A, in->lda, n, c0, c1, in->S, dA, lda, s), "convert");
+    if (kdone > 0)
+        CK(upd_tc(mode, HA + c0 * ldk, LA ? LA + c0 * ldk : NULL, ldk, dA + c0 + c0 * lda, lda, n - c0, 0, c1 - c0,
+                  kdone * b, c->st, s), "catch-up update");
+    return 0;
+}
+
+int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_refactor_ctx *rf,
+                            const lnb_stream_in *in, lnb_arena *ar, cudaStream_t s)
+{
+    if (!lnb_chol_f32_stream_ok(n, b, mode)) return lnb_set_error(LNB_EINVAL, "streamed factor: n %d, b %d", n, b);
+    const int64_t ldk = ldk_of(n);
+    float *dinv = (float *)lnb_arena_take(ar, (size_t)((b + 31) / 32) * 1024 * sizeof(float));
+    float *HA = (float *)lnb_arena_take(ar, (size_t)n * ldk * 4);
+    float *LA = mode == LNB_FACTOR_TF32X3 ? (float *)lnb_arena_take(ar, (size_t)n * ldk * 4) : NULL;
+    if (!dinv || !HA || (mode == LNB_FACTOR_TF32X3 && !LA))
+        return lnb_set_error(LNB_ENOMEM, "streamed factor workspace");
+    cudaStream_t crit = c->crit;
+    cudaEvent_t ev_start = c->ev[0], ev_trsm = c->ev[1], ev_next = c->ev[2], ev_done = c->ev[3];
+    CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
+    CK(cudaEventRecord(ev_start, s), "event");
+    CK(cudaStreamWaitEvent(crit, ev_start, 0), "event wait");
+
+    const int mt = (n + b - 1) / b;
+    const int ahead = stream_ahead() < 0 ? 0 : stream_ahead();
+    int joined = 0, e;   /* block columns 0..joined are converted and updated by every finished panel */
+    if ((e = join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, 0, 0, 0, crit))) return e;
+    for (int k = 0; k < mt; ++k) {
+        const int64_t k0 = (int64_t)k * b;
+        const int bs = (int)(n - k0 < b ? n - k0 : b);
+        float *Akk = dA + k0 + k0 * lda;
+        const int64_t mrem = n - k0 - bs;
+        { int _e = lnb_potrf_tile_f32(Akk, lda, bs, k0, dinv, c->st, crit); if (_e) return _e; }
+        if (rf) {
+            int info = lnb_status_read(c, crit);
+            if (info < 0) return info;
+            if (info > 0 && (e = refactor_tile(c, rf, dA, lda, k0, bs, b, dinv, ar, crit))) return e;
+        }
+        if (mrem <= 0) break;
+        float *hk = HA + (k0 + bs) * ldk + k0, *lk = LA ? LA + (k0 + bs) * ldk + k0 : NULL;
+        CK(lnb_k_trsm_rlt_prep_f32(Akk, lda, dinv, Akk + bs, lda, mrem, bs, hk, lk, (int)ldk, crit), "trsm+prep f32");
+        CK(cudaEventRecord(ev_trsm, crit), "event");
+        /* block columns whose data is here, as far as the host can tell now */
+        const int need = k + 2 < mt ? k + 2 : mt - 1;
+        const int cap = need + ahead < mt - 1 ? need + ahead : mt - 1;
+        int avail = joined;
+        while (avail + 1 <= cap && cudaEventQuery(in->arr[avail + 1]) == cudaSuccess) ++avail;
+        cudaGetLastError();   /* cudaErrorNotReady from the queries */
+        float *Ct = Akk + bs + (int64_t)bs * lda;
+        const int64_t nb1 = b < mrem ? b : mrem;
+        const int64_t nb2 = 2 * (int64_t)b < mrem ? 2 * (int64_t)b : mrem;
+        /* block column k+1 (the next panel) on the critical stream */
+        if (k + 1 > joined) {
+            if ((e = join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, k + 1, k + 1, k + 1, crit))) return e;
+        } else {
+            CK(upd_tc(mode, hk, lk, ldk, Ct, lda, mrem, 0, nb1, bs, c->st, crit), "update next panel");
+        }
+        CK(cudaStreamWaitEvent(s, ev_trsm, 0), "event wait");
+        if (k + 2 < mt) {
+            if (k + 2 > joined) {
+                if ((e = join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, k + 2, k + 2, k + 1, s))) return e;
+            } else {
+                CK(upd_tc(mode, hk, lk, ldk, Ct, lda, mrem, nb1, nb2, bs, c->st, s), "update panel k+2");
+            }
+        }
+        CK(cudaEventRecord(ev_next, s), "event");
+        /* the other joined columns take panel k; newly arrived ones catch up */
+        if (joined > k + 2) {
+            const int64_t r1 = ((int64_t)joined + 1) * b < n ? ((int64_t)joined + 1) * b - (k0 + bs) : mrem;
+            CK(upd_tc(mode, hk, lk, ldk, Ct, lda, mrem, nb2, r1, bs, c->st, s), "update rest");
+        }
+        const int jn = (joined > need ? joined : need) + 1;
+        if (avail >= jn && (e = join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, jn, avail, k + 1, s))) return e;
+        if (need > joined) joined = need;
+        if (avail > joined) joined = avail;
         CK(cudaStreamWaitEvent(crit, ev_next, 0), "event wait");
     }
     CK(cudaEventRecord(ev_done, crit), "event");

@@ -85,6 +85,20 @@ size_t lnb_refactor_ws_bytes(int b);
 int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_refactor_ctx *rf,
                      lnb_arena *ar, cudaStream_t s);
 int lnb_get_factor_mode(void);
+/* A matrix arriving block column by block column on another stream: block
+ * column j (columns [j b, (j+1) b), rows >= j b) of the FP64 copy A is
+ * complete once arr[j] has fired; S is the equilibration scale on the device. */
+typedef struct {
+    const double *A;
+    int64_t lda;
+    const double *S;
+    cudaEvent_t *arr;
+} lnb_stream_in;
+int lnb_chol_f32_stream_ok(int n, int b, int mode);
+size_t lnb_chol_f32_stream_ws_bytes(int n, int b, int mode);
+/* the FP32 factorization of lower(S A S) into dA while A arrives (see in) */
+int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_refactor_ctx *rf,
+                            const lnb_stream_in *in, lnb_arena *ar, cudaStream_t s);
 
 /* ---- FP64 triangular solves on device memory (lnb_solve.c) --------------- */
 size_t lnb_trsm_f64_ws_bytes(int64_t n);

@@ -99,9 +99,15 @@ int lnb_k_prep_bf16(const float *X, int64_t ldx, int64_t m, int kb, int kpad, fl
 /* A32 = lower(S A S) in FP32 with S = diag(1/sqrt(a_ii)) (S = I if !equilibrate) */
 int lnb_k_lower_to_f32(const double *A, int64_t lda, int64_t n, int equilibrate, double *s_out,
                        float *A32, int64_t ld32, lnb_stream_t s);
+/* A32 columns [c0, c1), rows >= column: lower(S A S) in FP32, S given */
+int lnb_k_lower_to_f32_cols(const double *A, int64_t lda, int64_t n, int64_t c0, int64_t c1, const double *S,
+                            float *A32, int64_t ld32, lnb_stream_t s);
+/* s[i] = 1/sqrt(a[i]) (1 when !on or a[i] <= 0) from a packed diagonal; s may alias a */
+int lnb_k_equil_scale_vec(const double *a, int64_t n, int on, double *s, lnb_stream_t st);
 /* tensor-core lower update (k_tc_update.cu); mode 0 TF32x3, 1 TF32, 2 BF16.
- * hi/lo: K-major operand copies (prow rows x kpad); C FP32 column-major. */
-int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int kpad, int64_t prow, float *C,
+ * hi/lo: K-major operand copies (prow rows, row stride kstride, first kdim K
+ * columns used); C FP32 column-major. */
+int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int64_t kstride, int64_t prow, float *C,
                         int64_t ldc, int64_t nrows, int64_t c0, int64_t c1, int kdim, const float *scale,
                         lnb_status_t *st, long long wait_ns, lnb_stream_t s);
 

@@ -58,7 +58,7 @@ typedef struct {
     int *sync;
 } irws;
 
-static size_t ir_ws_bytes(int64_t n, int64_t nrhs, int b, int mode)
+static size_t ir_ws_bytes(int64_t n, int64_t nrhs, int b, int mode, int streamed)
 {
     const int64_t ld32 = (n + 31) & ~(int64_t)31;
     const int64_t nb = (n + TRSV_H - 1) / TRSV_H;
@@ -66,7 +66,8 @@ static size_t ir_ws_bytes(int64_t n, int64_t nrhs, int b, int mode)
                lnb_align256((size_t)nb * TRSV_H * TRSV_H * 8) + 5 * lnb_align256((size_t)n * nrhs * 8) +
                lnb_align256((size_t)8 * (nrhs + 1) * 8) +
                lnb_align256((size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4) + 4096;
-    return s + lnb_chol_f32_ws_bytes((int)n, b, mode) + lnb_refactor_ws_bytes(b);
+    return s + (streamed ? lnb_chol_f32_stream_ws_bytes((int)n, b, mode) : lnb_chol_f32_ws_bytes((int)n, b, mode)) +
+           lnb_refactor_ws_bytes(b);
 }
 
 /* z = M^-1 r = S L^-T L^-1 S r   (in place in Z, reading R) */
@@ -107,8 +108,40 @@ static int residual(lnb_ctx *c, const irws *w, const double *dA, int64_t lda, co
     return 0;
 }
 
+/* streamed input of the host entry point: A arrives block column by block
+ * column (arr); the equilibration scale dS is already on the device */
+typedef struct {
+    const double *dS;
+    cudaEvent_t *arr;
+} ir_stream;
+
+static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda, const double *dB, int ldb,
+                  double *dX, int ldx, const lnb_ir_opts *opts_in, lnb_ir_result *res, cudaStream_t s,
+                  lnb_arena *arp, const ir_stream *in);
+
 int lnb_dsposv_ir_dev(int n, int nrhs, int b, const double *dA, int lda, const double *dB, int ldb, double *dX,
                       int ldx, const lnb_ir_opts *opts_in, lnb_ir_result *res, void *stream)
+{
+    if (n < 0 || nrhs < 0 || b <= 0 || b > 1024 || lda < (n > 1 ? n : 1) || ldb < (n > 1 ? n : 1) ||
+        ldx < (n > 1 ? n : 1))
+        return lnb_set_error(LNB_EINVAL, "dsposv_ir arguments");
+    if (nrhs > 64) return lnb_set_error(LNB_EINVAL, "dsposv_ir: nrhs = %d > 64", nrhs);
+    const int mode = opts_in ? opts_in->factor : LNB_FACTOR_TF32X3;
+    if (n == 0 || nrhs == 0) {
+        if (res) memset(res, 0, sizeof *res);
+        return 0;
+    }
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    void *ws = lnb_ws(c, ir_ws_bytes(n, nrhs, b, mode, 0));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    return ir_run(c, n, nrhs, b, dA, lda, dB, ldb, dX, ldx, opts_in, res, (cudaStream_t)stream, &ar, NULL);
+}
+
+static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda, const double *dB, int ldb,
+                  double *dX, int ldx, const lnb_ir_opts *opts_in, lnb_ir_result *res, cudaStream_t s,
+                  lnb_arena *arp, const ir_stream *in)
 {
     lnb_ir_opts opts;
     if (opts_in) opts = *opts_in;
@@ -123,11 +156,7 @@ int lnb_dsposv_ir_dev(int n, int nrhs, int b, const double *dA, int lda, const d
     lnb_ir_result rr;
     memset(&rr, 0, sizeof rr);
     if (n == 0 || nrhs == 0) { if (res) *res = rr; return 0; }
-    lnb_ctx *c = lnb_ctx_get();
-    if (!c) return LNB_ENODEV;
-    void *ws = lnb_ws(c, ir_ws_bytes(n, nrhs, b, mode));
-    if (!ws) return LNB_ENOMEM;
-    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    lnb_arena ar = *arp;
     irws w;
     w.n = n; w.nrhs = nrhs; w.ld32 = ((int64_t)n + 31) & ~(int64_t)31;
     const int64_t nb = ((int64_t)n + TRSV_H - 1) / TRSV_H;
@@ -143,14 +172,21 @@ int lnb_dsposv_ir_dev(int n, int nrhs, int b, const double *dA, int lda, const d
     w.scal = lnb_arena_take(&ar, (size_t)8 * (nrhs + 1) * 8);
     w.sync = lnb_arena_take(&ar, (size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4);
     if (!w.sync) return lnb_set_error(LNB_ENOMEM, "dsposv_ir workspace");
-    cudaStream_t s = (cudaStream_t)stream;
     const double tol = opts.tol > 0 ? opts.tol : 10.0 * n * LAPACK_EPS;
 
     /* ---- factor ---- */
     CK(cudaEventRecord(c->t0, s), "event");
-    CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, s), "convert");
     lnb_refactor_ctx rf = {dA, lda, w.S, 0, 0};
-    int e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &rf, &ar, s);
+    int e;
+    if (in) {
+        /* the matrix is converted block column by block column as it arrives */
+        CK(cudaMemcpyAsync(w.S, in->dS, (size_t)n * 8, cudaMemcpyDeviceToDevice, s), "scale");
+        const lnb_stream_in sin = {dA, lda, w.S, in->arr};
+        e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, &sin, &ar, s);
+    } else {
+        CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, s), "convert");
+        e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &rf, &ar, s);
+    }
     rr.refactored_tiles = rf.refactored;
     if (e) {
         if (e > 0 && res) { rr.info = e; *res = rr; }
@@ -252,40 +288,81 @@ int lnb_dsposv_ir_dev(int n, int nrhs, int b, const double *dA, int lda, const d
 int lnb_dsposv_ir(int n, int nrhs, int b, const double *A, int lda, const double *B, int ldb, double *X, int ldx,
                   const lnb_ir_opts *opts, lnb_ir_result *res)
 {
-    if (n < 0 || nrhs < 0 || lda < (n > 1 ? n : 1) || ldb < (n > 1 ? n : 1) || ldx < (n > 1 ? n : 1))
+    if (n < 0 || nrhs < 0 || b <= 0 || b > 1024 || lda < (n > 1 ? n : 1) || ldb < (n > 1 ? n : 1) ||
+        ldx < (n > 1 ? n : 1))
         return lnb_set_error(LNB_EINVAL, "dsposv_ir arguments");
-    if (n == 0 || nrhs == 0) return 0;
+    if (nrhs > 64) return lnb_set_error(LNB_EINVAL, "dsposv_ir: nrhs = %d > 64", nrhs);
+    if (n == 0 || nrhs == 0) {
+        if (res) memset(res, 0, sizeof *res);
+        return 0;
+    }
     if (!A || !B || !X) return lnb_set_error(LNB_EINVAL, "NULL argument");
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
+    const int mode = opts ? opts->factor : LNB_FACTOR_TF32X3;
+    /* the FP32 factorization starts while A is still crossing PCIe when the
+     * mode allows it (TF32 update paths, b a multiple of 32) */
+    const int streamed = lnb_chol_f32_stream_ok(n, b, mode);
     const int64_t ldd = ((int64_t)n + 7) & ~(int64_t)7;
-    double *dA = NULL, *dB = NULL, *dX = NULL;
-    if (cudaMalloc((void **)&dA, (size_t)ldd * n * 8) != cudaSuccess ||
-        cudaMalloc((void **)&dB, (size_t)ldd * nrhs * 8) != cudaSuccess ||
-        cudaMalloc((void **)&dX, (size_t)ldd * nrhs * 8) != cudaSuccess) {
-        cudaFree(dA); cudaFree(dB); cudaFree(dX);
-        cudaGetLastError();
-        return lnb_set_error(LNB_ENOMEM, "dsposv_ir: device buffers");
-    }
+    const size_t abytes = lnb_align256((size_t)ldd * n * 8), vbytes = lnb_align256((size_t)ldd * nrhs * 8);
+    void *ws = lnb_ws(c, abytes + 2 * vbytes + lnb_align256((size_t)n * 8) + 1024 +
+                          ir_ws_bytes(n, nrhs, b, mode, streamed));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    double *dA = lnb_arena_take(&ar, (size_t)ldd * n * 8);
+    double *dB = lnb_arena_take(&ar, (size_t)ldd * nrhs * 8);
+    double *dX = lnb_arena_take(&ar, (size_t)ldd * nrhs * 8);
+    double *dS = lnb_arena_take(&ar, (size_t)n * 8);
+    if (!dS) return lnb_set_error(LNB_ENOMEM, "dsposv_ir: device buffers");
     cudaStream_t s = c->main;
-    int e = 0;
-    /* lower block-columns of A only: the solver never reads the upper triangle */
-    for (int64_t c0 = 0; c0 < n && !e; c0 += 512) {
-        const int64_t wd = n - c0 < 512 ? n - c0 : 512;
-        if (cudaMemcpy2DAsync(dA + c0 + c0 * ldd, ldd * 8, A + c0 + c0 * (int64_t)lda, (size_t)lda * 8,
-                              (size_t)(n - c0) * 8, wd, cudaMemcpyHostToDevice, s) != cudaSuccess)
-            e = lnb_cuda_error(cudaGetLastError(), "A in");
+    const int64_t cw = streamed ? b : 512;   /* block columns of the copy: the factor's tiles when streamed */
+    const int nblk = (int)((n + cw - 1) / cw);
+    double *diag = NULL;
+    cudaEvent_t *arr = NULL;
+    int e = 0, nev = 0;
+    if (streamed) {
+        diag = (double *)malloc((size_t)n * 8);
+        arr = (cudaEvent_t *)calloc((size_t)nblk, sizeof(cudaEvent_t));
+        if (!diag || !arr) e = lnb_set_error(LNB_ENOMEM, "host buffers");
+        for (int64_t i = 0; !e && i < n; ++i) diag[i] = A[i + i * (int64_t)lda];
+        for (; !e && nev < nblk; ++nev)
+            if (cudaEventCreateWithFlags(&arr[nev], cudaEventDisableTiming) != cudaSuccess)
+                e = lnb_cuda_error(cudaGetLastError(), "arrival events");
     }
     if (!e && cudaMemcpy2DAsync(dB, ldd * 8, B, (size_t)ldb * 8, (size_t)n * 8, nrhs, cudaMemcpyHostToDevice, s) !=
                   cudaSuccess)
         e = lnb_cuda_error(cudaGetLastError(), "B in");
-    if (!e) e = lnb_dsposv_ir_dev(n, nrhs, b, dA, (int)ldd, dB, (int)ldd, dX, (int)ldd, opts, res, s);
+    /* equilibration scale from the host-side diagonal, ahead of the bulk copy */
+    if (!e && streamed) {
+        if (cudaMemcpyAsync(dS, diag, (size_t)n * 8, cudaMemcpyHostToDevice, s) != cudaSuccess)
+            e = lnb_cuda_error(cudaGetLastError(), "diagonal");
+        else if ((e = lnb_k_equil_scale_vec(dS, n, opts ? opts->equilibrate : 1, dS, s)) != 0)
+            e = lnb_cuda_error(e, "scale");
+    }
+    /* lower block columns of A only (the solver never reads the upper
+     * triangle); streamed, on the copy stream with an event per block column */
+    cudaStream_t cs = streamed ? c->copy : s;
+    for (int j = 0; j < nblk && !e; ++j) {
+        const int64_t c0 = (int64_t)j * cw, wd = n - c0 < cw ? n - c0 : cw;
+        if (cudaMemcpy2DAsync(dA + c0 + c0 * ldd, ldd * 8, A + c0 + c0 * (int64_t)lda, (size_t)lda * 8,
+                              (size_t)(n - c0) * 8, wd, cudaMemcpyHostToDevice, cs) != cudaSuccess ||
+            (streamed && cudaEventRecord(arr[j], cs) != cudaSuccess))
+            e = lnb_cuda_error(cudaGetLastError(), "A in");
+    }
+    if (!e) {
+        const ir_stream in = {dS, arr};
+        e = ir_run(c, n, nrhs, b, dA, (int)ldd, dB, (int)ldd, dX, (int)ldd, opts, res, s, &ar, streamed ? &in : NULL);
+    }
     if (e >= 0 || e == LNB_ENOCONV) {
         if (cudaMemcpy2DAsync(X, (size_t)ldx * 8, dX, ldd * 8, (size_t)n * 8, nrhs, cudaMemcpyDeviceToHost, s) !=
                 cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess)
             e = lnb_cuda_error(cudaGetLastError(), "X out");
     }
-    cudaFree(dA); cudaFree(dB); cudaFree(dX);
+    /* nothing may still be writing the cached buffers when this returns */
+    if (streamed) cudaStreamSynchronize(c->copy);
+    for (int j = 0; j < nev; ++j) cudaEventDestroy(arr[j]);
+    free(arr);
+    free(diag);
     return e;
 }

@@ -110,3 +110,65 @@ def test_ir_device_api_leaves_A_untouched(lnb, cuda):
     X = Xt.cpu().numpy().T
     assert O.backward_error_np(A0, X, B0) <= 10 * n * EPS
     assert res["factor_ms"] > 0 and res["solve_ms"] > 0
+
+
+@pytest.mark.parametrize("ahead", [None, "0", "1"])
+@pytest.mark.parametrize("factor,n,b", [("FACTOR_TF32X3", 6000, 512), ("FACTOR_TF32", 3000, 256)])
+def test_ir_streamed_host_path(lnb, cuda, monkeypatch, ahead, factor, n, b):
+    """The host entry point factors while A is still arriving: block columns
+    join the right-looking schedule through a catch-up update with every
+    finished panel.  LNB_STREAM_AHEAD = 0 forces a catch-up at every step (K
+    growing to n), 1 a mix; unset, columns join as soon as they land.  Every
+    variant refines to the FP64 bar and agrees with the device entry point."""
+    import torch
+    if ahead is None:
+        monkeypatch.delenv("LNB_STREAM_AHEAD", raising=False)
+    else:
+        monkeypatch.setenv("LNB_STREAM_AHEAD", ahead)
+    A0 = O.spd_covariance(n, 1e-3, seed=n)
+    B0 = np.asfortranarray(np.random.default_rng(n).standard_normal((n, 2)))
+    X, res = check(lnb, A0, B0, b, getattr(lnb, factor))
+    assert not res["used_pcg"] and res["refactored_tiles"] == 0
+    At = torch.tensor(np.ascontiguousarray(A0.T), device=cuda)
+    Bt = torch.tensor(np.ascontiguousarray(B0.T), device=cuda)
+    Xt = torch.zeros_like(Bt)
+    rc, res_d = lnb.dsposv_ir_dev(At, Bt, Xt, n, 2, b, lnb.ir_opts(factor=getattr(lnb, factor)))
+    torch.cuda.synchronize()
+    assert rc == 0
+    Xd = Xt.cpu().numpy().T
+    bound = 2 * np.linalg.cond(A0, np.inf) * 10 * n * EPS
+    assert np.abs(X - Xd).max() / np.abs(Xd).max() <= 2 * bound
+    assert abs(res["iterations"] - res_d["iterations"]) <= 1
+
+
+def near_singular_pair(n, i, eps):
+    """I with the 2 x 2 principal block [[1, 1 - eps], [1 - eps, 1]] at (i, i):
+    SPD (eigenvalues eps and 2 - eps), but 1 - eps rounds to 1 in FP32, so the
+    low-precision pivot of row i + 1 is exactly zero."""
+    A = np.eye(n)
+    A[i, i + 1] = A[i + 1, i] = 1.0 - eps
+    return np.asfortranarray(A)
+
+
+@pytest.mark.parametrize("api", ["host", "device"])
+def test_ir_fp64_refactor_of_failed_tile(lnb, cuda, api):
+    """A low-precision pivot that fails on an SPD matrix: the diagonal tile is
+    rebuilt in FP64 from the original matrix and refactored, and the solve
+    still reaches the FP64 bar (with the PCG fallback if refinement stalls)."""
+    import torch
+    n, b = 1024, 256
+    A0 = near_singular_pair(n, 300, 1e-9)
+    B0 = np.asfortranarray(np.random.default_rng(8).standard_normal((n, 1)))
+    opts = lnb.ir_opts(factor=lnb.FACTOR_TF32X3, max_iter=10, pcg_max_iter=100)
+    if api == "host":
+        rc, X, res = lnb.dsposv_ir(A0.copy(order="F"), B0, b, opts)
+    else:
+        At = torch.tensor(np.ascontiguousarray(A0.T), device=cuda)
+        Bt = torch.tensor(np.ascontiguousarray(B0.T), device=cuda)
+        Xt = torch.zeros_like(Bt)
+        rc, res = lnb.dsposv_ir_dev(At, Bt, Xt, n, 1, b, opts)
+        torch.cuda.synchronize()
+        X = Xt.cpu().numpy().T
+    assert rc == 0, (rc, res, lnb.last_error())
+    assert res["refactored_tiles"] >= 1
+    assert O.backward_error_np(A0, X, B0) <= 10 * n * EPS
