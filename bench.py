@@ -533,13 +533,18 @@ def ours_arm(args, world, rank, local):
         ach = per_flops / (per_ms * 1e-3) / 1e12
         if w["factor"] == "FP64":
             peak, src, kern = peaks["fp64"], "cuBLAS dgemm 8192^3 measured in this run", "k_syrk_lower_f64 (DMMA)"
-        elif w["factor"] == "TF32X3":
-            peak, src = peaks["tf32"] / 3.0, "cuBLAS TF32 GEMM 8192^3 measured in this run, / 3 products"
-            kern = "k_tc_syrk_lower<TF32X3> (tcgen05)"
-        elif w["factor"] == "BF16":
-            peak, src, kern = peaks["bf16"], "MEASURED_PEAKS.json bf16_tflops", "k_tc_syrk_lower<BF16> (tcgen05)"
         else:
-            peak, src, kern = peaks["tf32"], "cuBLAS TF32 GEMM measured in this run", "k_tc_syrk_lower"
+            # the library runs the update on CTA pairs unless LNB_TC_PAIR=0
+            pair = os.environ.get("LNB_TC_PAIR", "1") != "0"
+            name = "k_tc2_syrk_lower" if pair else "k_tc_syrk_lower"
+            how = "(tcgen05, CTA pairs)" if pair else "(tcgen05)"
+            if w["factor"] == "TF32X3":
+                peak, src = peaks["tf32"] / 3.0, "cuBLAS TF32 GEMM 8192^3 measured in this run, / 3 products"
+                kern = f"{name}<TF32X3> {how}"
+            elif w["factor"] == "BF16":
+                peak, src, kern = peaks["bf16"], "MEASURED_PEAKS.json bf16_tflops", f"{name}<BF16> {how}"
+            else:
+                peak, src, kern = peaks["tf32"], "cuBLAS TF32 GEMM measured in this run", f"{name}<TF32> {how}"
         line["roofline"] = {"bound": "tensor", "achieved": round(ach, 3), "peak": round(peak, 3),
                             "unit": "TFLOP/s", "frac": round(ach / peak, 4),
                             "traffic": traffic_from_profiles(kern.split()[0],

@@ -553,7 +553,11 @@ extern "C" int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int
         int64_t mt2 = tc_max_tiles() * 512 / (4 * (int64_t)kdim);   // a pair tile is four 128 x 128 tiles
         if (mt2 < 1) mt2 = 1;
         const int64_t pcap = (t2.count + mt2 - 1) / mt2;
-        if (pcap > pairs) pairs = pcap;
+        // more pairs than fit at once: whole waves, so that no pair runs its
+        // tiles after all the others have finished
+        const int64_t slots = sms / 2;
+        if (pcap > pairs) pairs = (pcap + slots - 1) / slots * slots;
+        if (pairs > t2.count) pairs = t2.count;
         dim3 grid2((unsigned)(2 * pairs));
         switch (mode) {
         case MODE_TF32X3:
@@ -586,7 +590,8 @@ extern "C" int lnb_k_tc_syrk_lower(int mode, const void *hi, const void *lo, int
     int64_t mt = tc_max_tiles() * 512 / kdim;
     if (mt < 1) mt = 1;
     const int64_t gcap = (tl.count + mt - 1) / mt;
-    if (gcap > g) g = gcap;
+    if (gcap > g) g = (gcap + sms - 1) / sms * sms;   // whole waves
+    if (g > tl.count) g = tl.count;
     dim3 grid((unsigned)g);
     switch (mode) {
     case MODE_TF32X3:
