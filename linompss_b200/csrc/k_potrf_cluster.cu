@@ -10,14 +10,17 @@
 // 32-column step j runs as
 //   (a) the owner of block row j factors its diagonal block in registers and
 //       forms X = L_jj^-1, which it stores into every CTA's shared memory;
-//   (c) every CTA solves its blocks below: L_ij = A_ij X^T, written to global
-//       memory and into every CTA's panel buffer (distributed shared memory);
+//   (c) every CTA solves its blocks below: L_ij = A_ij X^T, kept in its own
+//       slot and stored into every CTA's panel buffer (distributed shared
+//       memory);
 //   (e) every CTA updates its blocks A_ik -= L_ij L_kj^T, k in (j, i]; the
 //       owner of block row j + 1 updates that diagonal block first and factors
 //       it (step (a) of j + 1) while its other warps continue the update.
-// Hardware cluster barriers separate the phases; there is no spin-wait.
-// The per-block inverses X are written to dinv (column-major, 32 x 32 each)
-// for the panel solve that follows.
+// Hardware cluster barriers separate the phases; there is no spin-wait.  The
+// sweep stores nothing to global memory (each barrier's release would wait for
+// such stores); the finished blocks and the per-block inverses X (dinv,
+// column-major 32 x 32 each, for the panel solve that follows) are written out
+// after it.
 //
 // Algorithm: right-looking blocked Cholesky as in the reference's tile
 // schedule (src/chol_rl.c, POTRF/TRSM/SYRK/GEMM per step), applied inside one
@@ -36,7 +39,7 @@ constexpr int PNT = 256;             // threads per CTA
 constexpr int PBK = 32 * 32;         // floats in one block
 constexpr int PXS = 36;              // column stride of the shared inverse (conflict-free stores)
 constexpr int POWN = 2 * PCS + 1;    // blocks owned per CTA (rows q and 2 PCS - 1 - q)
-constexpr int PC_SMEM = ((POWN + PNB) * PBK + 32 * PXS + 32) * 4 + 16;
+constexpr int PC_SMEM = ((POWN + PNB) * PBK + 3 * 32 * PXS + 32) * 4 + 16;
 
 LNB_DEV int pc_owner(int i) { return i < PCS ? i : 2 * PCS - 1 - i; }
 // shared-memory slot of block (i, k), k <= i, in its owner q
@@ -114,11 +117,12 @@ LNB_DEV void pc_update(float *C, const float *P1, const float *P2, int lane)
     }
 }
 
-// step (a) for block row j by one warp of its owner: factor, inverse to every
-// CTA, L_jj and X to global memory; on failure the first bad row is published
-// to every CTA and dinv gets identity blocks from j on
-LNB_DEV void pc_diag_step(cg::cluster_group &cl, float *A, int64_t lda, int nb, int j, int64_t row0, float *own,
-                          float *inv, float *rv, int *s_fail, float *dinv, lnb_status_t *st, int q, int lane)
+// step (a) for block row j by one warp of its owner: factor (L_jj stays in its
+// slot), inverse into this CTA's xd area and to every CTA's inv buffer; on
+// failure the first bad row is published to every CTA.  Nothing goes to global
+// memory here: the write-out after the sweep does that.
+LNB_DEV void pc_diag_step(cg::cluster_group &cl, int nb, int j, int64_t row0, float *own, float *inv, float *xd,
+                          float *rv, int *s_fail, lnb_status_t *st, int q, int lane)
 {
     float *D = own + pc_slot(j, j, q) * PBK;
     const int bad = pc_factor_block(D, rv, lane);
@@ -128,23 +132,14 @@ LNB_DEV void pc_diag_step(cg::cluster_group &cl, float *A, int64_t lda, int nb, 
             atomicCAS(&st->info, 0, (int)(row0 + fail));
             for (int r = 0; r < PCS; ++r) *cl.map_shared_rank(s_fail, r) = fail;
         }
-        for (int e = lane; e < (nb - j) * PBK; e += 32) {
-            const int f = e % PBK;
-            dinv[(int64_t)j * PBK + e] = (f % 32 == f / 32) ? 1.f : 0.f;
-        }
         return;
     }
-    // L_jj, lower triangle only (the upper part of the tile is left untouched)
-    float *Ag = A + (int64_t)j * 32 + (int64_t)j * 32 * lda;
-#pragma unroll 4
-    for (int c = 0; c < 32; ++c)
-        if (c <= lane) Ag[lane + (int64_t)c * lda] = D[c * 32 + lane];
     float x[32];
     pc_inverse(D, rv, lane, x);
-    float *dg = dinv + (int64_t)j * PBK + lane * 32;
+    float *xl = xd + (j == q ? 0 : 32 * PXS) + lane * PXS;
 #pragma unroll
     for (int t = 0; t < 8; ++t)
-        *reinterpret_cast<float4 *>(dg + 4 * t) = make_float4(x[4 * t], x[4 * t + 1], x[4 * t + 2], x[4 * t + 3]);
+        *reinterpret_cast<float4 *>(xl + 4 * t) = make_float4(x[4 * t], x[4 * t + 1], x[4 * t + 2], x[4 * t + 3]);
     if (j + 1 < nb) {
         for (int r = 0; r < PCS; ++r) {
             float *di = cl.map_shared_rank(inv, r) + lane * PXS;
@@ -163,7 +158,8 @@ __global__ void __cluster_dims__(PCS, 1, 1) __launch_bounds__(PNT, 1)
     float *own = pcs;                     // owned blocks, column-major 32 x 32
     float *pb = own + POWN * PBK;         // panel column j: pb[i] = L_ij
     float *inv = pb + PNB * PBK;          // X_j: inv[m PXS + p] = X[p][m]
-    float *rv = inv + 32 * PXS;           // 1 / L[c][c] of the block being factored
+    float *xd = inv + 32 * PXS;           // inverses of this CTA's diagonal blocks (rows i1, i2), same layout
+    float *rv = xd + 2 * 32 * PXS;        // 1 / L[c][c] of the block being factored
     int *s_fail = reinterpret_cast<int *>(rv + 32);
     cg::cluster_group cl = cg::this_cluster();
     const int q = (int)cl.block_rank();
@@ -185,7 +181,7 @@ __global__ void __cluster_dims__(PCS, 1, 1) __launch_bounds__(PNT, 1)
         cp_async_wait<0>();
     }
     cl.sync();                            // every CTA runs before any remote access
-    if (q == 0 && warp == 0) pc_diag_step(cl, A, lda, nb, 0, row0, own, inv, rv, s_fail, dinv, st, q, lane);
+    if (q == 0 && warp == 0) pc_diag_step(cl, nb, 0, row0, own, inv, xd, rv, s_fail, st, q, lane);
     cl.sync();
     for (int j = 0; j + 1 < nb; ++j) {
         if (*s_fail) break;               // the same value in every CTA after the barrier
@@ -220,9 +216,11 @@ __global__ void __cluster_dims__(PCS, 1, 1) __launch_bounds__(PNT, 1)
                     *reinterpret_cast<float4 *>(dp + p0 * 32 + r0) = o0;
                     *reinterpret_cast<float4 *>(dp + (p0 + 1) * 32 + r0) = o1;
                 }
-                float *Ag = A + (int64_t)(i * 32 + r0) + (int64_t)(j * 32 + p0) * lda;
-                *reinterpret_cast<float4 *>(Ag) = o0;
-                *reinterpret_cast<float4 *>(Ag + lda) = o1;
+                // L_ij replaces A_ij in its slot once the group's four warps have read A_ij
+                asm volatile("bar.sync %0, 128;" ::"r"(1 + (warp >> 2)) : "memory");
+                float *Lo = own + pc_slot(i, j, q) * PBK;
+                *reinterpret_cast<float4 *>(Lo + p0 * 32 + r0) = o0;
+                *reinterpret_cast<float4 *>(Lo + (p0 + 1) * 32 + r0) = o1;
             }
         }
         cl.sync();
@@ -239,10 +237,48 @@ __global__ void __cluster_dims__(PCS, 1, 1) __launch_bounds__(PNT, 1)
             }
             if (diag_next && warp == 0) {
                 __syncwarp();
-                pc_diag_step(cl, A, lda, nb, j + 1, row0, own, inv, rv, s_fail, dinv, st, q, lane);
+                pc_diag_step(cl, nb, j + 1, row0, own, inv, xd, rv, s_fail, st, q, lane);
             }
         }
         cl.sync();
+    }
+    // Write-out.  A cluster barrier is a release: it waits until the CTA's earlier
+    // global stores are acknowledged, so the sweep keeps every finished block in
+    // shared memory and they all leave here.  Blocks (i, k) with k < jf are final
+    // (jf = the block of a failed pivot, nb without one); the others, like the
+    // upper triangle of the tile, keep their values in global memory.  Inverses:
+    // the factored diagonal blocks', identity from jf on.
+    const int fail = *s_fail;
+    const int jf = fail ? (fail - 1) / 32 : nb;
+    for (int rr = 0; rr < 2; ++rr) {
+        const int i = rr == 0 ? i1 : i2;
+        if (i >= nb) continue;
+        const int kend = i + 1 < jf ? i + 1 : jf;
+        for (int idx = tid; idx < kend * 256; idx += PNT) {
+            const int k = idx >> 8, e = idx & 255, c = e >> 3, r = 4 * (e & 7);
+            const float4 v = *reinterpret_cast<const float4 *>(own + pc_slot(i, k, q) * PBK + c * 32 + r);
+            float *g = A + (int64_t)(i * 32 + r) + (int64_t)(k * 32 + c) * lda;
+            if (k < i) {
+                *reinterpret_cast<float4 *>(g) = v;
+            } else {
+                if (r >= c) g[0] = v.x;
+                if (r + 1 >= c) g[1] = v.y;
+                if (r + 2 >= c) g[2] = v.z;
+                if (r + 3 >= c) g[3] = v.w;
+            }
+        }
+        // dinv block i, column-major: dinv[i 1024 + m 32 + p] = X[p][m]
+        for (int idx = tid; idx < 256; idx += PNT) {
+            const int m = idx >> 3, p = 4 * (idx & 7);
+            float4 v;
+            if (i < jf) {
+                v = *reinterpret_cast<const float4 *>(xd + rr * 32 * PXS + m * PXS + p);
+            } else {
+                v.x = (p == m) ? 1.f : 0.f; v.y = (p + 1 == m) ? 1.f : 0.f;
+                v.z = (p + 2 == m) ? 1.f : 0.f; v.w = (p + 3 == m) ? 1.f : 0.f;
+            }
+            *reinterpret_cast<float4 *>(dinv + (int64_t)i * PBK + m * 32 + p) = v;
+        }
     }
 }
 
