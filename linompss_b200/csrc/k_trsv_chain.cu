@@ -83,6 +83,15 @@ LNB_DEV void cp_async_mbar_arrive(uint64_t *bar)
 {
     asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
+// bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from
+// global to shared memory, counted on `bar`'s transaction count
+LNB_DEV void bulk_copy_g2s(void *smem, const void *gmem, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(smem)),
+                 "l"(gmem), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
 // hint: bring `bytes` (a multiple of 16, 16-byte aligned) into L2
 LNB_DEV void prefetch_l2(const void *p, uint32_t bytes)
 {
@@ -199,10 +208,11 @@ LNB_DEV void gemv_tile(const TT *S, const double *X, int m, int kq, double (&par
 template <bool TR>
 LNB_DEV int kd(int kq, int j) { return TR ? 2 * (kq + 4 * (j >> 1)) + (j & 1) : kq + 4 * j; }
 
-// inverse of op(T) on diagonal block i, this lane's 16 entries of row m
-// (stored in the precision of T, held in FP64)
+// inverse of op(T) on diagonal block i, this lane's 16 entries of row m, kept
+// in the precision of T: a conversion here would wait for each load, while the
+// raw values are first needed a step later
 template <bool TR, typename DT>
-LNB_DEV void load_dinv(const DT *dinv, int i, int m, int kq, double (&dv)[16])
+LNB_DEV void load_dinv(const DT *dinv, int i, int m, int kq, DT (&dv)[16])
 {
     const DT *D = dinv + (int64_t)i * TH * TH;   // inv(T_ii), column-major
     if constexpr (TR) {
@@ -219,7 +229,7 @@ LNB_DEV void load_dinv(const DT *dinv, int i, int m, int kq, double (&dv)[16])
         }
     } else {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) dv[j] = (double)__ldg(D + m + TH * kd<false>(kq, j));
+        for (int j = 0; j < 16; ++j) dv[j] = __ldg(D + m + TH * kd<false>(kq, j));
     }
 }
 
@@ -261,8 +271,23 @@ LNB_DEV void decode(int64_t q, int nb, int &row, int &chunk)
 
 struct ChainBars {
     uint64_t bfull[NBUF], bempty[NBUF], xfull[XR], xempty[XR];
+    uint64_t tfull[2];    // band tiles of a step landed (bulk path), by step parity
     int abort;
 };
+
+// the s-th step (s >= 1) stages its band tiles into buffer s & 1: the phase of
+// tfull[s & 1] it completes
+LNB_DEV uint32_t tile_phase(int s) { return (uint32_t)(((s & 1) ? (s - 1) >> 1 : (s - 2) >> 1) & 1); }
+static_assert(Cfg<float>::W * 64 <= NCOMP && Cfg<double>::W * 64 <= NCOMP, "one tile column per compute thread");
+
+// wait for copies this CTA issued before it leaves: bounded by budget_ns, and
+// unlike mbar_wait not cut short by an abort or a recorded timeout
+LNB_DEV void drain_wait(uint64_t *bar, uint32_t parity, long long budget_ns)
+{
+    const uint64_t t0 = globaltimer();
+    while (!tc::mbar_try_wait(bar, parity))
+        if ((long long)(globaltimer() - t0) > budget_ns) return;
+}
 
 template <typename TT, int NR, bool TR>
 __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
@@ -290,6 +315,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
         if (tid == 0) {
             for (int q = 0; q < NBUF; ++q) { tc::mbar_init(&cb->bfull[q], 8); tc::mbar_init(&cb->bempty[q], NCOMP); }
             for (int q = 0; q < XR; ++q) { tc::mbar_init(&cb->xfull[q], NCOMP); tc::mbar_init(&cb->xempty[q], 1); }
+            tc::mbar_init(&cb->tfull[0], 1);
+            tc::mbar_init(&cb->tfull[1], 1);
             cb->abort = 0;
             asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
@@ -368,24 +395,48 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
 
         // ---- compute warps ----
         const int m = tid >> 2, kq = tid & 3;
-        double dA[16], dB[16];
+        TT dA[16], dB[16];
         load_dinv<TR, TT>(a.dinv, blk(a, 0), m, kq, dA);
         bool okp = true;
+        // Whole 64 x 64 tiles with 16-byte-aligned columns: one bulk copy per
+        // tile column (one per compute thread), counted on tfull; otherwise
+        // cp.async in 16-byte pieces.
+        const bool bulk = a.vec && (a.n % TH == 0);
+        int staged = 0, consumed = 0;   // last step whose band tiles were issued / have landed (bulk path)
         // one chain step at position p; dcur holds inv(op T_pp), dnext receives the next one
-        auto step = [&](int p, double (&dcur)[16], double (&dnext)[16]) -> bool {
-            cp_async_wait<0>();
-            if (!bar_and(1, NCOMP, okp && !*(volatile int *)&cb->abort)) return false;
+        auto step = [&](int p, TT (&dcur)[16], TT (&dnext)[16]) -> bool {
+            bool okt = true;
+            if (!bulk) cp_async_wait<0>();
+            else if (p >= 1) {
+                okt = tc::mbar_wait(&cb->tfull[p & 1], tile_phase(p), a.wait_ns, &cb->abort, a.st);
+                if (okt) consumed = p;
+            }
+            if (!bar_and(1, NCOMP, okt && okp && !*(volatile int *)&cb->abort)) return false;
             // prefetch the band tiles of position p+1 and its inverse
             if (p + 1 < nb) {
                 const int ip = blk(a, p + 1);
+                TT *tb = tiles + ((p + 1) & 1) * W * TS;
+                if (bulk) {
+                    const int ntl = p + 1 < W ? p + 1 : W;
+                    if (tid == 0) tc::mbar_arrive_expect_tx(&cb->tfull[(p + 1) & 1], ntl * TH * TH * (int)sizeof(TT));
+                    const int k = 1 + (tid >> 6), col = tid & 63;
+                    if (k <= ntl) {
+                        const int jb = blk(a, p + 1 - k);
+                        const int rb = TR ? jb : ip, cbk = TR ? ip : jb;
+                        bulk_copy_g2s(tb + (k - 1) * TS + col * LD,
+                                      a.T + (int64_t)rb * TH + ((int64_t)cbk * TH + col) * a.ldt,
+                                      TH * (uint32_t)sizeof(TT), &cb->tfull[(p + 1) & 1]);
+                    }
+                    staged = p + 1;
+                } else {
 #pragma unroll
-                for (int k = 1; k <= W; ++k)
-                    if (p + 1 - k >= 0)
-                        stage_tile<TT, TR>(a, tiles + ((p + 1) & 1) * W * TS + (k - 1) * TS, ip, blk(a, p + 1 - k),
-                                           tid, NCOMP);
+                    for (int k = 1; k <= W; ++k)
+                        if (p + 1 - k >= 0)
+                            stage_tile<TT, TR>(a, tb + (k - 1) * TS, ip, blk(a, p + 1 - k), tid, NCOMP);
+                }
                 load_dinv<TR, TT>(a.dinv, ip, m, kq, dnext);
             }
-            cp_async_commit();
+            if (!bulk) cp_async_commit();
             // L2 prefetch PF steps ahead (band tiles, one column per thread, and the
             // diagonal inverse), so the cp.async of the next step is served from L2
             if (a.vec && p + PF < nb) {
@@ -422,7 +473,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
             for (int j = 0; j < 16; ++j) {
                 const int k = kd<TR>(kq, j);
 #pragma unroll
-                for (int r = 0; r < NR; ++r) xs[r] = fma(dcur[j], accs[r * TH + k], xs[r]);
+                for (int r = 0; r < NR; ++r) xs[r] = fma((double)dcur[j], accs[r * TH + k], xs[r]);
             }
             quad_sum<NR>(xs);
             const int i = blk(a, p);
@@ -445,6 +496,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
             if (ok && p + 1 < nb) ok = step(p + 1, dB, dA);
             if (!ok) {
                 cp_async_wait<0>();
+                // bulk copies still in flight land before the CTA leaves (bounded)
+                if (bulk && staged > consumed) drain_wait(&cb->tfull[staged & 1], tile_phase(staged), a.wait_ns);
                 if (tid == 0) { cb->abort = 1; atomicCAS(&a.st->timeout, 0, 3); a.st->timeout_item = p; }
                 return;
             }
