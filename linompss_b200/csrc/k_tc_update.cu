@@ -39,14 +39,11 @@ static int64_t tc_max_tiles()
 }
 
 // LNB_TC_PAIR=0 selects the single-CTA 128 x 128 kernel instead of CTA pairs
+// (read at every launch)
 static int tc_pair()
 {
-    static int v = -1;
-    if (v < 0) {
-        const char *e = getenv("LNB_TC_PAIR");
-        v = (e && *e) ? (atoi(e) != 0) : 1;
-    }
-    return v;
+    const char *e = getenv("LNB_TC_PAIR");
+    return (e && *e) ? (atoi(e) != 0) : 1;
 }
 
 template <int MODE>

@@ -137,3 +137,23 @@ def test_spotrs_chain_matches_fp64_solve(lnb, cuda, n, nrhs):
     got = Bt.cpu().numpy().T.astype(np.float64)
     # the device result is rounded to FP32 on the way out
     np.testing.assert_allclose(got, X, rtol=0, atol=2e-7 * np.abs(X).max())
+
+
+@pytest.mark.parametrize("mode", ["tf32x3", "tf32", "bf16"])
+@pytest.mark.parametrize("n,b", [(2048, 512), (1000, 256), (777, 200)])
+def test_update_cta_pairs_match_single_cta(lnb, monkeypatch, mode, n, b):
+    """The trailing update runs on 2-CTA clusters (256 x 256 tiles, cta_group::2
+    MMAs) by default; LNB_TC_PAIR=0 selects the single-CTA 128 x 128 kernel.
+    Both compute the same products in a different accumulation order, so the
+    factors agree to the precision of the mode and meet the same residual bound."""
+    A0 = O.spd_covariance(n, 1.0, seed=n + 11)
+    out = {}
+    for pair in ("1", "0"):
+        monkeypatch.setenv("LNB_TC_PAIR", pair)
+        lnb.set_factor_mode(MODES[mode])
+        A = np.asfortranarray(A0.astype(np.float32))
+        assert lnb.ompss_schol_rl(n, b, b, A, n) == 0
+        assert resid32(A0, A) <= RESID[mode]
+        out[pair] = np.tril(A).astype(np.float64)
+    tol = {"tf32x3": 2e-5, "tf32": 2e-3, "bf16": 2e-2}[mode]
+    np.testing.assert_allclose(out["1"], out["0"], rtol=0, atol=tol * np.abs(out["0"]).max())
