@@ -103,14 +103,50 @@ def barrier(world):
         dist.barrier()
 
 
+def _coll_device():
+    """tensors for collectives live where the process group's backend wants them"""
+    import torch.distributed as dist
+    return "cuda" if dist.get_backend() == "nccl" else "cpu"
+
+
 def allmax(world, v):
     if world == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device=_coll_device())
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def allgather_vec(world, vals):
+    """every rank's list of floats (same length on all ranks), as a world x k array"""
+    import numpy as np
+    if world == 1:
+        return np.asarray([vals], dtype=np.float64)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(vals, dtype=torch.float64, device=_coll_device())
+    out = torch.empty(world * t.numel(), dtype=torch.float64, device=t.device)
+    dist.all_gather_into_tensor(out, t)
+    return out.cpu().numpy().reshape(world, -1)
+
+
+def batch_shape(count, seed):
+    """orders and right-hand-side counts of the uneven batch: n ~ U{16..512}, nrhs ~ U{1..8}"""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return rng.integers(16, 513, count), rng.integers(1, 9, count)
+
+
+def shard_batch(ns, rs, world, rank):
+    """this rank's systems of the batch: longest-processing-time split by estimated
+    cost (lnb_batched_partition), the same on every rank"""
+    import numpy as np
+
+    import linompss_b200 as lnb
+    owner, load = lnb.batched_partition(ns, rs, world)
+    return np.nonzero(owner == rank)[0], load
 
 
 # ----------------------------------------------------------------------------
@@ -320,14 +356,13 @@ def traffic_from_profiles(kernel, alg_bytes_per_launch):
     return int(ratio * alg_bytes_per_launch)
 
 
-def make_batch(count, seed, device):
-    """`count` systems, n_i ~ U{16..512}, nrhs_i ~ U{1..8}, A_i = G G^T/n_i + 1e-2 I,
+def make_batch(ns, rs, seed, device):
+    """Systems of orders ns and right-hand-side counts rs, A_i = G G^T/n_i + 1e-2 I,
     packed column-major in one flat FP64 buffer (and B_i ~ N(0,1) likewise)."""
     import numpy as np
     import torch
-    rng = np.random.default_rng(seed)
-    ns = rng.integers(16, 513, count)
-    rs = rng.integers(1, 9, count)
+    ns = np.asarray(ns)
+    rs = np.asarray(rs)
     a_off = np.concatenate([[0], np.cumsum(ns.astype(np.int64) ** 2)[:-1]])
     b_off = np.concatenate([[0], np.cumsum(ns.astype(np.int64) * rs)[:-1]])
     A = torch.empty(int((ns.astype(np.int64) ** 2).sum()), dtype=torch.float64, device=device)
@@ -348,18 +383,22 @@ def make_batch(count, seed, device):
             t(b_off, torch.int64), A, B)
 
 
-def batched_arm(args, world, local, peaks):
+def batched_arm(args, world, rank, local, peaks):
     """Batched uneven solves: one persistent launch (autotuned panel width,
-    captured in a CUDA graph) against a loop of per-system plain FP64 solves."""
+    captured in a CUDA graph) against a loop of per-system plain FP64 solves.
+    With N GPUs the one batch is split across them (longest processing time
+    first on the estimated cost); the batch time is the slowest rank's."""
     import numpy as np
     import torch
 
     import linompss_b200 as lnb
     dev = torch.device("cuda", local)
     L = lnb.lib()
-    count = args.batch_count
-    ns, rs, a_off, b_off, nd, rd, ao, bo, dA, dB = make_batch(count, 4321 + local, dev)
-    flops = float(sum(n ** 3 / 3.0 + 2.0 * n * n * r for n, r in zip(ns.astype(float), rs.astype(float))))
+    ns_all, rs_all = batch_shape(args.batch_count, 4321)
+    mine, load = shard_batch(ns_all, rs_all, world, rank)
+    flops = float(sum(n ** 3 / 3.0 + 2.0 * n * n * r for n, r in zip(ns_all.astype(float), rs_all.astype(float))))
+    ns, rs, a_off, b_off, nd, rd, ao, bo, dA, dB = make_batch(ns_all[mine], rs_all[mine], 4321 + 17 * rank, dev)
+    count = len(ns)
     dX = torch.zeros_like(dB)
     info = torch.zeros(count, dtype=torch.int32, device=dev)
     iters = torch.zeros(count, dtype=torch.int32, device=dev)
@@ -397,6 +436,9 @@ def batched_arm(args, world, local, peaks):
         worst = max(worst, be / (n * eps))
     assert worst <= 10.0, f"batched backward error {worst} n eps"
     it = iters.cpu().numpy()
+    # the whole batch's refinement counts and worst error: one all-gather of
+    # per-rank summaries (the only collective of the batched arm)
+    g = allgather_vec(world, [float(count), float(it.sum()), float(it.min()), float(it.max()), worst])
     del gr
     # per-system plain FP64 launches on a copy (dposv factors A in place)
     Aw = dA.clone()
@@ -424,17 +466,21 @@ def batched_arm(args, world, local, peaks):
     t_loop = allmax(world, e0.elapsed_time(e1))
     del Aw, Bw, dA, dB, dX
     torch.cuda.empty_cache()
-    tf = world * flops / (t_batch * 1e-3) / 1e12
-    return {"systems": count, "n_range": [16, 512], "nrhs_range": [1, 8], "factor": "fp32 + fp64 refinement",
+    tf = flops / (t_batch * 1e-3) / 1e12
+    total = int(g[:, 0].sum())
+    return {"systems": total, "n_range": [16, 512], "nrhs_range": [1, 8], "factor": "fp32 + fp64 refinement",
+            "split": f"one batch over {world} GPU(s), longest processing time first (lnb_batched_partition)",
+            "scaling": "strong", "est_load_max_over_mean": round(float(load.max() / load.mean()), 4),
             "ms_per_batch": round(t_batch, 3), "value": round(tf, 4), "unit": UNIT,
-            "solves_per_s": round(world * count / (t_batch * 1e-3), 1),
+            "solves_per_s": round(total / (t_batch * 1e-3), 1),
             "frac_of_fp64_dgemm_peak": round(tf / peaks["fp64"], 4),
             "frac_of_tf32_peak": round(tf / peaks["tf32"], 4),
             "per_system_loop_ms": round(t_loop, 3), "speedup_vs_per_system_launches": round(t_loop / t_batch, 2),
             "per_system_loop": "lnb_dposv_dev (plain FP64, b=128) once per system, same stream",
             "launch": "one persistent launch in a CUDA graph, replayed", "cta_threads": pw,
-            "max_backward_error_over_n_eps_sample64": round(worst, 4),
-            "refinement_iterations": {"min": int(it.min()), "max": int(it.max()), "mean": round(float(it.mean()), 2)}}
+            "max_backward_error_over_n_eps_sample64": round(float(g[:, 4].max()), 4),
+            "refinement_iterations": {"min": int(g[:, 2].min()), "max": int(g[:, 3].max()),
+                                      "mean": round(float(g[:, 1].sum() / total), 2)}}
 
 
 def ours_arm(args, world, rank, local):
@@ -627,7 +673,7 @@ def ours_arm(args, world, rank, local):
                        "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_sec * 1e3, 3), "api": api}
     line["clocks"] = clk.summary()
     if not args.no_batched:
-        line["batched"] = batched_arm(args, world, local, peaks)
+        line["batched"] = batched_arm(args, world, rank, local, peaks)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ns = min(n, 8192)

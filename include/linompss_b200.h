@@ -245,6 +245,15 @@ LNB_EXPORT int lnb_batched_autotune(int count, const int *n_dev, const int *nrhs
                                     const int64_t *a_off_dev, const int64_t *b_off_dev,
                                     const double *dA, const double *dB, double *dX,
                                     int mode, int max_iter, void *stream);
+/* Multi-GPU split of one batch (host only, no device work): the systems in
+ * decreasing order of estimated cost n^3/3 + 2 n^2 nrhs (equal costs: lower
+ * index first), each given to the part with the least cost so far (ties: lower
+ * part) -- longest-processing-time first.  owner[s] receives the part (0 ..
+ * parts-1) of system s; load[p] (may be NULL) the estimated flops of part p.
+ * The result depends only on the arguments, so every rank computes the same
+ * split.  Returns 0 or LNB_EINVAL.  (The reference has no batched solver.) */
+LNB_EXPORT int lnb_batched_partition(int count, const int *n, const int *nrhs, int parts, int *owner,
+                                     double *load);
 
 /* ======================================================================== */
 /* 5. Runtime                                                                 */

@@ -328,6 +328,20 @@ def batched_posv_dev(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode=FAC
     return _chk(lib().lnb_batched_posv_dev(*args, _p(info), _p(iters), _stream(stream)))
 
 
+def batched_partition(ns, rs, parts: int):
+    """Split one batch over `parts` GPUs, longest-processing-time first on the
+    estimated cost n^3/3 + 2 n^2 nrhs (lnb_batched_partition).  Returns
+    (owner, load): the part of each system and the estimated flops per part."""
+    ns = np.ascontiguousarray(ns, dtype=np.int32)
+    rs = np.ascontiguousarray(rs, dtype=np.int32)
+    if ns.shape != rs.shape:
+        raise ValueError("n and nrhs must have the same length")
+    owner = np.empty(ns.size, dtype=np.int32)
+    load = np.empty(max(parts, 1), dtype=np.float64)
+    _chk(lib().lnb_batched_partition(C.c_int(ns.size), _p(ns), _p(rs), C.c_int(parts), _p(owner), _p(load)))
+    return owner, load
+
+
 def batched_autotune(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode=FACTOR_FP32, max_iter=10,
                      stream=None) -> int:
     """Times the solver's CTA sizes on this batch, keeps the fastest for later

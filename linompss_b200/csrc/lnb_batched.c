@@ -12,6 +12,7 @@
  * lnb_batched_autotune, which times the candidates on the caller's own batch
  * and keeps the faster one for the rest of the process.
  */
+#include <stdlib.h>
 #include <string.h>
 
 #include "lnb_host.h"
@@ -94,4 +95,44 @@ int lnb_batched_autotune(int count, const int *n_dev, const int *nrhs_dev, const
     }
     g_pw[mode == LNB_FACTOR_FP64] = pick;
     return pick;
+}
+
+/* ---- multi-GPU split of a batch -------------------------------------------- */
+typedef struct { double cost; int idx; } part_item;
+
+static int part_cmp(const void *a, const void *b)
+{
+    const part_item *x = (const part_item *)a, *y = (const part_item *)b;
+    if (x->cost != y->cost) return x->cost > y->cost ? -1 : 1;
+    return x->idx - y->idx;
+}
+
+int lnb_batched_partition(int count, const int *n, const int *nrhs, int parts, int *owner, double *load)
+{
+    if (count < 0 || parts <= 0 || (count > 0 && (!n || !nrhs || !owner)))
+        return lnb_set_error(LNB_EINVAL, "batched partition: count %d, parts %d", count, parts);
+    double *acc = (double *)calloc((size_t)parts, sizeof(double));
+    part_item *it = (part_item *)malloc((size_t)(count > 0 ? count : 1) * sizeof(part_item));
+    if (!acc || !it) {
+        free(acc);
+        free(it);
+        return lnb_set_error(LNB_ENOMEM, "batched partition: host memory");
+    }
+    for (int s = 0; s < count; ++s) {
+        const double ns = (double)n[s], rs = (double)nrhs[s];
+        it[s].cost = ns * ns * ns / 3.0 + 2.0 * ns * ns * rs;
+        it[s].idx = s;
+    }
+    qsort(it, (size_t)count, sizeof(part_item), part_cmp);
+    for (int k = 0; k < count; ++k) {
+        int best = 0;
+        for (int p = 1; p < parts; ++p)
+            if (acc[p] < acc[best]) best = p;
+        owner[it[k].idx] = best;
+        acc[best] += it[k].cost;
+    }
+    if (load) memcpy(load, acc, (size_t)parts * sizeof(double));
+    free(acc);
+    free(it);
+    return 0;
 }
