@@ -309,6 +309,29 @@ static int join_cols(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode,
     return 0;
 }
 
+/* LNB_UPD_DEPTH: panels a block column beyond the look-ahead collects before it
+ * takes them in one update of K = depth b (default 2; 1 updates every step) */
+static int upd_depth(void)
+{
+    const char *e = getenv("LNB_UPD_DEPTH");
+    const int v = (e && *e) ? atoi(e) : 2;
+    return v < 1 ? 1 : v;
+}
+
+/* 0, or the library error for a failed CUDA call */
+static int ck_cuda(int err, const char *where) { return err ? lnb_cuda_error(err, where) : 0; }
+
+/* block columns j0..j1 take panels p0..p1 (all of width b) in one update */
+static int apply_panels(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, const float *HA, const float *LA,
+                        int64_t ldk, int j0, int j1, int p0, int p1, cudaStream_t s)
+{
+    const int64_t c0 = (int64_t)j0 * b, c1 = ((int64_t)j1 + 1) * b < n ? ((int64_t)j1 + 1) * b : n;
+    const int64_t ko = (int64_t)p0 * b;
+    CK(upd_tc(mode, HA + c0 * ldk + ko, LA ? LA + c0 * ldk + ko : NULL, ldk, dA + c0 + c0 * lda, lda, n - c0, 0,
+              c1 - c0, (p1 - p0 + 1) * b, c->st, s), "panel update");
+    return 0;
+}
+
 int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_refactor_ctx *rf,
                             const lnb_stream_in *in, lnb_arena *ar, cudaStream_t s)
 {
@@ -319,69 +342,89 @@ int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, in
     float *LA = mode == LNB_FACTOR_TF32X3 ? (float *)lnb_arena_take(ar, (size_t)n * ldk * 4) : NULL;
     if (!dinv || !HA || (mode == LNB_FACTOR_TF32X3 && !LA))
         return lnb_set_error(LNB_ENOMEM, "streamed factor workspace");
+    const int mt = (n + b - 1) / b;
+    /* u[j]: panels applied to block column j so far (j <= joined) */
+    int *u = (int *)calloc((size_t)mt, sizeof(int));
+    if (!u) return lnb_set_error(LNB_ENOMEM, "streamed factor: host memory");
     cudaStream_t crit = c->crit;
     cudaEvent_t ev_start = c->ev[0], ev_trsm = c->ev[1], ev_next = c->ev[2], ev_done = c->ev[3];
-    CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
-    CK(cudaEventRecord(ev_start, s), "event");
-    CK(cudaStreamWaitEvent(crit, ev_start, 0), "event wait");
-
-    const int mt = (n + b - 1) / b;
+    int e = 0;
+#define RUN(x)                   \
+    do {                         \
+        if ((e = (x)) != 0) goto out; \
+    } while (0)
+    RUN(ck_cuda(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset"));
+    RUN(ck_cuda(cudaEventRecord(ev_start, s), "event"));
+    RUN(ck_cuda(cudaStreamWaitEvent(crit, ev_start, 0), "event wait"));
+    {
     const int ahead = stream_ahead() < 0 ? 0 : stream_ahead();
-    int joined = 0, e;   /* block columns 0..joined are converted and updated by every finished panel */
-    if ((e = join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, 0, 0, 0, crit))) return e;
+    const int depth = upd_depth();
+    /* block columns 0..joined are in the working matrix; without `in` all are */
+    int joined = in ? 0 : mt - 1;
+    if (in) RUN(join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, 0, 0, 0, crit));
     for (int k = 0; k < mt; ++k) {
         const int64_t k0 = (int64_t)k * b;
         const int bs = (int)(n - k0 < b ? n - k0 : b);
         float *Akk = dA + k0 + k0 * lda;
         const int64_t mrem = n - k0 - bs;
-        { int _e = lnb_potrf_tile_f32(Akk, lda, bs, k0, dinv, c->st, crit); if (_e) return _e; }
+        RUN(lnb_potrf_tile_f32(Akk, lda, bs, k0, dinv, c->st, crit));
         if (rf) {
-            int info = lnb_status_read(c, crit);
-            if (info < 0) return info;
-            if (info > 0 && (e = refactor_tile(c, rf, dA, lda, k0, bs, b, dinv, ar, crit))) return e;
+            const int info = lnb_status_read(c, crit);
+            if (info < 0) { e = info; goto out; }
+            if (info > 0) RUN(refactor_tile(c, rf, dA, lda, k0, bs, b, dinv, ar, crit));
         }
         if (mrem <= 0) break;
         float *hk = HA + (k0 + bs) * ldk + k0, *lk = LA ? LA + (k0 + bs) * ldk + k0 : NULL;
-        CK(lnb_k_trsm_rlt_prep_f32(Akk, lda, dinv, Akk + bs, lda, mrem, bs, hk, lk, (int)ldk, crit), "trsm+prep f32");
-        CK(cudaEventRecord(ev_trsm, crit), "event");
+        RUN(ck_cuda(lnb_k_trsm_rlt_prep_f32(Akk, lda, dinv, Akk + bs, lda, mrem, bs, hk, lk, (int)ldk, crit),
+                           "trsm+prep f32"));
+        RUN(ck_cuda(cudaEventRecord(ev_trsm, crit), "event"));
         /* block columns whose data is here, as far as the host can tell now */
         const int need = k + 2 < mt ? k + 2 : mt - 1;
-        const int cap = need + ahead < mt - 1 ? need + ahead : mt - 1;
         int avail = joined;
-        while (avail + 1 <= cap && cudaEventQuery(in->arr[avail + 1]) == cudaSuccess) ++avail;
-        cudaGetLastError();   /* cudaErrorNotReady from the queries */
-        float *Ct = Akk + bs + (int64_t)bs * lda;
-        const int64_t nb1 = b < mrem ? b : mrem;
-        const int64_t nb2 = 2 * (int64_t)b < mrem ? 2 * (int64_t)b : mrem;
-        /* block column k+1 (the next panel) on the critical stream */
-        if (k + 1 > joined) {
-            if ((e = join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, k + 1, k + 1, k + 1, crit))) return e;
-        } else {
-            CK(upd_tc(mode, hk, lk, ldk, Ct, lda, mrem, 0, nb1, bs, c->st, crit), "update next panel");
+        if (in) {
+            const int cap = need + ahead < mt - 1 ? need + ahead : mt - 1;
+            while (avail + 1 <= cap && cudaEventQuery(in->arr[avail + 1]) == cudaSuccess) ++avail;
+            cudaGetLastError();   /* cudaErrorNotReady from the queries */
         }
-        CK(cudaStreamWaitEvent(s, ev_trsm, 0), "event wait");
+        /* block column k+1 (the next panel), complete through panel k, on the critical stream */
+        if (k + 1 > joined) RUN(join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, k + 1, k + 1, k + 1, crit));
+        else RUN(apply_panels(c, n, b, dA, lda, mode, HA, LA, ldk, k + 1, k + 1, u[k + 1], k, crit));
+        u[k + 1] = k + 1;
+        RUN(ck_cuda(cudaStreamWaitEvent(s, ev_trsm, 0), "event wait"));
         if (k + 2 < mt) {
-            if (k + 2 > joined) {
-                if ((e = join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, k + 2, k + 2, k + 1, s))) return e;
-            } else {
-                CK(upd_tc(mode, hk, lk, ldk, Ct, lda, mrem, nb1, nb2, bs, c->st, s), "update panel k+2");
+            if (k + 2 > joined) RUN(join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, k + 2, k + 2, k + 1, s));
+            else RUN(apply_panels(c, n, b, dA, lda, mode, HA, LA, ldk, k + 2, k + 2, u[k + 2], k, s));
+            u[k + 2] = k + 1;
+        }
+        RUN(ck_cuda(cudaEventRecord(ev_next, s), "event"));
+        /* the other joined columns take their pending panels once `depth` have
+         * collected, one launch per run of columns with the same backlog */
+        for (int j = k + 3; j <= joined;) {
+            int j1 = j;
+            while (j1 + 1 <= joined && u[j1 + 1] == u[j]) ++j1;
+            if (k + 1 - u[j] >= depth) {
+                RUN(apply_panels(c, n, b, dA, lda, mode, HA, LA, ldk, j, j1, u[j], k, s));
+                for (int q = j; q <= j1; ++q) u[q] = k + 1;
             }
+            j = j1 + 1;
         }
-        CK(cudaEventRecord(ev_next, s), "event");
-        /* the other joined columns take panel k; newly arrived ones catch up */
-        if (joined > k + 2) {
-            const int64_t r1 = ((int64_t)joined + 1) * b < n ? ((int64_t)joined + 1) * b - (k0 + bs) : mrem;
-            CK(upd_tc(mode, hk, lk, ldk, Ct, lda, mrem, nb2, r1, bs, c->st, s), "update rest");
-        }
+        /* newly arrived columns catch up with panels 0..k */
         const int jn = (joined > need ? joined : need) + 1;
-        if (avail >= jn && (e = join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, jn, avail, k + 1, s))) return e;
+        if (avail >= jn) {
+            RUN(join_cols(c, n, b, dA, lda, mode, in, HA, LA, ldk, jn, avail, k + 1, s));
+            for (int q = jn; q <= avail; ++q) u[q] = k + 1;
+        }
         if (need > joined) joined = need;
         if (avail > joined) joined = avail;
-        CK(cudaStreamWaitEvent(crit, ev_next, 0), "event wait");
+        RUN(ck_cuda(cudaStreamWaitEvent(crit, ev_next, 0), "event wait"));
     }
-    CK(cudaEventRecord(ev_done, crit), "event");
-    CK(cudaStreamWaitEvent(s, ev_done, 0), "event wait");
-    return 0;
+    }
+    RUN(ck_cuda(cudaEventRecord(ev_done, crit), "event"));
+    RUN(ck_cuda(cudaStreamWaitEvent(s, ev_done, 0), "event wait"));
+out:
+#undef RUN
+    free(u);
+    return e;
 }
 
 /* ---- entry points ---------------------------------------------------------- */

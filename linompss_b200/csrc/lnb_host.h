@@ -96,7 +96,9 @@ typedef struct {
 } lnb_stream_in;
 int lnb_chol_f32_stream_ok(int n, int b, int mode);
 size_t lnb_chol_f32_stream_ws_bytes(int n, int b, int mode);
-/* the FP32 factorization of lower(S A S) into dA while A arrives (see in) */
+/* The FP32 factorization of lower(S A S) into dA, keeping every panel's
+ * operand copies: while A arrives (in != NULL, dA filled block column by block
+ * column), or with dA already complete (in == NULL). */
 int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_refactor_ctx *rf,
                             const lnb_stream_in *in, lnb_arena *ar, cudaStream_t s);
 

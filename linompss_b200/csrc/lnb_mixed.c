@@ -133,7 +133,9 @@ int lnb_dsposv_ir_dev(int n, int nrhs, int b, const double *dA, int lda, const d
     }
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
-    void *ws = lnb_ws(c, ir_ws_bytes(n, nrhs, b, mode, 0));
+    /* TF32 update paths with whole 32-blocks run the all-panels schedule (see
+     * lnb_chol_f32_stream_run), which needs the larger workspace */
+    void *ws = lnb_ws(c, ir_ws_bytes(n, nrhs, b, mode, lnb_chol_f32_stream_ok(n, b, mode)));
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     return ir_run(c, n, nrhs, b, dA, lda, dB, ldb, dX, ldx, opts_in, res, (cudaStream_t)stream, &ar, NULL);
@@ -185,7 +187,12 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
         e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, &sin, &ar, s);
     } else {
         CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, s), "convert");
-        e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &rf, &ar, s);
+        /* every panel's operands kept: columns beyond the look-ahead take their
+         * panels two at a time, halving the passes over the trailing matrix */
+        if (lnb_chol_f32_stream_ok(n, b, mode))
+            e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, NULL, &ar, s);
+        else
+            e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &rf, &ar, s);
     }
     rr.refactored_tiles = rf.refactored;
     if (e) {

@@ -172,3 +172,24 @@ def test_ir_fp64_refactor_of_failed_tile(lnb, cuda, api):
     assert rc == 0, (rc, res, lnb.last_error())
     assert res["refactored_tiles"] >= 1
     assert O.backward_error_np(A0, X, B0) <= 10 * n * EPS
+
+
+@pytest.mark.parametrize("depth", ["1", "2", "3"])
+def test_ir_device_path_panel_grouping(lnb, cuda, monkeypatch, depth):
+    """The device entry point keeps every panel's operand copies, so columns
+    beyond the look-ahead can take their panels `depth` at a time (one update
+    with K = depth * b, LNB_UPD_DEPTH).  Every grouping refines to the FP64 bar
+    in the same number of iterations, give or take one."""
+    import torch
+    monkeypatch.setenv("LNB_UPD_DEPTH", depth)
+    n, b, nrhs = 5120, 512, 2
+    A0 = O.spd_covariance(n, 1e-3, seed=31)
+    B0 = np.random.default_rng(31).standard_normal((n, nrhs))
+    At = torch.tensor(np.ascontiguousarray(A0.T), device=cuda)
+    Bt = torch.tensor(np.ascontiguousarray(B0.T), device=cuda)
+    Xt = torch.zeros_like(Bt)
+    rc, res = lnb.dsposv_ir_dev(At, Bt, Xt, n, nrhs, b, lnb.ir_opts(factor=lnb.FACTOR_TF32X3))
+    torch.cuda.synchronize()
+    assert rc == 0, (res, lnb.last_error())
+    assert O.backward_error_np(A0, Xt.cpu().numpy().T, B0) <= 10 * n * EPS
+    assert res["iterations"] <= 4 and not res["used_pcg"]
