@@ -397,12 +397,17 @@ int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, in
             u[k + 2] = k + 1;
         }
         RUN(ck_cuda(cudaEventRecord(ev_next, s), "event"));
-        /* the other joined columns take their pending panels once `depth` have
-         * collected, one launch per run of columns with the same backlog */
+        /* The other joined columns take their pending panels once `depth` have
+         * collected, one launch per run of columns with the same backlog and
+         * group.  Blocks of 8 columns belong to groups 0 .. depth-1 in turn;
+         * group g takes its first g panels one at a time, so the groups' long
+         * updates fall on different steps and the per-step update work stays
+         * close to that of one panel for all columns. */
         for (int j = k + 3; j <= joined;) {
+            const int g = (j / 8) % depth;
             int j1 = j;
-            while (j1 + 1 <= joined && u[j1 + 1] == u[j]) ++j1;
-            if (k + 1 - u[j] >= depth) {
+            while (j1 + 1 <= joined && u[j1 + 1] == u[j] && ((j1 + 1) / 8) % depth == g) ++j1;
+            if (k + 1 - u[j] >= (k < g ? 1 : depth)) {
                 RUN(apply_panels(c, n, b, dA, lda, mode, HA, LA, ldk, j, j1, u[j], k, s));
                 for (int q = j; q <= j1; ++q) u[q] = k + 1;
             }
