@@ -38,8 +38,13 @@ int lnb_get_factor_mode(void) { return g_schol_mode; }
 
 static inline int64_t kpad_of(int b) { return ((int64_t)b + 63) & ~(int64_t)63; }
 
+size_t lnb_chol_f32_stream_ws_bytes(int n, int b, int mode);
+int lnb_chol_f32_stream_ok(int n, int b, int mode);
+
 size_t lnb_chol_f32_ws_bytes(int n, int b, int mode)
 {
+    /* TF32 paths with whole 32-blocks keep every panel's operands */
+    if (lnb_chol_f32_stream_ok(n, b, mode)) return lnb_chol_f32_stream_ws_bytes(n, b, mode);
     size_t bytes = lnb_align256((size_t)((b + 31) / 32) * 1024 * sizeof(float)) + 256;
     const int64_t kp = kpad_of(b);
     if (mode == LNB_FACTOR_TF32X3) bytes += 4 * lnb_align256((size_t)n * kp * 4);
@@ -174,6 +179,9 @@ static int upd32(const panelbuf *pb, int slot, const float *P, int64_t ldp, floa
 int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_refactor_ctx *rf,
                      lnb_arena *ar, cudaStream_t s)
 {
+    /* TF32 update paths with whole 32-blocks: every panel's operands kept, far
+     * columns updated several panels at a time */
+    if (lnb_chol_f32_stream_ok(n, b, mode)) return lnb_chol_f32_stream_run(c, n, b, dA, lda, mode, rf, NULL, ar, s);
     float *dinv = (float *)lnb_arena_take(ar, (size_t)((b + 31) / 32) * 1024 * sizeof(float));
     if (!dinv) return lnb_set_error(LNB_ENOMEM, "chol32 workspace");
     panelbuf pb;

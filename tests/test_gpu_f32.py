@@ -66,19 +66,23 @@ def test_schol_modes_sizes(lnb, mode, n, b):
 
 
 def test_tf32x3_matches_fp32_simt(lnb):
-    """The split product recovers FP32-level accuracy: TF32x3 and the SIMT
-    FP32 update agree to FP32 rounding, far closer than a single TF32 product."""
+    """The split product recovers FP32-level accuracy: measured against the
+    FP64 factor of the same (FP32-valued) matrix, the TF32x3 factor's error is
+    at the level of the SIMT FP32 factor's, and a single TF32 product's is
+    several times larger.  (The factors differ in accumulation order, so the
+    comparison is made against the FP64 factor, not between the modes.)"""
     n, b = 1536, 256
     A0 = O.spd_covariance(n, 0.1, seed=7).astype(np.float32)
-    out = {}
+    L64 = np.linalg.cholesky(A0.astype(np.float64))
+    scale = np.abs(L64).max()
+    err = {}
     for mode in ("fp32", "tf32x3", "tf32"):
         lnb.set_factor_mode(MODES[mode])
         A = np.asfortranarray(A0.copy())
         assert lnb.ompss_schol_rl(n, b, b, A, n) == 0
-        out[mode] = np.tril(A).astype(np.float64)
-    d3 = np.abs(out["tf32x3"] - out["fp32"]).max()
-    d1 = np.abs(out["tf32"] - out["fp32"]).max()
-    assert d3 < 1e-4 and d3 * 20 < d1, (d3, d1)
+        err[mode] = np.abs(np.tril(A).astype(np.float64) - L64).max() / scale
+    assert err["tf32x3"] <= max(4 * err["fp32"], 2e-5), err
+    assert err["tf32"] >= 4 * err["tf32x3"], err
 
 
 def test_schol_hypermatrix(lnb):
