@@ -100,6 +100,20 @@ LNB_EXPORT int ompss_dtrsm(ompssblas_t side, ompssblas_t uplo, ompssblas_t trans
                            ompssblas_t diag, int m, int n, int b, double alpha,
                            double *A, int lda, double *B, int ldb);
 
+/* Blocked symmetric rank-k update on the triangle `uplo` of C:
+ * C = alpha op(A) op(A)^T + beta C, op(A) = A (n x k) for trans 'N', A^T
+ * (A k x n) for 'T'; the other triangle is not touched.  Replaces
+ * syrk/ompss_syrk.h:20,22 (-> SYRK_MAIN syrk_main.c, tile GEMM/SYRK tasks of
+ * width b).  b is the reference's tile size; the GPU computes the triangle in
+ * one launch, so b only has to be positive.  The reference's first k-chunk is
+ * always b wide (syrk_main.c), so for k < b it reads past column k; this
+ * library follows BLAS for every k.  ompss_ssyrk computes in FP64 and rounds
+ * the result once.  Returns 0 or LNB_E* (the reference returns void). */
+LNB_EXPORT int ompss_dsyrk(ompssblas_t uplo, ompssblas_t trans, int b, int n, int k, double alpha,
+                           double *A, int lda, double beta, double *C, int ldc);
+LNB_EXPORT int ompss_ssyrk(ompssblas_t uplo, ompssblas_t trans, int b, int n, int k, float alpha,
+                           float *A, int lda, float beta, float *C, int ldc);
+
 /* Tile-task ABI: one BLAS/LAPACK operation on one tile, run on the GPU.
  * Replace tasks_potrf.h:24-28, tasks_trsm.h:23-27, tasks_syrk.h:20-24,
  * task_gemm.h:27-31 (exported from libbblas with the trailing OmpSs priority

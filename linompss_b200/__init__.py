@@ -180,6 +180,25 @@ def ompss_dtrsm(side, uplo, trans, diag, m, n, b, alpha, A, lda, B, ldb) -> int:
     return _chk(f(opt(side), opt(uplo), opt(trans), opt(diag), m, n, b, alpha, _p(A), lda, _p(B), ldb))
 
 
+def ompss_dsyrk(uplo, trans, b, n, k, alpha, A, lda, Cm, ldc, beta=1.0) -> int:
+    """Cm = alpha op(A) op(A)^T + beta Cm on the triangle `uplo` of Cm (in place)."""
+    _colmajor(A)
+    _colmajor(Cm)
+    f = lib().ompss_dsyrk
+    f.argtypes = [ompssblas_t, ompssblas_t, C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int,
+                  C.c_double, C.c_void_p, C.c_int]
+    return _chk(f(opt(uplo), opt(trans), b, n, k, alpha, _p(A), lda, beta, _p(Cm), ldc))
+
+
+def ompss_ssyrk(uplo, trans, b, n, k, alpha, A, lda, Cm, ldc, beta=1.0) -> int:
+    _colmajor(A, np.float32)
+    _colmajor(Cm, np.float32)
+    f = lib().ompss_ssyrk
+    f.argtypes = [ompssblas_t, ompssblas_t, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_int,
+                  C.c_float, C.c_void_p, C.c_int]
+    return _chk(f(opt(uplo), opt(trans), b, n, k, alpha, _p(A), lda, beta, _p(Cm), ldc))
+
+
 def task_dpotrf(uplo: str, n: int, A: np.ndarray, lda: int, p: int = 0) -> int:
     f = lib().task_dpotrf
     f.argtypes = [ompssblas_t, C.c_int, C.c_void_p, C.c_int, C.c_int]

@@ -113,6 +113,78 @@ int task_dgemm(ompssblas_t transa, ompssblas_t transb, int bm, int bn, int bk, d
     return 0;
 }
 
+int lnb_k_f32_to_f64(const float *X, int64_t ldx, int64_t m, int64_t k, double *D, int64_t ldd, cudaStream_t st);
+int lnb_k_f64_to_f32(const double *D, int64_t ldd, int64_t m, int64_t k, float *X, int64_t ldx, cudaStream_t st);
+
+/* C = alpha op(A) op(A)^T + beta C on triangle u of the host matrix C (FP64
+ * or, with single != 0, FP32 host arrays computed in FP64 on the device) */
+static int syrk_host(char u, char t, int n, int k, double alpha, const void *A, int lda, double beta, void *C,
+                     int ldc, int single)
+{
+    if (n < 0 || k < 0) return lnb_set_error(LNB_EINVAL, "syrk sizes n = %d, k = %d", n, k);
+    if (n == 0) return 0;
+    const int64_t am = t == 'N' ? n : k, an = t == 'N' ? k : n;
+    if (lda < (am > 1 ? am : 1) || ldc < (n > 1 ? n : 1)) return lnb_set_error(LNB_EINVAL, "syrk ld");
+    if (!A || !C) return lnb_set_error(LNB_EINVAL, "syrk: NULL argument");
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const size_t sa = lnb_align256((size_t)am * (an ? an : 1) * 8), sc = lnb_align256((size_t)n * n * 8);
+    const size_t sa4 = single ? lnb_align256((size_t)am * (an ? an : 1) * 4) : 0;
+    const size_t sc4 = single ? lnb_align256((size_t)n * n * 4) : 0;
+    void *ws = lnb_ws(c, sa + sc + sa4 + sc4 + 1024);
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    double *dA = lnb_arena_take(&ar, sa), *dC = lnb_arena_take(&ar, sc);
+    float *fA = single ? (float *)lnb_arena_take(&ar, sa4) : NULL;
+    float *fC = single ? (float *)lnb_arena_take(&ar, sc4) : NULL;
+    cudaStream_t s = c->main;
+    int e;
+    if (!single) {
+        if ((e = put(dA, am, (const double *)A, lda, am, an, s)) || (e = put(dC, n, (const double *)C, ldc, n, n, s)))
+            return e;
+    } else {
+        if (am > 0 && an > 0) {
+            CK(cudaMemcpy2DAsync(fA, (size_t)am * 4, A, (size_t)lda * 4, (size_t)am * 4, an, cudaMemcpyHostToDevice, s),
+               "syrk A in");
+            CK(lnb_k_f32_to_f64(fA, am, am, an, dA, am, s), "widen A");
+        }
+        CK(cudaMemcpy2DAsync(fC, (size_t)n * 4, C, (size_t)ldc * 4, (size_t)n * 4, n, cudaMemcpyHostToDevice, s),
+           "syrk C in");
+        CK(lnb_k_f32_to_f64(fC, n, n, n, dC, n, s), "widen C");
+    }
+    CK(lnb_k_gemm_tri_f64(t == 'N' ? 'N' : 'T', t == 'N' ? 'T' : 'N', n, n, k, alpha, dA, am, dA, am, beta, dC, n, u,
+                          s), "syrk");
+    if (!single) {
+        if ((e = get((double *)C, ldc, dC, n, n, n, s))) return e;
+    } else {
+        CK(lnb_k_f64_to_f32(dC, n, n, n, fC, n, s), "narrow C");
+        CK(cudaMemcpy2DAsync(C, (size_t)ldc * 4, fC, (size_t)n * 4, (size_t)n * 4, n, cudaMemcpyDeviceToHost, s),
+           "syrk C out");
+    }
+    CK(cudaStreamSynchronize(s), "syrk sync");
+    return 0;
+}
+
+int ompss_dsyrk(ompssblas_t uplo, ompssblas_t trans, int b, int n, int k, double alpha, double *A, int lda,
+                double beta, double *C, int ldc)
+{
+    char u = 0, t = 0;
+    int e;
+    if ((e = opt(uplo.s, "LU", &u, "uplo")) || (e = opt(trans.s, "NT", &t, "trans"))) return e;
+    if (b <= 0) return lnb_set_error(LNB_EINVAL, "syrk tile size b = %d", b);
+    return syrk_host(u, t, n, k, alpha, A, lda, beta, C, ldc, 0);
+}
+
+int ompss_ssyrk(ompssblas_t uplo, ompssblas_t trans, int b, int n, int k, float alpha, float *A, int lda,
+                float beta, float *C, int ldc)
+{
+    char u = 0, t = 0;
+    int e;
+    if ((e = opt(uplo.s, "LU", &u, "uplo")) || (e = opt(trans.s, "NT", &t, "trans"))) return e;
+    if (b <= 0) return lnb_set_error(LNB_EINVAL, "syrk tile size b = %d", b);
+    return syrk_host(u, t, n, k, alpha, A, lda, beta, C, ldc, 1);
+}
+
 int task_dsyrk(ompssblas_t uplo, ompssblas_t trans, int n, int k, double alpha, double *A, int lda,
                double beta, double *C, int ldc, int p)
 {
@@ -120,25 +192,7 @@ int task_dsyrk(ompssblas_t uplo, ompssblas_t trans, int n, int k, double alpha, 
     char u = 0, t = 0;
     int e;
     if ((e = opt(uplo.s, "LU", &u, "uplo")) || (e = opt(trans.s, "NT", &t, "trans"))) return e;
-    if (n < 0 || k < 0) return lnb_set_error(LNB_EINVAL, "syrk sizes");
-    if (n == 0) return 0;
-    const int64_t am = t == 'N' ? n : k, an = t == 'N' ? k : n;
-    if (lda < (am > 1 ? am : 1) || ldc < (n > 1 ? n : 1)) return lnb_set_error(LNB_EINVAL, "syrk ld");
-    lnb_ctx *c = lnb_ctx_get();
-    if (!c) return LNB_ENODEV;
-    const size_t sa = lnb_align256((size_t)am * (an ? an : 1) * 8), sc = lnb_align256((size_t)n * n * 8);
-    void *ws = lnb_ws(c, sa + sc + 512);
-    if (!ws) return LNB_ENOMEM;
-    lnb_arena ar = {(char *)ws, 0, c->ws_size};
-    double *dA = lnb_arena_take(&ar, sa), *dC = lnb_arena_take(&ar, sc);
-    cudaStream_t s = c->main;
-    if ((e = put(dA, am, A, lda, am, an, s)) || (e = put(dC, n, C, ldc, n, n, s))) return e;
-    /* C = alpha op(A) op(A)^T + beta C on triangle u */
-    CK(lnb_k_gemm_tri_f64(t == 'N' ? 'N' : 'T', t == 'N' ? 'T' : 'N', n, n, k, alpha, dA, am, dA, am, beta,
-                          dC, n, u, s), "syrk");
-    if ((e = get(C, ldc, dC, n, n, n, s))) return e;
-    CK(cudaStreamSynchronize(s), "syrk sync");
-    return 0;
+    return syrk_host(u, t, n, k, alpha, A, lda, beta, C, ldc, 0);
 }
 
 int task_dtrsm(ompssblas_t side, ompssblas_t uplo, ompssblas_t trans, ompssblas_t diag, int bm, int bn,

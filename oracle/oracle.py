@@ -121,6 +121,15 @@ def ltrsm(uplo: str, trans: str, diag: str, bm: int, alpha: float, A: np.ndarray
                      _ptr(B), _i64(B.shape[0]))
 
 
+def syrk(uplo: str, trans: str, n: int, k: int, alpha: float, A: np.ndarray, beta: float, Cm: np.ndarray) -> None:
+    """Cm = alpha op(A) op(A)^T + beta Cm on triangle `uplo` (orc_dsyrk, or orc_ssyrk for FP32), in place"""
+    single = Cm.dtype == np.float32
+    f = lib().orc_ssyrk if single else lib().orc_dsyrk
+    T = C.c_float if single else C.c_double
+    f(C.c_char(uplo.encode()), C.c_char(trans.encode()), _i64(n), _i64(k), T(alpha), _ptr(A), _i64(A.shape[0]),
+      T(beta), _ptr(Cm), _i64(Cm.shape[0]))
+
+
 def spdsolv(A: np.ndarray, B: np.ndarray, b: int) -> int:
     m, nrhs = B.shape
     return lib().orc_dspdsolv(_i64(m), _i64(nrhs), _i64(b), _ptr(A), _ptr(B))
@@ -214,6 +223,14 @@ def ref_dtrsm(side, uplo, trans, diag, m, n, b, alpha, A, lda, B, ldb) -> None:
                                      C.c_void_p, C.c_int]
     f(ref_opt(side), ref_opt(uplo), ref_opt(trans), ref_opt(diag), m, n, b, alpha,
       _ptr(A), lda, _ptr(B), ldb)
+
+
+def ref_dsyrk(uplo, trans, b, n, k, alpha, A, lda, beta, Cm, ldc) -> None:
+    """the reference's own blocked ompss_dsyrk (syrk_main.c), Cm updated in place"""
+    f = ref().ompss_dsyrk
+    f.argtypes = [_OmpssBlas] * 2 + [C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_double,
+                                     C.c_void_p, C.c_int]
+    f(ref_opt(uplo), ref_opt(trans), b, n, k, alpha, _ptr(A), lda, beta, _ptr(Cm), ldc)
 
 
 def ref_cg(A: np.ndarray, rhs: np.ndarray, bm: int, tol: float, steps: int):

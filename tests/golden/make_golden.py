@@ -14,6 +14,8 @@ scaled down to a few hundred KB in total:
   chol_*      tests/dense_tests/potrf_test.c (SPD = U[0,1) symmetric + n I;
               a ragged n % b != 0 case like N=1989, b=533)
   spdsolv_*   spdsolv.c / spdsolv_setup.c (B = A X with X ~ U[0,1))
+  dsyrk_*     the reference's ompss_dsyrk (syrk_main.c): 4 uplo/trans cases and beta 0,
+              ragged n and k against b, lda and ldc padded
   dtrsm_*     tests/dense_tests/trsm_test.c (4 left cases, lda != m, ldb != m,
               alpha = -2.11, entries U[0,1) + 100 -- scaled to M=60, N=50, b=13)
   dcg_*       itref.c dcg_pure on a G G^T/n + I matrix
@@ -95,6 +97,26 @@ def dtrsm_cases():
                  bb=np.int64(BB), alpha=np.float64(alpha))
 
 
+def dsyrk_cases():
+    # blocked ompss_dsyrk (syrk_main.c): ragged n and k against the tile size,
+    # lda and ldc larger than the matrices, all four uplo/trans cases, and beta 0
+    n, k, b, alpha = 70, 40, 16, -1.3
+    rng = np.random.default_rng(21)
+    for uplo in "LU":
+        for trans in "NT":
+            for beta in (0.7, 0.0):
+                if beta == 0.0 and (uplo, trans) != ("L", "N"):
+                    continue
+                lda = (n if trans == "N" else k) + 5
+                A = np.asfortranarray(rng.standard_normal((lda, k if trans == "N" else n)))
+                C0 = np.asfortranarray(rng.standard_normal((n + 3, n)))
+                D = C0.copy(order="F")
+                O.ref_dsyrk(uplo, trans, b, n, k, alpha, A, lda, beta, D, n + 3)
+                tag = "b0" if beta == 0.0 else "b"
+                save(f"dsyrk_{uplo}{trans}_{tag}", A=A, C=C0, out=D, n=np.int64(n), k=np.int64(k),
+                     bb=np.int64(b), alpha=np.float64(alpha), beta=np.float64(beta))
+
+
 def dcg_cases():
     for n, bm, steps, tol, seed in ((64, 16, 8, 1e-10, 14), (64, 16, 200, 1e-10, 14),
                                     (100, 32, 300, 1e-12, 15)):
@@ -147,5 +169,6 @@ if __name__ == "__main__":
     schol_case()
     spdsolv_cases()
     dtrsm_cases()
+    dsyrk_cases()
     dcg_cases()
     itref_cases()

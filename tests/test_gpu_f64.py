@@ -260,3 +260,48 @@ def test_itref_golden(lnb, golden_dir, name):
     assert norms[k - 1] <= float(d["prec"])
     np.testing.assert_allclose(x, xo, rtol=0, atol=1e-12)
     assert O.backward_error(d["A"], x, d["rhs"]) <= 10 * n * EPS
+
+
+@pytest.mark.parametrize("case", ["LN_b", "LN_b0", "LT_b", "UN_b", "UT_b"])
+def test_ompss_dsyrk_golden(lnb, golden_dir, case):
+    """ompss_dsyrk against the reference's blocked SYRK (syrk_main.c): ragged
+    n and k against the tile size, padded lda/ldc, beta 0; the other triangle
+    and the rows past n stay as they were."""
+    d = load(golden_dir, "dsyrk_" + case)
+    n, k, bb = int(d["n"]), int(d["k"]), int(d["bb"])
+    alpha, beta = float(d["alpha"]), float(d["beta"])
+    A = d["A"].copy(order="F")
+    Cm = d["C"].copy(order="F")
+    assert lnb.ompss_dsyrk(case[0], case[1], bb, n, k, alpha, A, A.shape[0], Cm, Cm.shape[0], beta=beta) == 0
+    ref = d["out"]
+    np.testing.assert_allclose(Cm, ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+    if beta != 0.0:
+        np.testing.assert_array_equal(Cm[n:], d["C"][n:])
+
+
+@pytest.mark.parametrize("uplo,trans", [("L", "N"), ("U", "T")])
+def test_ompss_ssyrk_vs_fp64(lnb, uplo, trans):
+    """The FP32 twin computes in FP64 and rounds once: within FP32 rounding of
+    the exact result of its FP32 inputs; the other triangle untouched."""
+    rng = np.random.default_rng(5)
+    n, k = 300, 130
+    A = np.asfortranarray(rng.standard_normal((n, k) if trans == "N" else (k, n)).astype(np.float32))
+    C0 = np.asfortranarray(rng.standard_normal((n, n)).astype(np.float32))
+    Cm = C0.copy(order="F")
+    assert lnb.ompss_ssyrk(uplo, trans, 64, n, k, 0.5, A, A.shape[0], Cm, n, beta=-1.0) == 0
+    op = A.astype(np.float64) if trans == "N" else A.astype(np.float64).T
+    ref = -1.0 * C0.astype(np.float64) + 0.5 * op @ op.T
+    tri = np.tril if uplo == "L" else np.triu
+    np.testing.assert_allclose(tri(Cm.astype(np.float64)), tri(ref), rtol=0,
+                               atol=2 * np.finfo(np.float32).eps * np.abs(ref).max())
+    other = (lambda x: np.triu(x, 1)) if uplo == "L" else (lambda x: np.tril(x, -1))
+    np.testing.assert_array_equal(other(Cm), other(C0))
+
+
+def test_ompss_dsyrk_rejects_bad_arguments(lnb):
+    A = np.zeros((4, 4), order="F")
+    Cm = np.zeros((4, 4), order="F")
+    with pytest.raises(lnb.LinompssError):
+        lnb.ompss_dsyrk("X", "N", 2, 4, 4, 1.0, A, 4, Cm, 4)
+    with pytest.raises(lnb.LinompssError):
+        lnb.ompss_dsyrk("L", "N", 0, 4, 4, 1.0, A, 4, Cm, 4)

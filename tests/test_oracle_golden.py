@@ -132,3 +132,15 @@ def test_oracle_vs_live_reference_ragged():
     O.chol_rl(A1, 20)
     O.ref_chol("rl", A2, 20)
     np.testing.assert_allclose(np.tril(A1), np.tril(A2), rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("case", ["LN_b", "LN_b0", "LT_b", "UN_b", "UT_b"])
+def test_blocked_dsyrk(golden_dir, case):
+    """The oracle's SYRK against the reference's own blocked ompss_dsyrk
+    (syrk_main.c): the requested triangle, the other one untouched."""
+    d = load(golden_dir, "dsyrk_" + case)
+    n, k, alpha, beta = int(d["n"]), int(d["k"]), float(d["alpha"]), float(d["beta"])
+    uplo, trans = case[0], case[1]
+    Cm = d["C"].copy(order="F")
+    O.syrk(uplo, trans, n, k, alpha, np.asfortranarray(d["A"]), beta, Cm)
+    np.testing.assert_allclose(Cm, d["out"], rtol=0, atol=1e-12 * np.abs(d["out"]).max())
