@@ -6,11 +6,11 @@
 //   potrf   : leaf diagonal tile in shared memory (k_potrf.cuh)
 //   trsm    : panel solve B <- B L^-T, SIMT, rows resident in shared memory,
 //             left-looking over 32-column blocks with the leaf's 32x32 inverses;
-//             optionally writes the TF32 operand copies of the result
+//             optionally writes the TF32 operand copies of the result for the
+//             tensor-core update (hi/lo split x = hi + lo, hi = rna_tf32(x))
 //   syrk    : SIMT lower-triangle update (nested diagonal tiles; plain FP32 mode)
-//   prep    : column-major panel -> K-major operand copies for the tensor-core
-//             update: TF32 hi/lo split (x = hi + lo, hi = rna_tf32(x)), or BF16
-//             scaled by a power of two per 128-row block
+//   prep    : column-major panel -> K-major BF16 operand copy scaled by a power
+//             of two per 128-row block
 //   convert : FP64 A -> FP32 lower triangle with optional symmetric diagonal
 //             equilibration  As = S A S,  S = diag(1/sqrt(a_ii))
 #include "common.cuh"
@@ -292,35 +292,6 @@ __global__ void __launch_bounds__(256) k_syrk_lower_f32_simt(const float *__rest
         }
 }
 
-// ------------------------------------------------------------------------
-// panel prep: X (m x kb, column-major FP32) -> K-major operand copies
-// ------------------------------------------------------------------------
-// mode 0: hi/lo TF32 split into two fp32 arrays; mode 1: hi only
-__global__ void __launch_bounds__(256) k_prep_tf32(const float *__restrict__ X, int64_t ldx, int64_t m, int kb,
-                                                   int kpad, float *hi, float *lo)
-{
-    __shared__ float t[32][33];
-    const int64_t r0 = (int64_t)blockIdx.x * 32;
-    const int k0 = blockIdx.y * 32;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 8 rows of 32
-    for (int i = ty; i < 32; i += 8) {                        // read column k0+i, rows r0+tx
-        const int k = k0 + i;
-        const int64_t r = r0 + tx;
-        t[i][tx] = (k < kb && r < m) ? X[r + (int64_t)k * ldx] : 0.f;
-    }
-    __syncthreads();
-    for (int i = ty; i < 32; i += 8) {                        // write row r0+i, k0+tx
-        const int64_t r = r0 + i;
-        const int k = k0 + tx;
-        if (r < m && k < kpad) {
-            const float x = t[tx][i];
-            const float h = tf32_rna(x);
-            hi[r * kpad + k] = h;
-            if (lo) lo[r * kpad + k] = x - h;
-        }
-    }
-}
-
 // per 128-row block: scale = smallest power of two >= max |x| (1 if the block is zero)
 __global__ void __launch_bounds__(256) k_prep_bf16_scale(const float *__restrict__ X, int64_t ldx, int64_t m, int kb,
                                                          float *scale)
@@ -469,16 +440,6 @@ extern "C" int lnb_k_syrk_lower_f32_simt(const float *P, int64_t ldp, float *C, 
     if (nrows <= c0 || c1 <= c0 || kdim <= 0) return 0;
     dim3 grid((unsigned)((c1 - c0 + 63) / 64), (unsigned)((nrows - c0 + 63) / 64));
     k_syrk_lower_f32_simt<<<grid, 256, 0, s>>>(P, ldp, C, ldc, nrows, c0, c1, kdim);
-    lnb_prof_count(1);
-    return (int)cudaGetLastError();
-}
-
-extern "C" int lnb_k_prep_tf32(const float *X, int64_t ldx, int64_t m, int kb, int kpad, float *hi, float *lo,
-                               lnb_stream_t s)
-{
-    if (m <= 0) return 0;
-    dim3 grid((unsigned)((m + 31) / 32), (unsigned)((kpad + 31) / 32));
-    k_prep_tf32<<<grid, 256, 0, s>>>(X, ldx, m, kb, kpad, hi, lo);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }

@@ -346,14 +346,6 @@ __global__ void __launch_bounds__(256) k_gemm_f64(char ta, char tb, int64_t M, i
         }
 }
 
-__global__ void k_copy_lower_f64(const double *src, int64_t lds, double *dst, int64_t ldd, int64_t n)
-{
-    const int64_t c = blockIdx.y;
-    for (int64_t r = c + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n;
-         r += (int64_t)gridDim.x * blockDim.x)
-        dst[r + c * ldd] = src[r + c * lds];
-}
-
 }  // namespace lnb
 
 // ========================================================================
@@ -424,13 +416,6 @@ extern "C" int lnb_k_syrk_lower_f64(const double *P, int64_t ldp, double *C, int
     }
 }
 
-extern "C" int lnb_k_gemm_f64(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
-                              const double *A, int64_t lda, const double *B, int64_t ldb, double beta,
-                              double *C, int64_t ldc, lnb_stream_t s)
-{
-    return lnb_k_gemm_tri_f64(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, 0, s);
-}
-
 extern "C" int lnb_k_gemm_tri_f64(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
                                   const double *A, int64_t lda, const double *B, int64_t ldb,
                                   double beta, double *C, int64_t ldc, char tri, lnb_stream_t s)
@@ -442,12 +427,3 @@ extern "C" int lnb_k_gemm_tri_f64(char ta, char tb, int64_t m, int64_t n, int64_
     return (int)cudaGetLastError();
 }
 
-extern "C" int lnb_k_copy_lower_f64(const double *src, int64_t lds, double *dst, int64_t ldd,
-                                    int64_t n, lnb_stream_t s)
-{
-    if (n <= 0) return 0;
-    dim3 grid((unsigned)((n + 255) / 256 < 64 ? (n + 255) / 256 : 64), (unsigned)n);
-    k_copy_lower_f64<<<grid, 256, 0, s>>>(src, lds, dst, ldd, n);
-    lnb_prof_count(1);
-    return (int)cudaGetLastError();
-}

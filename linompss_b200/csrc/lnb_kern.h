@@ -41,11 +41,8 @@ int lnb_k_trsm_rlt_f64(const double *L, int64_t lda, const double *dinv, double 
  * k < kdim.  P and C are both indexed from the trailing matrix's origin. */
 int lnb_k_syrk_lower_f64(const double *P, int64_t ldp, double *C, int64_t ldc,
                          int64_t nrows, int64_t c0, int64_t c1, int kdim, lnb_stream_t s);
-/* Generic C = alpha op(A) op(B) + beta C on device memory (tile-task ABI). */
-int lnb_k_gemm_f64(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
-                   const double *A, int64_t lda, const double *B, int64_t ldb, double beta,
-                   double *C, int64_t ldc, lnb_stream_t s);
-/* Same, restricted to the triangle tri ('L' or 'U') of C; tri = 0: full. */
+/* Generic C = alpha op(A) op(B) + beta C on device memory (tile-task ABI),
+ * restricted to the triangle tri ('L' or 'U') of C; tri = 0: full. */
 int lnb_k_gemm_tri_f64(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
                        const double *A, int64_t lda, const double *B, int64_t ldb, double beta,
                        double *C, int64_t ldc, char tri, lnb_stream_t s);
@@ -90,10 +87,8 @@ int lnb_k_trsm_rlt_prep_f32(const float *L, int64_t lda, const float *dinv, floa
                             int bs, float *hi, float *lo, int kpad, lnb_stream_t s);
 int lnb_k_syrk_lower_f32_simt(const float *P, int64_t ldp, float *C, int64_t ldc, int64_t nrows,
                               int64_t c0, int64_t c1, int kdim, lnb_stream_t s);
-/* K-major operand copies of a solved panel X (m x kb, ld ldx): TF32 hi (and
- * lo = x - hi when lo != NULL), or BF16 with per-128-row power-of-two scales */
-int lnb_k_prep_tf32(const float *X, int64_t ldx, int64_t m, int kb, int kpad, float *hi, float *lo,
-                    lnb_stream_t s);
+/* K-major BF16 operand copy of a solved panel X (m x kb, ld ldx) with
+ * per-128-row power-of-two scales (the TF32 copies come from the panel solve) */
 int lnb_k_prep_bf16(const float *X, int64_t ldx, int64_t m, int kb, int kpad, float *scale, void *out,
                     lnb_stream_t s);
 /* A32 = lower(S A S) in FP32 with S = diag(1/sqrt(a_ii)) (S = I if !equilibrate) */
@@ -157,10 +152,6 @@ int lnb_k_cg_xr_f64(int64_t n, const double *num, const double *den, const doubl
 int lnb_k_cg_p_f64(int64_t n, int mode, const double *num, const double *den, const double *r,
                    double *p, lnb_stream_t s);
 int lnb_k_axpy3_f64(int64_t n, double a, const double *x, const double *y, double *z, lnb_stream_t s);
-
-/* ---- utility ------------------------------------------------------------- */
-int lnb_k_copy_lower_f64(const double *src, int64_t lds, double *dst, int64_t ldd, int64_t n,
-                         lnb_stream_t s);
 
 #ifdef __cplusplus
 }
