@@ -161,3 +161,31 @@ def test_update_cta_pairs_match_single_cta(lnb, monkeypatch, mode, n, b):
         out[pair] = np.tril(A).astype(np.float64)
     tol = {"tf32x3": 2e-5, "tf32": 2e-3, "bf16": 2e-2}[mode]
     np.testing.assert_allclose(out["1"], out["0"], rtol=0, atol=tol * np.abs(out["0"]).max())
+
+
+@pytest.mark.parametrize("bs", [64, 96, 160, 352, 480, 512])
+def test_cluster_diagonal_factor_single_tile(lnb, bs):
+    """One diagonal tile (n = b, whole 32-blocks): the 8-CTA cluster factor alone,
+    for odd and even block counts (block rows q and 15 - q per CTA).  The factor
+    meets the FP32 residual bound and matches the FP64 Cholesky; the upper
+    triangle keeps its input values."""
+    lnb.set_factor_mode(MODES["tf32x3"])
+    A0 = O.spd_covariance(bs, 0.5, seed=bs)
+    A = np.asfortranarray(A0.astype(np.float32))
+    upper = np.triu(A, 1).copy()
+    assert lnb.ompss_schol_rl(bs, bs, bs, A, bs) == 0
+    assert resid32(A0, A) <= RESID["tf32x3"]
+    L = np.linalg.cholesky(A0)
+    np.testing.assert_allclose(np.tril(A), L, rtol=0, atol=2e-5 * np.abs(L).max())
+    np.testing.assert_array_equal(np.triu(A, 1), upper)
+
+
+@pytest.mark.parametrize("bs,bad", [(512, 0), (512, 31), (512, 32), (512, 300), (512, 511), (160, 100)])
+def test_cluster_diagonal_factor_reports_pivot(lnb, bs, bad):
+    """A non-positive pivot inside a single cluster-factored tile is reported
+    1-based, from the first block (step before the sweep) to the last one."""
+    lnb.set_factor_mode(MODES["tf32x3"])
+    A0 = O.spd_diag_dominant(bs, seed=bs + bad).astype(np.float32)
+    A0[bad, bad] = -5.0
+    A = np.asfortranarray(A0.copy())
+    assert lnb.ompss_schol_rl(bs, bs, bs, A, bs) == bad + 1
