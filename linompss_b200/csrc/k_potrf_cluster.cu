@@ -51,19 +51,30 @@ LNB_DEV int pc_slot(int i, int k, int q) { return i < PCS ? k : q + 1 + k; }
 // the first non-positive pivot.
 LNB_DEV int pc_factor_block(float *D, float *rv, int lane)
 {
-    float a[32];
+    // dd[cc]: every lane's copy of the diagonal entry lane cc holds in a[cc].
+    // It takes the same fma(-x, x, .) with the broadcast x = L[cc][c] as lane
+    // cc's own entry, so it is bit-identical, and the next pivot needs no
+    // shuffle on the chain of 32 dependent columns.
+    float a[32], dd[32];
 #pragma unroll
-    for (int c = 0; c < 32; ++c) a[c] = D[c * 32 + lane];
+    for (int c = 0; c < 32; ++c) {
+        a[c] = D[c * 32 + lane];
+        dd[c] = D[c * 32 + c];
+    }
     int bad = 0;
 #pragma unroll
     for (int c = 0; c < 32; ++c) {
-        const float d = __shfl_sync(0xffffffffu, a[c], c);
+        const float d = dd[c];
         if (bad == 0 && !(d > 0.f)) bad = c + 1;
         const float s = rsqrtf(d);
         a[c] = (lane == c) ? d * s : a[c] * s;
         if (lane == 0) rv[c] = s;
 #pragma unroll
-        for (int cc = c + 1; cc < 32; ++cc) a[cc] = fmaf(-a[c], __shfl_sync(0xffffffffu, a[c], cc), a[cc]);
+        for (int cc = c + 1; cc < 32; ++cc) {
+            const float x = __shfl_sync(0xffffffffu, a[c], cc);
+            a[cc] = fmaf(-a[c], x, a[cc]);
+            dd[cc] = fmaf(-x, x, dd[cc]);
+        }
     }
 #pragma unroll
     for (int c = 0; c < 32; ++c) D[c * 32 + lane] = a[c];
