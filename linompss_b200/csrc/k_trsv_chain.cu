@@ -563,8 +563,9 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
             for (int r = 0; r < NR; ++r)
                 if ((r & 3) == kq && m < in_ && r < a.nrhs)
                     atomicAdd(a.B + (oi + m) + (int64_t)r * a.ldb, -part[r]);
-            fence_acq_rel_gpu();
         }
+        // the CTA barrier orders every thread's updates before thread 0's
+        // GPU-scope release fence, which publishes them with the counter
         __syncthreads();
         if (tid == 0) {
             fence_acq_rel_gpu();
