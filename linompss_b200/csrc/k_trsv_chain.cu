@@ -28,6 +28,8 @@
 //     counter.  Items of row i only wait on blocks j < i-W, which the chain
 //     produced before it needs row i, so the walk cannot deadlock.
 // Every wait is bounded and reports a site code in the status word.
+#include <string.h>
+
 #include "common.cuh"
 #include "tc_sm100.cuh"
 
@@ -61,6 +63,7 @@ struct Args {
     const TT *T; int64_t ldt; const TT *dinv;   // inverses stored in the precision of T
     double *B; int64_t ldb; int64_t n; int nrhs;
     int nb, fwd, vec;           // vec: T and ldt allow 16-byte copies
+    int tma;                    // the chain CTA stages its band tiles through the tensor map (FP32)
     int *ticket, *cnt, *ready;  // cnt/ready indexed by chain position
     lnb_status_t *st; long long wait_ns;
 };
@@ -91,6 +94,11 @@ LNB_DEV void bulk_copy_g2s(void *smem, const void *gmem, uint32_t bytes, uint64_
                      smem_u32(smem)),
                  "l"(gmem), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
+}
+// hint: bring the box at (x, y) of a tensor map into L2
+LNB_DEV void prefetch_box_l2(const CUtensorMap *map, int x, int y)
+{
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global [%0, {%1, %2}];" ::"l"(map), "r"(x), "r"(y) : "memory");
 }
 // hint: bring `bytes` (a multiple of 16, 16-byte aligned) into L2
 LNB_DEV void prefetch_l2(const void *p, uint32_t bytes)
@@ -203,6 +211,39 @@ LNB_DEV void gemv_tile(const TT *S, const double *X, int m, int kq, double (&par
     }
 }
 
+// A 64 x 64 FP32 tile staged by TMA as two 32-row boxes (64 columns of 128
+// bytes each) in the 128-byte-swizzled layout: element (row r, column c) of
+// the stored block.  Needs a 1024-byte-aligned tile.
+LNB_DEV int swz(int r, int c) { return ((r >> 5) << 11) + (c << 5) + ((((r & 31) >> 2) ^ (c & 7)) << 2) + (r & 3); }
+
+// gemv_tile for a tile in that layout (FP32)
+template <int NR, bool TR>
+LNB_DEV void gemv_tile_sw(const float *S, const double *X, int m, int kq, double (&part)[NR])
+{
+    if constexpr (TR) {
+        // op[m][k] = stored (row k, column m); rows k0..k0+3 are one 16-byte chunk
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int k0 = 4 * (kq + 4 * u);
+            const float4 q = *reinterpret_cast<const float4 *>(S + swz(k0, m));
+            const float v[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+#pragma unroll
+                for (int r = 0; r < NR; ++r) part[r] = fma((double)v[e], X[r * TH + k0 + e], part[r]);
+        }
+    } else {
+        // op[m][k] = stored (row m, column k)
+#pragma unroll
+        for (int v = 0; v < 16; ++v) {
+            const int k = kq + 4 * v;
+            const double t = (double)S[swz(m, k)];
+#pragma unroll
+            for (int r = 0; r < NR; ++r) part[r] = fma(t, X[r * TH + k], part[r]);
+        }
+    }
+}
+
 // k owned by lane kq for the j-th inverse element (same partition as the
 // FP64 tiles, so the reads of the staged vector are conflict-free)
 template <bool TR>
@@ -290,7 +331,7 @@ LNB_DEV void drain_wait(uint64_t *bar, uint32_t parity, long long budget_ns)
 }
 
 template <typename TT, int NR, bool TR>
-__global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
+__global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a, const __grid_constant__ CUtensorMap tmT)
 {
     constexpr int W = Cfg<TT>::W, CW = Cfg<TT>::CW;
     constexpr int LD = Ld<TT, TR>::v;
@@ -307,8 +348,10 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
 
     if (item == 0) {
         // ================= the chain CTA =================
-        TT *tiles = reinterpret_cast<TT *>(sm_raw);                                  // [2][W][TS]
-        double *ring = reinterpret_cast<double *>(sm_raw + sizeof(TT) * 2 * W * TS);  // [W+1][NR][64]
+        // tiles 1024-byte aligned (the swizzled TMA layout needs it)
+        unsigned char *sm = reinterpret_cast<unsigned char *>(((uintptr_t)sm_raw + 1023) & ~(uintptr_t)1023);
+        TT *tiles = reinterpret_cast<TT *>(sm);                                       // [2][W][TS]
+        double *ring = reinterpret_cast<double *>(sm + sizeof(TT) * 2 * W * TS);       // [W+1][NR][64]
         double *bbuf = ring + (W + 1) * NR * TH;                                      // [NBUF][NR][64]
         double *accs = bbuf + NBUF * NR * TH;                                         // [NR][64]
         ChainBars *cb = reinterpret_cast<ChainBars *>(accs + NR * TH);
@@ -416,7 +459,22 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
             if (p + 1 < nb) {
                 const int ip = blk(a, p + 1);
                 TT *tb = tiles + ((p + 1) & 1) * W * TS;
-                if (bulk) {
+                if (a.tma) {
+                    // one thread: two 32-row boxes per band tile, counted on tfull
+                    if (tid == 0) {
+                        const int ntl = p + 1 < W ? p + 1 : W;
+                        tc::mbar_arrive_expect_tx(&cb->tfull[(p + 1) & 1], ntl * TH * TH * (int)sizeof(TT));
+                        for (int k = 1; k <= ntl; ++k) {
+                            const int jb = blk(a, p + 1 - k);
+                            const int rb = TR ? jb : ip, cbk = TR ? ip : jb;
+#pragma unroll
+                            for (int h = 0; h < 2; ++h)
+                                tc::tma_load_2d(tb + (k - 1) * TS + h * 2048, &tmT, &cb->tfull[(p + 1) & 1],
+                                                rb * TH + 32 * h, cbk * TH);
+                        }
+                    }
+                    staged = p + 1;
+                } else if (bulk) {
                     const int ntl = p + 1 < W ? p + 1 : W;
                     if (tid == 0) tc::mbar_arrive_expect_tx(&cb->tfull[(p + 1) & 1], ntl * TH * TH * (int)sizeof(TT));
                     const int k = 1 + (tid >> 6), col = tid & 63;
@@ -439,7 +497,18 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
             if (!bulk) cp_async_commit();
             // L2 prefetch PF steps ahead (band tiles, one column per thread, and the
             // diagonal inverse), so the cp.async of the next step is served from L2
-            if (a.vec && p + PF < nb) {
+            if (a.tma) {
+                if (tid == 0 && p + PF < nb) {
+                    const int ip = blk(a, p + PF);
+                    for (int k = 1; k <= W && p + PF - k >= 0; ++k) {
+                        const int jb = blk(a, p + PF - k);
+                        const int rb = TR ? jb : ip, cbk = TR ? ip : jb;
+                        prefetch_box_l2(&tmT, rb * TH, cbk * TH);
+                        prefetch_box_l2(&tmT, rb * TH + 32, cbk * TH);
+                    }
+                    prefetch_l2(a.dinv + (int64_t)ip * TH * TH, TH * TH * sizeof(TT));
+                }
+            } else if (a.vec && p + PF < nb) {
                 const int k = 1 + (tid >> 6);
                 if (k <= W && p + PF - k >= 0)
                     prefetch_tile_col<TT, TR>(a, blk(a, p + PF), blk(a, p + PF - k), tid & 63);
@@ -451,9 +520,16 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a)
             for (int r = 0; r < NR; ++r) part[r] = 0.0;
 #pragma unroll
             for (int k = 1; k <= W; ++k)
-                if (p - k >= 0)
-                    gemv_tile<TT, NR, TR>(tiles + (p & 1) * W * TS + (k - 1) * TS, ring + ((p - k) % (W + 1)) * NR * TH,
-                                          m, kq, part);
+                if (p - k >= 0) {
+                    const TT *tk = tiles + (p & 1) * W * TS + (k - 1) * TS;
+                    const double *xk = ring + ((p - k) % (W + 1)) * NR * TH;
+                    if constexpr (sizeof(TT) == 4) {
+                        if (a.tma) gemv_tile_sw<NR, TR>(reinterpret_cast<const float *>(tk), xk, m, kq, part);
+                        else gemv_tile<TT, NR, TR>(tk, xk, m, kq, part);
+                    } else {
+                        gemv_tile<TT, NR, TR>(tk, xk, m, kq, part);
+                    }
+                }
             quad_sum<NR>(part);
             const int slot = p % NBUF;
             const bool okb = tc::mbar_wait(&cb->bfull[slot], (p / NBUF) & 1, a.wait_ns, &cb->abort, a.st);
@@ -581,13 +657,14 @@ constexpr size_t smem_bytes()
 {
     constexpr int W = Cfg<TT>::W, CW = Cfg<TT>::CW;
     constexpr size_t TSB = sizeof(TT) * TH * Ld<TT, TR>::v;
-    constexpr size_t chainb = 2 * W * TSB + sizeof(double) * ((W + 1) + NBUF + 1) * NR * TH + sizeof(ChainBars);
+    constexpr size_t chainb =
+        1024 + 2 * W * TSB + sizeof(double) * ((W + 1) + NBUF + 1) * NR * TH + sizeof(ChainBars);
     constexpr size_t workb = 2 * CW * TSB + sizeof(double) * CW * NR * TH;
     return chainb > workb ? chainb : workb;
 }
 
 template <typename TT, int NR, bool TR>
-int launch(const Args<TT> &a, lnb_stream_t s)
+int launch(const Args<TT> &a, const CUtensorMap &tm, lnb_stream_t s)
 {
     constexpr int W = Cfg<TT>::W, CW = Cfg<TT>::CW;
     constexpr size_t smem = smem_bytes<TT, NR, TR>();
@@ -603,9 +680,35 @@ int launch(const Args<TT> &a, lnb_stream_t s)
     if (S > 0) witems = CW * (S / CW) * (S / CW + 1) / 2 + (S % CW) * (S / CW + 1);
     int64_t grid = 1 + witems;
     if (grid > sms) grid = sms;
-    k_trsm_chain<TT, NR, TR><<<(unsigned)grid, NTHR, smem, s>>>(a);
+    k_trsm_chain<TT, NR, TR><<<(unsigned)grid, NTHR, smem, s>>>(a, tm);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
+}
+
+// FP32 n x n column-major T (ld ldt) as a 2D tensor map with 32 x 64 boxes in
+// the 128-byte-swizzled layout; 0 on success
+typedef CUresult (*EncodeTiledFnC)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static int tile_map(CUtensorMap *m, const void *T, int64_t n, int64_t ldt)
+{
+    static EncodeTiledFnC fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return -1;
+        fn = (EncodeTiledFnC)p;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)n, (cuuint64_t)n};
+    cuuint64_t strides[1] = {(cuuint64_t)ldt * 4};
+    cuuint32_t box[2] = {32, 64};
+    cuuint32_t estr[2] = {1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(T), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : -1;
 }
 
 template <typename TT>
@@ -620,11 +723,17 @@ int trsm_chain(char uplo, char trans, int64_t n, int64_t nrhs, const TT *T, int6
     a.vec = ((uintptr_t)T % 16 == 0) && ((ldt * (int64_t)sizeof(TT)) % 16 == 0);
     a.ticket = sync; a.cnt = sync + 4; a.ready = sync + 4 + a.nb;
     a.st = st; a.wait_ns = wait_ns;
+    // FP32 T in whole 64-blocks with 16-byte-aligned columns: the chain CTA's
+    // band tiles come through a tensor map (boxes 32 rows x 64 columns, 128-byte swizzle)
+    CUtensorMap tm;
+    memset(&tm, 0, sizeof tm);
+    a.tma = 0;
+    if (sizeof(TT) == 4 && a.vec && n % TH == 0 && tile_map(&tm, T, n, ldt) == 0) a.tma = 1;
     const bool tr = trans == 'T';
-    if (nrhs <= 1) return tr ? launch<TT, 1, true>(a, s) : launch<TT, 1, false>(a, s);
-    if (nrhs <= 2) return tr ? launch<TT, 2, true>(a, s) : launch<TT, 2, false>(a, s);
-    if (nrhs <= 4) return tr ? launch<TT, 4, true>(a, s) : launch<TT, 4, false>(a, s);
-    return tr ? launch<TT, 8, true>(a, s) : launch<TT, 8, false>(a, s);
+    if (nrhs <= 1) return tr ? launch<TT, 1, true>(a, tm, s) : launch<TT, 1, false>(a, tm, s);
+    if (nrhs <= 2) return tr ? launch<TT, 2, true>(a, tm, s) : launch<TT, 2, false>(a, tm, s);
+    if (nrhs <= 4) return tr ? launch<TT, 4, true>(a, tm, s) : launch<TT, 4, false>(a, tm, s);
+    return tr ? launch<TT, 8, true>(a, tm, s) : launch<TT, 8, false>(a, tm, s);
 }
 
 }  // namespace chain
