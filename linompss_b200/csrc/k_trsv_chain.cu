@@ -583,17 +583,54 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a, const __grid
     }
 
     // ================= worker CTAs =================
-    TT *wbuf = reinterpret_cast<TT *>(sm_raw);                                     // [2][CW][TS]
-    double *xw = reinterpret_cast<double *>(sm_raw + sizeof(TT) * 2 * CW * TS);    // [CW][NR][64]
+    // tiles 1024-byte aligned (the swizzled TMA layout needs it)
+    unsigned char *wsm = reinterpret_cast<unsigned char *>(((uintptr_t)sm_raw + 1023) & ~(uintptr_t)1023);
+    TT *wbuf = reinterpret_cast<TT *>(wsm);                                        // [2][CW][TS]
+    double *xw = reinterpret_cast<double *>(wsm + sizeof(TT) * 2 * CW * TS);       // [CW][NR][64]
+    uint64_t *wfull = reinterpret_cast<uint64_t *>(xw + CW * NR * TH);             // [2], TMA staging
     const int64_t total = 1 + items_before<W, CW>(nb);
     const int m = tid >> 2, kq = tid & 3;
     int buf = 0;
     int row = 0, chunk = 0;
+    // TMA staging: thread 0 issues two 32-row boxes per tile, counted on wfull[b];
+    // use[b] counts the completed phases of wfull[b], pend[b] marks boxes in flight
+    int use[2] = {0, 0}, pend[2] = {0, 0};
+    if (a.tma) {
+        if (tid == 0) {
+            tc::mbar_init(&wfull[0], 1);
+            tc::mbar_init(&wfull[1], 1);
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+    }
+    auto stage_item = [&](int b, int irow, int j0, int j1) {
+        if (a.tma) {
+            if (tid == 0) {
+                tc::mbar_arrive_expect_tx(&wfull[b], (j1 - j0) * TH * TH * (int)sizeof(TT));
+                for (int jj = j0; jj < j1; ++jj) {
+                    const int i = blk(a, irow), j = blk(a, jj);
+                    const int rb = TR ? j : i, cbk = TR ? i : j;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        tc::tma_load_2d(wbuf + b * CW * TS + (jj - j0) * TS + h * 2048, &tmT, &wfull[b],
+                                        rb * TH + 32 * h, cbk * TH);
+                }
+            }
+            pend[b] = 1;
+        } else {
+            for (int jj = j0; jj < j1; ++jj)
+                stage_tile<TT, TR>(a, wbuf + b * CW * TS + (jj - j0) * TS, blk(a, irow), blk(a, jj), tid, NTHR);
+        }
+    };
+    // boxes in flight land before the CTA leaves (bounded)
+    auto drain = [&]() {
+        for (int b = 0; b < 2; ++b)
+            if (pend[b]) drain_wait(&wfull[b], (uint32_t)(use[b] & 1), a.wait_ns);
+    };
     if (item < total) {
         decode<W, CW>(item - 1, nb, row, chunk);
         const int j0 = chunk * CW, j1 = min(j0 + CW, row - W);
-        for (int jj = j0; jj < j1; ++jj)
-            stage_tile<TT, TR>(a, wbuf + (jj - j0) * TS, blk(a, row), blk(a, jj), tid, NTHR);
+        stage_item(0, row, j0, j1);
     }
     cp_async_commit();
     while (item < total) {
@@ -605,9 +642,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a, const __grid
         if (next < total) {
             decode<W, CW>(next - 1, nb, nrow, nchunk);
             const int j0 = nchunk * CW, j1 = min(j0 + CW, nrow - W);
-            for (int jj = j0; jj < j1; ++jj)
-                stage_tile<TT, TR>(a, wbuf + (buf ^ 1) * CW * TS + (jj - j0) * TS, blk(a, nrow), blk(a, jj), tid,
-                                   NTHR);
+            stage_item(buf ^ 1, nrow, j0, j1);
         }
         cp_async_commit();
         const int j0 = chunk * CW, j1 = min(j0 + CW, row - W);
@@ -616,21 +651,40 @@ __global__ void __launch_bounds__(NTHR, 1) k_trsm_chain(Args<TT> a, const __grid
             if (!s_ok) { atomicCAS(&a.st->timeout, 0, 6); a.st->timeout_item = (int)item; }
         }
         __syncthreads();
-        if (!s_ok) { cp_async_wait<0>(); return; }
+        if (!s_ok) { cp_async_wait<0>(); drain(); return; }
         for (int idx = tid; idx < (j1 - j0) * NR * TH; idx += NTHR) {
             const int t = idx / (NR * TH), r = (idx / TH) % NR, k = idx % TH;
             const int j = blk(a, j0 + t);
             const int64_t oj = (int64_t)j * TH;
             xw[idx] = (k < blen(a, j) && r < a.nrhs) ? __ldcg(a.B + (oj + k) + (int64_t)r * a.ldb) : 0.0;
         }
-        cp_async_wait<1>();
-        __syncthreads();
+        if (a.tma) {
+            volatile int no_abort = 0;
+            const bool okw = tc::mbar_wait(&wfull[buf], (uint32_t)(use[buf] & 1), a.wait_ns, &no_abort, a.st);
+            if (okw) { ++use[buf]; pend[buf] = 0; }
+            if (!__syncthreads_and(okw)) {
+                if (tid == 0) { atomicCAS(&a.st->timeout, 0, 7); a.st->timeout_item = (int)item; }
+                drain();
+                return;
+            }
+        } else {
+            cp_async_wait<1>();
+            __syncthreads();
+        }
         if (tid < NCOMP) {
             double part[NR];
 #pragma unroll
             for (int r = 0; r < NR; ++r) part[r] = 0.0;
-            for (int jj = j0; jj < j1; ++jj)
-                gemv_tile<TT, NR, TR>(wbuf + buf * CW * TS + (jj - j0) * TS, xw + (jj - j0) * NR * TH, m, kq, part);
+            for (int jj = j0; jj < j1; ++jj) {
+                const TT *tk = wbuf + buf * CW * TS + (jj - j0) * TS;
+                const double *xk = xw + (jj - j0) * NR * TH;
+                if constexpr (sizeof(TT) == 4) {
+                    if (a.tma) gemv_tile_sw<NR, TR>(reinterpret_cast<const float *>(tk), xk, m, kq, part);
+                    else gemv_tile<TT, NR, TR>(tk, xk, m, kq, part);
+                } else {
+                    gemv_tile<TT, NR, TR>(tk, xk, m, kq, part);
+                }
+            }
             quad_sum<NR>(part);
             const int i = blk(a, row);
             const int64_t oi = (int64_t)i * TH;
@@ -659,7 +713,7 @@ constexpr size_t smem_bytes()
     constexpr size_t TSB = sizeof(TT) * TH * Ld<TT, TR>::v;
     constexpr size_t chainb =
         1024 + 2 * W * TSB + sizeof(double) * ((W + 1) + NBUF + 1) * NR * TH + sizeof(ChainBars);
-    constexpr size_t workb = 2 * CW * TSB + sizeof(double) * CW * NR * TH;
+    constexpr size_t workb = 1024 + 2 * CW * TSB + sizeof(double) * CW * NR * TH + 16;
     return chainb > workb ? chainb : workb;
 }
 
