@@ -28,6 +28,7 @@
 //     counter.  Items of row i only wait on blocks j < i-W, which the chain
 //     produced before it needs row i, so the walk cannot deadlock.
 // Every wait is bounded and reports a site code in the status word.
+#include <stdlib.h>
 #include <string.h>
 
 #include "common.cuh"
@@ -782,7 +783,9 @@ int trsm_chain(char uplo, char trans, int64_t n, int64_t nrhs, const TT *T, int6
     CUtensorMap tm;
     memset(&tm, 0, sizeof tm);
     a.tma = 0;
-    if (sizeof(TT) == 4 && a.vec && n % TH == 0 && tile_map(&tm, T, n, ldt) == 0) a.tma = 1;
+    const char *env = getenv("LNB_CHAIN_TMA");   /* 0: stage by bulk copies instead */
+    const bool want = !(env && *env && atoi(env) == 0);
+    if (want && sizeof(TT) == 4 && a.vec && n % TH == 0 && tile_map(&tm, T, n, ldt) == 0) a.tma = 1;
     const bool tr = trans == 'T';
     if (nrhs <= 1) return tr ? launch<TT, 1, true>(a, tm, s) : launch<TT, 1, false>(a, tm, s);
     if (nrhs <= 2) return tr ? launch<TT, 2, true>(a, tm, s) : launch<TT, 2, false>(a, tm, s);
