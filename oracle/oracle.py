@@ -233,6 +233,14 @@ def ref_dsyrk(uplo, trans, b, n, k, alpha, A, lda, beta, Cm, ldc) -> None:
     f(ref_opt(uplo), ref_opt(trans), b, n, k, alpha, _ptr(A), lda, beta, _ptr(Cm), ldc)
 
 
+def ref_ssyrk(uplo, trans, b, n, k, alpha, A, lda, beta, Cm, ldc) -> None:
+    """the reference's own blocked ompss_ssyrk (syrk_main.c, FP32), Cm updated in place"""
+    f = ref().ompss_ssyrk
+    f.argtypes = [_OmpssBlas] * 2 + [C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_int, C.c_float,
+                                     C.c_void_p, C.c_int]
+    f(ref_opt(uplo), ref_opt(trans), b, n, k, alpha, _ptr(A), lda, beta, _ptr(Cm), ldc)
+
+
 def ref_cg(A: np.ndarray, rhs: np.ndarray, bm: int, tol: float, steps: int):
     n = A.shape[0]
     x = np.zeros(n)

@@ -15,7 +15,7 @@ scaled down to a few hundred KB in total:
               a ragged n % b != 0 case like N=1989, b=533)
   spdsolv_*   spdsolv.c / spdsolv_setup.c (B = A X with X ~ U[0,1))
   dsyrk_*     the reference's ompss_dsyrk (syrk_main.c): 4 uplo/trans cases and beta 0,
-              ragged n and k against b, lda and ldc padded
+              ragged n and k against b, lda and ldc padded; ssyrk_* its FP32 twin
   dtrsm_*     tests/dense_tests/trsm_test.c (4 left cases, lda != m, ldb != m,
               alpha = -2.11, entries U[0,1) + 100 -- scaled to M=60, N=50, b=13)
   dcg_*       itref.c dcg_pure on a G G^T/n + I matrix
@@ -117,6 +117,18 @@ def dsyrk_cases():
                      bb=np.int64(b), alpha=np.float64(alpha), beta=np.float64(beta))
 
 
+def ssyrk_case():
+    # the FP32 twin ompss_ssyrk, lower and no transpose, ragged n and k against b
+    n, k, b, alpha, beta = 70, 40, 16, -1.3, 0.7
+    rng = np.random.default_rng(22)
+    A = np.asfortranarray(rng.standard_normal((n + 5, k)).astype(np.float32))
+    C0 = np.asfortranarray(rng.standard_normal((n + 3, n)).astype(np.float32))
+    D = C0.copy(order="F")
+    O.ref_ssyrk("L", "N", b, n, k, alpha, A, n + 5, beta, D, n + 3)
+    save("ssyrk_LN_b", A=A, C=C0, out=D, n=np.int64(n), k=np.int64(k), bb=np.int64(b),
+         alpha=np.float64(alpha), beta=np.float64(beta))
+
+
 def dcg_cases():
     for n, bm, steps, tol, seed in ((64, 16, 8, 1e-10, 14), (64, 16, 200, 1e-10, 14),
                                     (100, 32, 300, 1e-12, 15)):
@@ -170,5 +182,6 @@ if __name__ == "__main__":
     spdsolv_cases()
     dtrsm_cases()
     dsyrk_cases()
+    ssyrk_case()
     dcg_cases()
     itref_cases()

@@ -305,3 +305,19 @@ def test_ompss_dsyrk_rejects_bad_arguments(lnb):
         lnb.ompss_dsyrk("X", "N", 2, 4, 4, 1.0, A, 4, Cm, 4)
     with pytest.raises(lnb.LinompssError):
         lnb.ompss_dsyrk("L", "N", 0, 4, 4, 1.0, A, 4, Cm, 4)
+
+
+def test_ompss_ssyrk_golden(lnb, golden_dir):
+    """ompss_ssyrk against the reference's FP32 blocked SYRK: the library sums in
+    FP64 and rounds once, so it differs from the reference's FP32 sums by their
+    rounding; the other triangle and the rows past n are untouched."""
+    d = load(golden_dir, "ssyrk_LN_b")
+    n, k, bb = int(d["n"]), int(d["k"]), int(d["bb"])
+    A = d["A"].copy(order="F")
+    Cm = d["C"].copy(order="F")
+    assert lnb.ompss_ssyrk("L", "N", bb, n, k, float(d["alpha"]), A, A.shape[0], Cm, Cm.shape[0],
+                           beta=float(d["beta"])) == 0
+    tol = 4 * k * np.finfo(np.float32).eps * np.abs(d["out"]).max()
+    np.testing.assert_allclose(Cm, d["out"], rtol=0, atol=tol)
+    np.testing.assert_array_equal(np.triu(Cm[:n], 1), np.triu(d["C"][:n], 1))
+    np.testing.assert_array_equal(Cm[n:], d["C"][n:])

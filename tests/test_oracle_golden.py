@@ -144,3 +144,14 @@ def test_blocked_dsyrk(golden_dir, case):
     Cm = d["C"].copy(order="F")
     O.syrk(uplo, trans, n, k, alpha, np.asfortranarray(d["A"]), beta, Cm)
     np.testing.assert_allclose(Cm, d["out"], rtol=0, atol=1e-12 * np.abs(d["out"]).max())
+
+
+def test_blocked_ssyrk(golden_dir):
+    """The oracle's FP32 SYRK against the reference's ompss_ssyrk: FP32 sums in a
+    different order, so within FP32 rounding of the k-term dot products."""
+    d = load(golden_dir, "ssyrk_LN_b")
+    n, k = int(d["n"]), int(d["k"])
+    Cm = d["C"].copy(order="F")
+    O.syrk("L", "N", n, k, float(d["alpha"]), np.asfortranarray(d["A"]), float(d["beta"]), Cm)
+    tol = 4 * k * np.finfo(np.float32).eps * np.abs(d["out"]).max()
+    np.testing.assert_allclose(Cm, d["out"], rtol=0, atol=tol)
