@@ -134,9 +134,10 @@ LNB_EXPORT int task_dgemm(ompssblas_t transa, ompssblas_t transb, int bm, int bn
  * iterate on exit; stops at ||r||_2/||b||_2 <= tol or after `steps` steps.
  * Returns -1 if converged, else the number of steps (the reference's own
  * convention, itref.c:922-924).  The recurrence is the reference's as it
- * executes, including its direction update p = 2 r (see DESIGN notes in the
- * source); bm is the reference's row-block size and only affects the order
- * of partial sums there. */
+ * executes: its direction update runs with the old and new residual ratio
+ * fixed at 1 and with aliased operands, so it computes p = 2 r, a damped
+ * steepest descent rather than textbook CG.  bm is the reference's
+ * row-block size and only affects the order of partial sums there. */
 LNB_EXPORT int ompss_dcg(int n, int bm, const double *A, int lda, const double *b, double *x,
                          double tol, int steps);
 
@@ -169,9 +170,13 @@ LNB_EXPORT int lnb_schol_dev(int n, int b, float *dA, int lda, int *info_dev, vo
  * caller's stream only.  Its scratch (block inverses + status word) is a
  * fixed file-scope device array of 256 KB held by every GPU that loads the
  * library until exit; tile sizes b > 1024 are rejected with LNB_ETOOBIG.
- * The first call on a device looks up that array's device address; make
- * that first call before any stream capture.  All calls share the array:
- * calls that overlap on the GPU (other streams, other host threads) race. */
+ * The first call on a device looks up that array's device address and
+ * keeps it; make that first call before any stream capture.  Under lazy
+ * module loading that first call may also load the library's kernels, which
+ * the CUDA driver does with its own memory.  cudaDeviceReset destroys the
+ * array with the context, so do not call this entry point again after a
+ * reset in the same process.  All calls share the array: calls that overlap
+ * on the GPU (other streams, other host threads) race. */
 LNB_EXPORT int lnb_dchol_noalloc_dev(int n, int b, double *dA, int lda, int *info_dev, void *stream);
 
 /* Triangular solves with the lower factor: trans 'N' solves L Y = B,

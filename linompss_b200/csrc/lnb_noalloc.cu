@@ -19,13 +19,18 @@
 #include "lnb_host.h"
 
 // inverses for tiles up to LNB_NOALLOC_MAX_B (32 blocks of 32 x 32 doubles),
-// then the status word (2 doubles = 16 bytes)
+// then the status word, rounded up to whole doubles
 #define LNB_NOALLOC_MAX_B 1024
 #define LNB_NOALLOC_DINV ((LNB_NOALLOC_MAX_B / 32) * 1024)
-static __device__ __align__(256) double g_noalloc_scratch[LNB_NOALLOC_DINV + 2];
+#define LNB_NOALLOC_STATUS ((sizeof(lnb_status_t) + sizeof(double) - 1) / sizeof(double))
+static __device__ __align__(256) double g_noalloc_scratch[LNB_NOALLOC_DINV + LNB_NOALLOC_STATUS];
+static_assert(sizeof(g_noalloc_scratch) >= LNB_NOALLOC_DINV * sizeof(double) + sizeof(lnb_status_t),
+              "the status word must fit behind the block inverses");
 
 // device address of g_noalloc_scratch, looked up once per device with that
-// device current (a host-side reference to the symbol is not a device address)
+// device current (a host-side reference to the symbol is not a device address).
+// The cached address lives as long as the device's primary context: a
+// cudaDeviceReset in the caller's process makes it stale.
 static double *g_scratch_dev[64];
 
 static int scratch_for_current_device(double **out)

@@ -9,7 +9,10 @@
 #
 # Invoked by `make -C oracle ref`; never run the reference's own autotools.
 
-REF_SRC ?= /root/reference/src
+REF_SRC ?=
+ifeq ($(strip $(REF_SRC)),)
+$(error set REF_SRC to the reference's src/ directory)
+endif
 OUT     := _ref
 CC      ?= gcc
 RCFLAGS := -O2 -w -fPIC -DHAVE_CONFIG_H -I$(OUT) \

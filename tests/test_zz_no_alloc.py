@@ -34,14 +34,21 @@ def lib(cuda):
     return L
 
 
-def factor(lib, fn, A0, b, dev):
+def factor(lib, fn, A0, b, dev, free_bytes=None):
+    """Factor A0 through entry point `fn`; if free_bytes is a list, append the
+    device's free memory just before and just after the call."""
     import torch
     n = A0.shape[0]
     At = torch.tensor(np.ascontiguousarray(A0.T), device=dev)   # column-major view
     info = torch.full((1,), -99, dtype=torch.int32, device=dev)
     stream = torch.cuda.current_stream()
+    torch.cuda.synchronize()
+    if free_bytes is not None:
+        free_bytes.append(torch.cuda.mem_get_info()[0])
     rc = getattr(lib, fn)(n, b, At.data_ptr(), At.stride(0), info.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize()
+    if free_bytes is not None:
+        free_bytes.append(torch.cuda.mem_get_info()[0])
     assert rc == 0, rc
     return At.cpu().numpy().T, int(info.item())
 
@@ -49,10 +56,14 @@ def factor(lib, fn, A0, b, dev):
 @pytest.mark.parametrize("cases", [[(1000, 256, 1), (700, 100, 2)], [(512, 512, 3), (1537, 1024, 4)]])
 def test_noalloc_matches_regular_entry_point_twice(lib, cuda, cases):
     eps = np.finfo(float).eps
-    for n, b, seed in cases:     # two calls in a row on different inputs
+    for call, (n, b, seed) in enumerate(cases):     # two calls in a row on different inputs
         A0 = O.spd_covariance(n, 1e-2, seed=seed)
         L_ref, info_ref = factor(lib, "lnb_dchol_dev", A0, b, cuda)
-        L_na, info_na = factor(lib, "lnb_dchol_noalloc_dev", A0, b, cuda)
+        free = []
+        L_na, info_na = factor(lib, "lnb_dchol_noalloc_dev", A0, b, cuda, free)
+        if call > 0:
+            # the property the entry point exists for: a warm call takes no device memory
+            assert free[0] == free[1], f"free device memory changed by {free[0] - free[1]} bytes"
         assert info_ref == 0 and info_na == 0
         np.testing.assert_allclose(np.tril(L_na), np.tril(L_ref), rtol=0, atol=64 * n * eps * np.abs(L_ref).max())
         np.testing.assert_array_equal(np.triu(L_na, 1), np.triu(A0, 1))
