@@ -66,6 +66,9 @@ def parse():
     p.add_argument("--no-plain", action="store_true", help="skip the plain-FP64 comparison (mixed/bf16)")
     p.add_argument("--no-batched", action="store_true", help="skip the batched uneven-systems measurement")
     p.add_argument("--batch-count", type=int, default=10000)
+    p.add_argument("--no-configs", action="store_true", help="skip the other configurations' records")
+    p.add_argument("--ref-budget-s", type=float, default=150.0,
+                   help="reference arm: stop timing full-size calls once their total passes this")
     a = p.parse_args()
     w = dict(WORKLOADS[a.workload])
     for k in ("n", "b", "nrhs"):
@@ -291,32 +294,84 @@ def cpu_run(n, b, nrhs, steps, warmup, A_host=None):
     return flops_of(n, nrhs) / sec / 1e12, kind, (cores if kind == "reference" else 1), sec
 
 
+def workload_inputs(w, rank, device):
+    """The seeded inputs of a workload: A (n x n, symmetric) and B (nrhs x n,
+    i.e. the n x nrhs right-hand sides column-major), on `device`."""
+    import torch
+    A0 = make_spd(w["n"], w["delta"], 1234 + rank, device, w["scaled"])
+    g = torch.Generator(device=device)
+    g.manual_seed(99 + rank)
+    B0 = torch.randn(w["nrhs"], w["n"], dtype=torch.float64, device=device, generator=g)
+    return A0, B0
+
+
+def workload_config(args, w, world):
+    """`config` of the JSON line: the workload, identical for both arms"""
+    return {"workload": f"spd_{args.workload}_n{w['n']}_b{w['b']}_rhs{w['nrhs']}", "n": w["n"], "b": w["b"],
+            "nrhs": w["nrhs"],
+            "matrix": ("D (G G^T/n + %g I) D" if w["scaled"] else "G G^T/n + %g I") % w["delta"],
+            "inputs": "A: G ~ N(0,1) seed 1234 (torch generator on the device); B ~ N(0,1) seed 99",
+            "l2": "inputs larger than L2 (126 MB); plain-FP64 A restored between steps",
+            "parallelism": f"replicas x{world}"}
+
+
 def reference_arm(args, world, rank):
+    """The reference's own FP64-accurate solve, dspdsolv_main (spdsolv_main.c:10-20:
+    tile Cholesky + two blocked triangular solves), compiled from its sources
+    (oracle/_ref/libref.so, OpenBLAS on every host thread), on the SAME seeded
+    inputs and size as this workload.  One full-size call takes tens of seconds
+    on the host, so the warm-up calls run an n = 4096 slice of the same matrix
+    and the timed steps stop once their total passes --ref-budget-s (at least
+    one full-size call); `steps` reports the calls actually timed."""
     if rank != 0:
         return
+    import numpy as np
     w = args.w
-    # bounded sample of the workload: same distribution at n = 8192 (the reference
-    # has no mixed-precision path: its FP64-accurate solve is dspdsolv_main)
-    n = min(w["n"], 8192)
-    b = min(w["b"], 512)
-    A = None
-    try:
-        import torch
-        if torch.cuda.is_available():
-            A = make_spd(n, w["delta"], 0, "cuda", w["scaled"]).cpu().numpy()
-    except Exception:
-        A = None
-    v, kind, cores, sec = cpu_run(n, b, w["nrhs"], args.steps, args.warmup, A)
-    line = {"metric": METRIC, "value": round(v, 6), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": f"spd_{args.workload}_n{w['n']}_b{w['b']}_rhs{w['nrhs']}",
-                       "sample": f"n={n} b={b}", "n": n, "b": b, "nrhs": w["nrhs"]},
+    n, b, nrhs = w["n"], w["b"], w["nrhs"]
+    cores = os.cpu_count() or 1
+    os.environ["OPENBLAS_NUM_THREADS"] = str(cores)
+    from oracle import oracle as O
+    kind = "reference" if O.ref_available() else "port"
+    import torch
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    A0d, B0d = workload_inputs(w, 0, dev)
+    A0 = A0d.cpu().numpy().T                          # symmetric: the transposed view is column-major
+    B0 = np.asfortranarray(B0d.cpu().numpy().T)
+    solve = O.ref_spdsolv if kind == "reference" else O.spdsolv
+    nw = min(n, 4096)
+    for _ in range(args.warmup):
+        A = np.asfortranarray(A0[:nw, :nw])
+        B = np.asfortranarray(B0[:nw])
+        solve(A, B, min(b, nw))
+    times = []
+    A = np.empty_like(A0, order="F")
+    B = np.empty_like(B0, order="F")
+    for i in range(args.steps):
+        A[...] = A0
+        B[...] = B0
+        t0 = time.perf_counter()
+        rc = solve(A, B, b)
+        t1 = time.perf_counter()
+        assert rc == 0, rc
+        times.append(t1 - t0)
+        if sum(times) >= args.ref_budget_s:
+            break
+    sec = statistics.mean(times)
+    v = flops_of(n, nrhs) / sec / 1e12
+    # accuracy of the reference's solution, checked in FP64 on the device
+    be = None
+    if dev == "cuda":
+        X = torch.tensor(np.ascontiguousarray(B.T), device=dev)
+        be = backward_error_dev(A0d, X, B0d)
+    line = {"metric": METRIC, "value": round(v, 6), "unit": UNIT, "n_gpus": args.gpus, "steps": len(times),
+            "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": round(sec * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": workload_config(args, w, world),
+            "result": {"backward_error": be},
             "cpu_baseline": {"value": round(v, 6), "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": f"dspdsolv_main n={n} b={b} nrhs={w['nrhs']} of the {args.workload} "
-                                       f"workload's distribution, OpenBLAS threads={cores}, median of "
-                                       f"{args.steps} after {args.warmup} warm-up"},
+                             "sample": f"the full workload: dspdsolv_main n={n} b={b} nrhs={nrhs} on the same "
+                                       f"seeded inputs, OpenBLAS threads={cores}, mean of {len(times)} call(s); "
+                                       f"warm-up on the leading {nw} x {nw} block"},
             "e2e": {"value": round(v, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -483,6 +538,180 @@ def batched_arm(args, world, rank, local, peaks):
                                       "mean": round(float(g[:, 1].sum() / total), 2)}}
 
 
+def fp64_oracle_solve(A, B):
+    """X (nrhs x n) solving A X^T = B^T in FP64 by an independent algorithm:
+    cuSOLVER's potrf + potrs (LAPACK's blocked Cholesky), through torch.  A
+    checker only; the library never calls it."""
+    import torch
+    Lc = torch.linalg.cholesky(A)
+    X = torch.cholesky_solve(B.t().contiguous(), Lc).t().contiguous()
+    del Lc
+    torch.cuda.empty_cache()
+    return X
+
+
+def fwd_err(X, Xref):
+    """normwise forward error max|X - Xref| / max|Xref|"""
+    return float((X - Xref).abs().max() / Xref.abs().max())
+
+
+def factor_residual_dev(A, L):
+    """||A - L L^T||_inf / (n eps ||A||_inf), the bar of potrf_test.c:31-36,
+    in FP64 on the device; L is the column-major lower factor stored as a
+    (cols, ld) tensor (so L.t() is the matrix), A symmetric."""
+    import numpy as np
+    import torch
+    n = A.shape[0]
+    Lm = torch.tril(L.t())
+    R = Lm @ Lm.t()
+    del Lm
+    R.sub_(A)
+    num = R.abs().sum(dim=1).max()
+    del R
+    torch.cuda.empty_cache()
+    return float(num / (n * np.finfo(float).eps / 2 * A.abs().sum(dim=1).max()))
+
+
+def time_events(fn, reps, s, prep=None):
+    """mean device time (ms) of reps calls of fn on stream s (prep outside the events)"""
+    import torch
+    evs = []
+    for _ in range(reps):
+        if prep is not None:
+            prep()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        fn()
+        e1.record(s)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    return statistics.mean(a.elapsed_time(b) for a, b in evs)
+
+
+def config_records(args, world, rank, dev, peaks):
+    """The other reference configurations, each at its full stated size and input
+    distribution, timed on the device (mean of a few calls after one warm-up)
+    with its accuracy checked:
+      fp64_n16384 : plain FP64 factor + solves, b = 512, 1 and 64 rhs, with the
+                    factor residual ||A - L L^T||_inf/(n eps ||A||_inf)
+      tf32x3_delta: the headline workload's matrix family at delta 1e-1 and 1e-5
+      bf16_n49152 : per-tile-scaled BF16 factor + FP64 refinement / PCG, b = 1024,
+                    8 rhs, D-scaled, delta 1e-2 and 1e-4, beside the plain FP64 solve
+    Each mixed record carries iterations, PCG use, refactored tiles, backward
+    error and the forward error against an FP64 cuSOLVER solve."""
+    import numpy as np
+    import torch
+
+    import linompss_b200 as lnb
+    eps = np.finfo(float).eps / 2
+    s = torch.cuda.current_stream()
+    reps = max(1, min(args.steps, 3))
+    out = {}
+
+    def plain(A0, B0, n, b, nrhs, resid):
+        A = torch.empty_like(A0)
+        B = torch.empty_like(B0)
+        info = torch.zeros(1, dtype=torch.int32, device=dev)
+
+        def prep():
+            A.copy_(A0)
+            B.copy_(B0)
+        run = lambda: lnb.dposv_dev(A, B, n, nrhs, b, info=info, stream=s)
+        time_events(run, 1, s, prep)
+        ms = allmax(world, time_events(run, reps, s, prep))
+        assert int(info.item()) == 0
+        rec = {"ms": round(ms, 3), "value": round(world * flops_of(n, nrhs) / ms / 1e9, 4),
+               "backward_error": backward_error_dev(A0, B, B0)}
+        assert rec["backward_error"] <= 10 * n * eps, rec
+        if resid:
+            rec["factor_residual"] = factor_residual_dev(A0, A)
+            assert rec["factor_residual"] <= 10.0, rec
+        X = B.clone()
+        del A, B
+        torch.cuda.empty_cache()
+        return rec, X
+
+    def mixed(A0, B0, n, b, nrhs, factor):
+        X = torch.zeros_like(B0)
+        opts = lnb.ir_opts(factor=getattr(lnb, "FACTOR_" + factor), max_iter=40, pcg_max_iter=400)
+        res = {}
+
+        def run():
+            rc, r = lnb.dsposv_ir_dev(A0, B0, X, n, nrhs, b, opts, stream=s)
+            assert rc == 0, (rc, r, lnb.last_error())
+            res.update(r)
+        time_events(run, 1, s)
+        ms = allmax(world, time_events(run, reps, s))
+        rec = {"ms": round(ms, 3), "value": round(world * flops_of(n, nrhs) / ms / 1e9, 4),
+               "backward_error": backward_error_dev(A0, X, B0)}
+        assert rec["backward_error"] <= 10 * n * eps, rec
+        rec.update({k: res.get(k) for k in ("iterations", "used_pcg", "pcg_iterations", "refactored_tiles",
+                                            "factor_ms", "solve_ms")})
+        return rec, X
+
+    # configuration 2: plain FP64, n = 16384, b = 512, 1 and 64 right-hand sides
+    n, b = 16384, 512
+    A0 = make_spd(n, 1e-2, 2024 + rank, dev)
+    g = torch.Generator(device=dev)
+    g.manual_seed(7 + rank)
+    rec2 = {"n": n, "b": b, "matrix": "G G^T/n + 0.01 I", "bound": "fp64 DMMA tensor"}
+    for nrhs in (1, 64):
+        B0 = torch.randn(nrhs, n, dtype=torch.float64, device=dev, generator=g)
+        r, X = plain(A0, B0, n, b, nrhs, resid=(nrhs == 1))
+        r["forward_error_vs_fp64_oracle"] = fwd_err(X, fp64_oracle_solve(A0, B0))
+        r["frac_of_fp64_dgemm_peak"] = round(r["value"] / peaks["fp64"], 4)
+        rec2[f"rhs{nrhs}"] = r
+        del B0, X
+    out["fp64_n16384_b512"] = rec2
+    del A0
+    torch.cuda.empty_cache()
+
+    # configuration 3: the delta sweep of the headline matrix family
+    n, b = 32768, 512
+    A0 = make_spd(n, 0.0, 1234 + rank, dev)        # G G^T / n; delta added below
+    g.manual_seed(99 + rank)
+    B0 = torch.randn(1, n, dtype=torch.float64, device=dev, generator=g)
+    rec3 = {"n": n, "b": b, "factor": "tf32x3"}
+    cur = 0.0
+    for delta in (1e-1, 1e-5):
+        A0.diagonal().add_(delta - cur)
+        cur = delta
+        r, X = mixed(A0, B0, n, b, 1, "TF32X3")
+        r["forward_error_vs_fp64_oracle"] = fwd_err(X, fp64_oracle_solve(A0, B0))
+        rec3[f"delta_{delta:g}"] = r
+        del X
+    out["tf32x3_n32768_delta_sweep"] = rec3
+    del A0, B0
+    torch.cuda.empty_cache()
+
+    # configuration 4: BF16 per-tile-scaled factor, n = 49152, b = 1024, 8 rhs, D-scaled
+    n, b, nrhs = 49152, 1024, 8
+    A0 = make_spd(n, 0.0, 4900 + rank, dev)
+    gd = torch.Generator(device=dev)
+    gd.manual_seed(4901 + rank)
+    d = torch.pow(10.0, torch.rand(n, dtype=torch.float64, device=dev, generator=gd) * 4.0 - 2.0)
+    A0.mul_(d[:, None]).mul_(d[None, :])
+    B0 = torch.randn(nrhs, n, dtype=torch.float64, device=dev, generator=gd)
+    rec4 = {"n": n, "b": b, "nrhs": nrhs, "matrix": "D (G G^T/n + delta I) D, D = diag(10^u), u ~ U[-2,2]",
+            "factor": "bf16 (per-tile power-of-two scales), equilibrated, PCG fallback"}
+    cur = 0.0
+    for delta in (1e-2, 1e-4):
+        A0.diagonal().add_((delta - cur) * d * d)
+        cur = delta
+        r, X = mixed(A0, B0, n, b, nrhs, "BF16")
+        r["forward_error_vs_fp64_oracle"] = fwd_err(X, fp64_oracle_solve(A0, B0))
+        del X
+        p, Xp = plain(A0, B0, n, b, nrhs, resid=False)
+        r["fp64_plain_ms"] = p["ms"]
+        r["speedup_vs_fp64_plain"] = round(p["ms"] / r["ms"], 3)
+        del Xp
+        rec4[f"delta_{delta:g}"] = r
+    out["bf16_n49152_b1024_rhs8"] = rec4
+    del A0, B0, d
+    torch.cuda.empty_cache()
+    return out
+
+
 def ours_arm(args, world, rank, local):
     import numpy as np
     import torch
@@ -498,10 +727,7 @@ def ours_arm(args, world, rank, local):
     eps = np.finfo(float).eps / 2
     peaks = measure_peaks(dev)
 
-    A0 = make_spd(n, w["delta"], 1234 + rank, dev, w["scaled"])
-    g = torch.Generator(device=dev)
-    g.manual_seed(99 + rank)
-    B0 = torch.randn(nrhs, n, dtype=torch.float64, device=dev, generator=g)   # column-major (nrhs, ld=n)
+    A0, B0 = workload_inputs(w, rank, dev)        # B0: column-major (nrhs, ld=n)
     s = torch.cuda.current_stream()
     mixed = w["factor"] != "FP64"
 
@@ -562,15 +788,19 @@ def ours_arm(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if not mixed else "f64 (factor " +
             w["factor"].lower() + ")", "data": "synthetic",
-            "config": {"workload": f"spd_{args.workload}_n{n}_b{b}_rhs{nrhs}", "n": n, "b": b, "nrhs": nrhs,
-                       "matrix": ("D (G G^T/n + %g I) D" if w["scaled"] else "G G^T/n + %g I") % w["delta"],
-                       "factor": w["factor"].lower(), "backward_error": bw,
-                       "l2": "inputs larger than L2 (126 MB); plain-FP64 A restored between steps",
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config(args, w, world),
             "gpu_launches": prof["launches"]}
+    # accuracy: backward error, and forward error against an independent FP64
+    # solve of the same A and B (LAPACK's potrf/potrs algorithm, cuSOLVER)
+    Xo = fp64_oracle_solve(A0, B0)
+    line["result"] = {"factor": w["factor"].lower(), "backward_error": bw,
+                      "backward_error_bar": 10 * n * eps, "forward_error_vs_fp64_oracle": fwd_err(Xres, Xo),
+                      "fp64_oracle": "cuSOLVER potrf + potrs in FP64 (torch.linalg) on the same A, B"}
+    del Xo
     if mixed:
-        line["config"]["ir"] = {k: last.get(k) for k in ("iterations", "used_pcg", "pcg_iterations",
-                                                         "factor_ms", "solve_ms", "backward_error")}
+        line["result"]["ir"] = {k: last.get(k) for k in ("iterations", "used_pcg", "pcg_iterations",
+                                                         "refactored_tiles", "factor_ms", "solve_ms",
+                                                         "backward_error")}
 
     # roofline of the dominant kernel (the trailing update), timed live
     if prof["update_ms"] > 0:
@@ -674,6 +904,10 @@ def ours_arm(args, world, rank, local):
     line["clocks"] = clk.summary()
     if not args.no_batched:
         line["batched"] = batched_arm(args, world, rank, local, peaks)
+    if args.workload == "mixed" and not args.no_configs:
+        del A0, B0, X
+        torch.cuda.empty_cache()
+        line["configs"] = config_records(args, world, rank, dev, peaks)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ns = min(n, 8192)

@@ -179,6 +179,24 @@ LNB_EXPORT int lnb_schol_dev(int n, int b, float *dA, int lda, int *info_dev, vo
  * on the GPU (other streams, other host threads) race. */
 LNB_EXPORT int lnb_dchol_noalloc_dev(int n, int b, double *dA, int lda, int *info_dev, void *stream);
 
+/* Schedule of the FP64 factorizations (ompss_dchol_*, dspdsolv_main,
+ * lnb_dchol_dev, lnb_dposv_dev).  Process-wide setting; the environment
+ * variable LNB_CHOL_SCHED ("dag" / "streams") overrides it.
+ *   LNB_SCHED_STREAMS: right-looking steps issued by the host on two streams
+ *     (diagonal factor and panel solve on a high-priority stream, the big
+ *     fused DMMA trailing updates behind them): best for large n.
+ *   LNB_SCHED_DAG: one persistent launch that walks the tile task DAG on the
+ *     device (64 x 64 tiles handed out by an atomic ticket in priority order,
+ *     dependencies tracked by per-tile flags, every wait bounded): best where
+ *     the critical path dominates.  The tile size b only shapes the stream
+ *     schedule; the DAG uses its own 64-wide tiles (the factor is the same up
+ *     to rounding).
+ *   LNB_SCHED_AUTO (default): the device DAG for n <= 4096, streams above. */
+#define LNB_SCHED_AUTO     0
+#define LNB_SCHED_STREAMS  1
+#define LNB_SCHED_DAG      2
+LNB_EXPORT void lnb_set_chol_schedule(int sched);
+
 /* Triangular solves with the lower factor: trans 'N' solves L Y = B,
  * 'T' solves L^T X = B, 'B' (both) solves L L^T X = B.  dB: n x nrhs, ld = ldb. */
 LNB_EXPORT int lnb_dpotrs_dev(int n, int nrhs, const double *dL, int lda, double *dB, int ldb,
@@ -307,6 +325,10 @@ LNB_EXPORT int  lnb_prof_read(lnb_prof_t *out);
  * (LNB_ETIMEOUT when the bound works).  wait_us bounds the wait.  The GPU
  * context stays usable afterwards. */
 LNB_EXPORT int lnb_selftest_wait_timeout(long long wait_us);
+/* The same for the factorization's device DAG (LNB_SCHED_DAG): the first
+ * diagonal tile is never handed out, so every other task's wait runs out;
+ * returns LNB_ETIMEOUT when the bound works. */
+LNB_EXPORT int lnb_selftest_chol_wait_timeout(long long wait_us);
 
 #ifdef __cplusplus
 }

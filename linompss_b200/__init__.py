@@ -33,6 +33,7 @@ LIB_PATH = os.path.join(_HERE, "liblinompss_b200.so")
 LNB_OK, LNB_EINVAL, LNB_ENODEV, LNB_ECUDA, LNB_ENOMEM, LNB_ETIMEOUT, LNB_ENOCONV, LNB_ETOOBIG = (
     0, -1, -2, -3, -4, -5, -6, -7)
 FACTOR_FP64, FACTOR_FP32, FACTOR_TF32X3, FACTOR_BF16, FACTOR_TF32 = 0, 1, 2, 3, 4
+SCHED_AUTO, SCHED_STREAMS, SCHED_DAG = 0, 1, 2
 
 
 class LinompssError(RuntimeError):
@@ -378,6 +379,13 @@ def sspdsolv_main(m: int, n: int, b: int, A: np.ndarray, B: np.ndarray) -> int:
     _colmajor(A, np.float32)
     _colmajor(B, np.float32)
     return _chk(lib().sspdsolv_main(C.c_int(m), C.c_int(n), C.c_int(b), _p(A), _p(B)))
+
+
+def set_chol_schedule(sched: int) -> None:
+    """Schedule of the FP64 factorizations: SCHED_AUTO, SCHED_STREAMS (host-issued
+    look-ahead on two streams) or SCHED_DAG (one persistent launch walking the
+    tile DAG on the device)."""
+    lib().lnb_set_chol_schedule(C.c_int(sched))
 
 
 def set_wait_limit_us(us: int) -> None:

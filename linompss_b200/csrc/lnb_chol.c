@@ -69,10 +69,91 @@ int lnb_potrf_tile_f64(double *Akk, int64_t lda, int bs, int64_t row0, double *d
     return 0;
 }
 
+/* ---- schedule choice --------------------------------------------------------
+ * LNB_SCHED_STREAMS: the host-issued two-stream look-ahead below (big fused
+ * DMMA updates; best when the trailing matrix is large).
+ * LNB_SCHED_DAG: one persistent launch that walks the tile DAG on the device
+ * (k_chol_dag.cu; best when the critical path dominates).
+ * LNB_SCHED_AUTO picks by size: the device DAG up to LNB_DAG_AUTO_MAX_N.
+ * The environment variable LNB_CHOL_SCHED ("dag" / "streams") overrides the
+ * process-wide setting. */
+#define LNB_DAG_AUTO_MAX_N 4096
+static int g_sched = LNB_SCHED_AUTO;
+
+void lnb_set_chol_schedule(int sched)
+{
+    if (sched == LNB_SCHED_AUTO || sched == LNB_SCHED_STREAMS || sched == LNB_SCHED_DAG) g_sched = sched;
+}
+
+int lnb_chol_f64_uses_dag(int n)
+{
+    const char *e = getenv("LNB_CHOL_SCHED");
+    if (e && *e) {
+        if (!strcmp(e, "dag")) return 1;
+        if (!strcmp(e, "streams")) return 0;
+    }
+    if (g_sched == LNB_SCHED_DAG) return 1;
+    if (g_sched == LNB_SCHED_STREAMS) return 0;
+    return n <= LNB_DAG_AUTO_MAX_N;
+}
+
 size_t lnb_chol_f64_ws_bytes(int n, int b)
 {
-    (void)n;
-    return lnb_align256((size_t)((b + 31) / 32) * 1024 * sizeof(double)) + 256;
+    return lnb_align256((size_t)((b + 31) / 32) * 1024 * sizeof(double)) + 256 +
+           lnb_align256((size_t)lnb_chol_dag_w_doubles(n) * sizeof(double)) +
+           lnb_align256((size_t)lnb_chol_dag_ints(n) * sizeof(int)) + 512;
+}
+
+/* the device-DAG schedule; w_out (may be NULL) receives the 64 x 64
+ * diagonal-block inverses of L, the layout the triangular solves use */
+static int chol_f64_dag(lnb_ctx *c, int n, double *dA, int64_t lda, lnb_arena *ar, cudaStream_t s,
+                        double *copy_back, int64_t ldh, double **w_out)
+{
+    double *W = (double *)lnb_arena_take(ar, (size_t)lnb_chol_dag_w_doubles(n) * sizeof(double));
+    int *sync = (int *)lnb_arena_take(ar, (size_t)lnb_chol_dag_ints(n) * sizeof(int));
+    if (!W || !sync) return lnb_set_error(LNB_ENOMEM, "chol dag workspace");
+    CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
+    CK(lnb_k_chol_dag_f64(dA, lda, n, W, sync, c->st, lnb_wait_ns(), c->sms, 0, s), "chol dag");
+    if (copy_back) {
+        for (int64_t c0 = 0; c0 < n; c0 += 512) {
+            const int64_t w = n - c0 < 512 ? n - c0 : 512;
+            CK(cudaMemcpy2DAsync(copy_back + c0 + c0 * ldh, (size_t)ldh * sizeof(double), dA + c0 + c0 * lda,
+                                 (size_t)lda * sizeof(double), (size_t)(n - c0) * sizeof(double), (size_t)w,
+                                 cudaMemcpyDeviceToHost, s), "factor copy");
+        }
+    }
+    if (w_out) *w_out = W;
+    return 0;
+}
+
+int lnb_chol_f64_run_w(lnb_ctx *c, int n, int b, double *dA, int64_t lda, lnb_arena *ar, cudaStream_t s,
+                       double *copy_back, int64_t ldh, double **w_out)
+{
+    if (w_out) *w_out = NULL;
+    if (lnb_chol_f64_uses_dag(n)) return chol_f64_dag(c, n, dA, lda, ar, s, copy_back, ldh, w_out);
+    return lnb_chol_f64_run(c, n, b, dA, lda, ar, s, copy_back, ldh);
+}
+
+int lnb_selftest_chol_wait_timeout(long long wait_us)
+{
+    /* 512 x 512 zeros.  The ticket starts at 1, so the first diagonal tile is
+     * never factored and every task below it waits on a flag nothing sets. */
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    const int64_t n = 512;
+    void *ws = lnb_ws(c, lnb_align256(n * n * 8) + lnb_chol_f64_ws_bytes((int)n, 64));
+    if (!ws) return LNB_ENOMEM;
+    lnb_arena ar = {(char *)ws, 0, c->ws_size};
+    double *A = lnb_arena_take(&ar, n * n * 8);
+    double *W = (double *)lnb_arena_take(&ar, (size_t)lnb_chol_dag_w_doubles(n) * sizeof(double));
+    int *sync = (int *)lnb_arena_take(&ar, (size_t)lnb_chol_dag_ints(n) * sizeof(int));
+    if (!sync) return lnb_set_error(LNB_ENOMEM, "self-test workspace");
+    cudaStream_t s = c->main;
+    CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
+    CK(cudaMemsetAsync(A, 0, n * n * 8, s), "zero");
+    CK(lnb_k_chol_dag_f64(A, n, n, W, sync, c->st, (wait_us > 0 ? wait_us : 1000) * 1000LL, c->sms, 1, s),
+       "chol dag");
+    return lnb_status_read(c, s);
 }
 
 int lnb_chol_f64_run(lnb_ctx *c, int n, int b, double *dA, int64_t lda, lnb_arena *ar,
@@ -177,7 +258,7 @@ static int chol_host(int n, int b, double *A, int lda)
     cudaStream_t s = c->main;
     if ((e = copy_lower(dA, ldd, A, lda, n, b, cudaMemcpyHostToDevice, s))) return e;
     const int pinned = lnb_host_is_pinned(A);
-    if ((e = lnb_chol_f64_run(c, n, b, dA, ldd, &ar, s, pinned ? A : NULL, lda))) return e;
+    if ((e = lnb_chol_f64_run_w(c, n, b, dA, ldd, &ar, s, pinned ? A : NULL, lda, NULL))) return e;
     if (!pinned && (e = copy_lower(A, lda, dA, ldd, n, b, cudaMemcpyDeviceToHost, s))) return e;
     return lnb_status_read(c, s);
 }
@@ -208,7 +289,7 @@ static int chol_hyper(int mt, int b, double **Ah)
                                  tile, (size_t)b * sizeof(double), (size_t)b * sizeof(double), (size_t)b,
                                  cudaMemcpyHostToDevice, s), "tile in");
         }
-    int e = lnb_chol_f64_run(c, (int)n, b, dA, ldd, &ar, s, NULL, 0);
+    int e = lnb_chol_f64_run_w(c, (int)n, b, dA, ldd, &ar, s, NULL, 0, NULL);
     if (e) return e;
     for (int j = 0; j < mt; ++j)
         for (int i = j; i < mt; ++i)
@@ -235,7 +316,7 @@ int lnb_dchol_dev(int n, int b, double *dA, int lda, int *info_dev, void *stream
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     cudaStream_t s = (cudaStream_t)stream;
-    if ((e = lnb_chol_f64_run(c, n, b, dA, lda, &ar, s, NULL, 0))) return e;
+    if ((e = lnb_chol_f64_run_w(c, n, b, dA, lda, &ar, s, NULL, 0, NULL))) return e;
     if (info_dev)
         CK(cudaMemcpyAsync(info_dev, &c->st->info, sizeof(int), cudaMemcpyDeviceToDevice, s), "info");
     return 0;

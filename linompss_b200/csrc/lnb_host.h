@@ -67,6 +67,14 @@ size_t lnb_chol_f64_ws_bytes(int n, int b);
 int lnb_chol_f64_run(lnb_ctx *c, int n, int b, double *dA, int64_t lda, lnb_arena *ar,
                      cudaStream_t s, double *copy_back, int64_t ldh);
 
+/* the schedule the FP64 factorization of order n runs: 1 device DAG, 0 streams */
+int lnb_chol_f64_uses_dag(int n);
+/* Factor with the chosen schedule.  w_out (may be NULL) receives the device
+ * DAG's 64 x 64 diagonal-block inverses of L (the triangular solves' layout),
+ * or NULL when the stream schedule ran. */
+int lnb_chol_f64_run_w(lnb_ctx *c, int n, int b, double *dA, int64_t lda, lnb_arena *ar, cudaStream_t s,
+                       double *copy_back, int64_t ldh, double **w_out);
+
 /* ---- FP32-storage factorization (lnb_chol32.c) ---------------------------- */
 int lnb_potrf_tile_f32(float *Akk, int64_t lda, int bs, int64_t row0, float *dinv, lnb_status_t *st,
                        cudaStream_t s);

@@ -47,6 +47,16 @@ int lnb_k_gemm_tri_f64(char ta, char tb, int64_t m, int64_t n, int64_t k, double
                        const double *A, int64_t lda, const double *B, int64_t ldb, double beta,
                        double *C, int64_t ldc, char tri, lnb_stream_t s);
 
+/* Whole FP64 factorization as one persistent launch walking the tile DAG on
+ * the device (k_chol_dag.cu): 64 x 64 tiles, A in place (lower), W receives
+ * the inverses of the diagonal tiles (64 x 64 column-major each, identity past
+ * n), sync lnb_chol_dag_ints(n) ints of scratch (zeroed by the launcher).
+ * ticket0 > 0 only in the wait self-test. */
+int64_t lnb_chol_dag_ints(int64_t n);
+int64_t lnb_chol_dag_w_doubles(int64_t n);
+int lnb_k_chol_dag_f64(double *A, int64_t lda, int64_t n, double *W, int *sync, lnb_status_t *st,
+                       long long wait_ns, int sms, int ticket0, lnb_stream_t s);
+
 /* ---- triangular solves (k_trsv.cu) --------------------------------------- */
 /* Inverses of the h x h diagonal blocks of T: dinv block q (h x h,
  * column-major) is (T[qh:qh+h, qh:qh+h])^-1 for the triangle `uplo` of T,

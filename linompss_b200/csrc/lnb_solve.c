@@ -138,11 +138,16 @@ int lnb_dposv_dev(int n, int nrhs, int b, double *dA, int lda, double *dB, int l
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     cudaStream_t s = (cudaStream_t)stream;
-    int e = lnb_chol_f64_run(c, n, b, dA, lda, &ar, s, NULL, 0);
+    double *dinv = NULL;
+    int e = lnb_chol_f64_run_w(c, n, b, dA, lda, &ar, s, NULL, 0, &dinv);
     if (e) return e;
     if (nrhs > 0) {
-        double *dinv = (double *)lnb_arena_take(&ar, (size_t)nb * TRSV_H * TRSV_H * sizeof(double));
-        CK(lnb_k_trtri_blocks_f64(dA, lda, n, TRSV_H, 'L', 0, dinv, s), "trtri");
+        /* the device DAG leaves the 64 x 64 diagonal-block inverses the solves use */
+        if (!dinv) {
+            dinv = (double *)lnb_arena_take(&ar, (size_t)nb * TRSV_H * TRSV_H * sizeof(double));
+            if (!dinv) return lnb_set_error(LNB_ENOMEM, "posv workspace");
+            CK(lnb_k_trtri_blocks_f64(dA, lda, n, TRSV_H, 'L', 0, dinv, s), "trtri");
+        }
         if ((e = lnb_trsm_f64_run(c, 'L', 'N', 'N', n, nrhs, 1.0, dA, lda, dB, ldb, &ar, s, dinv))) return e;
         if ((e = lnb_trsm_f64_run(c, 'L', 'T', 'N', n, nrhs, 1.0, dA, lda, dB, ldb, &ar, s, dinv))) return e;
     }
@@ -181,12 +186,16 @@ int dspdsolv_main(int m, int nrhs, int b, double *A, double *B)
         CK(cudaMemcpy2DAsync(dB, ldd * sizeof(double), B, (size_t)m * sizeof(double),
                              (size_t)m * sizeof(double), nrhs, cudaMemcpyHostToDevice, s), "B in");
     const int pinned = lnb_host_is_pinned(A);
-    int e = lnb_chol_f64_run(c, m, b, dA, ldd, &ar, s, pinned ? A : NULL, m);
+    double *dinv = NULL;
+    int e = lnb_chol_f64_run_w(c, m, b, dA, ldd, &ar, s, pinned ? A : NULL, m, &dinv);
     if (e) return e;
     if (nrhs > 0) {
-        const int64_t nb = ceil_div(m, TRSV_H);
-        double *dinv = (double *)lnb_arena_take(&ar, (size_t)nb * TRSV_H * TRSV_H * sizeof(double));
-        CK(lnb_k_trtri_blocks_f64(dA, ldd, m, TRSV_H, 'L', 0, dinv, s), "trtri");
+        if (!dinv) {
+            const int64_t nb = ceil_div(m, TRSV_H);
+            dinv = (double *)lnb_arena_take(&ar, (size_t)nb * TRSV_H * TRSV_H * sizeof(double));
+            if (!dinv) return lnb_set_error(LNB_ENOMEM, "spdsolv workspace");
+            CK(lnb_k_trtri_blocks_f64(dA, ldd, m, TRSV_H, 'L', 0, dinv, s), "trtri");
+        }
         if ((e = lnb_trsm_f64_run(c, 'L', 'N', 'N', m, nrhs, 1.0, dA, ldd, dB, ldd, &ar, s, dinv))) return e;
         if ((e = lnb_trsm_f64_run(c, 'L', 'T', 'N', m, nrhs, 1.0, dA, ldd, dB, ldd, &ar, s, dinv))) return e;
         CK(cudaMemcpy2DAsync(B, (size_t)m * sizeof(double), dB, ldd * sizeof(double),
