@@ -649,6 +649,40 @@ def config_records(args, world, rank, dev, peaks):
                                             "factor_ms", "solve_ms")})
         return rec, X
 
+    def schedules(A0, B0, n, b, nrhs):
+        """plain FP64 factor + solves under each FP64 schedule (device DAG vs
+        host-issued streams), same inputs; the library's default picks by n"""
+        rec = {}
+        try:
+            for name, sched in (("dag", lnb.SCHED_DAG), ("streams", lnb.SCHED_STREAMS)):
+                lnb.set_chol_schedule(sched)
+                r, X = plain(A0, B0, n, b, nrhs, resid=False)
+                rec[name + "_ms"] = r["ms"]
+                rec[name + "_backward_error"] = r["backward_error"]
+                del X
+        finally:
+            lnb.set_chol_schedule(lnb.SCHED_AUTO)
+        rec["dag_speedup"] = round(rec["streams_ms"] / rec["dag_ms"], 3)
+        return rec
+
+    # configuration 1: plain FP64, n = 2048, b = 256, 1 rhs, (R + R^T)/2 + n I
+    n, b = 2048, 256
+    gr = torch.Generator(device=dev)
+    gr.manual_seed(rank)
+    R = torch.rand(n, n, dtype=torch.float64, device=dev, generator=gr)
+    A0 = (R + R.t()) / 2
+    A0.diagonal().add_(float(n))
+    del R
+    xt = torch.rand(1, n, dtype=torch.float64, device=dev, generator=gr) * 2 - 1
+    B0 = (A0 @ xt.t()).t().contiguous()
+    r, X = plain(A0, B0, n, b, 1, resid=True)
+    r["forward_error_vs_x_true"] = fwd_err(X, xt)
+    r["forward_error_vs_fp64_oracle"] = fwd_err(X, fp64_oracle_solve(A0, B0))
+    r["schedule"] = "dag" if n <= 4096 else "streams"
+    r["schedules"] = schedules(A0, B0, n, b, 1)
+    out["fp64_n2048_b256"] = r
+    del A0, B0, X, xt
+
     # configuration 2: plain FP64, n = 16384, b = 512, 1 and 64 right-hand sides
     n, b = 16384, 512
     A0 = make_spd(n, 1e-2, 2024 + rank, dev)
@@ -660,6 +694,8 @@ def config_records(args, world, rank, dev, peaks):
         r, X = plain(A0, B0, n, b, nrhs, resid=(nrhs == 1))
         r["forward_error_vs_fp64_oracle"] = fwd_err(X, fp64_oracle_solve(A0, B0))
         r["frac_of_fp64_dgemm_peak"] = round(r["value"] / peaks["fp64"], 4)
+        if nrhs == 1:
+            r["schedules"] = schedules(A0, B0, n, b, nrhs)
         rec2[f"rhs{nrhs}"] = r
         del B0, X
     out["fp64_n16384_b512"] = rec2

@@ -42,7 +42,7 @@ constexpr int LDK = TS + 4;         // k-major staged rows (= 4 mod 16 doubles: 
 constexpr int CHUNK = BK * LDK;     // doubles per staged operand chunk
 constexpr int LDS = TS + 1;         // row-major tile for the diagonal factor
 constexpr int SMEM_STAGES = 2 * 2 * CHUNK * (int)sizeof(double);          // 2 stages x {A, B}
-constexpr int SMEM_POTRF = 2 * TS * LDS * (int)sizeof(double);            // S and W
+constexpr int SMEM_POTRF = (2 * TS * LDS + 32) * (int)sizeof(double);     // S, W and the pivot reciprocals
 constexpr int SMEM = SMEM_STAGES > SMEM_POTRF ? SMEM_STAGES : SMEM_POTRF;
 
 struct Args {
@@ -59,56 +59,59 @@ struct Args {
 
 // ---- one warp: Cholesky of a 32 x 32 block and its inverse ------------------
 // S: row-major (ld lds), lower part read and written.  X: row-major (ld ldx),
-// receives inv(L) (lower; zeros above).  Lane r owns row r in registers; the
-// column sweep broadcasts pivots and L's column by shuffles, and carries the
-// inverse along (forward substitution in row form: row c of X is scaled by
-// 1 / L_cc once final, then subtracted from the rows below).  Returns the
-// local column of the first non-positive pivot, or 32.  After a failure the
-// failed pivot and the columns after it keep their updated values (LAPACK's
-// potf2 stops there) and X's rows from the failure on are identity rows.
-LNB_DEV int warp_potrf32_inv(double *S, int lds, double *X, int ldx)
+// receives inv(L) (lower; zeros above).  rd: 32 doubles of scratch.
+// Factor: lane r owns row r in registers; a runtime loop over the columns
+// keeps a[0] the current column (the array shifts down by one per step, so
+// every index is a compile-time constant) and reads L's finished column back
+// from shared memory, where every lane reads the same word (a broadcast).
+// Inverse: lane q forms column q of inv(L) by forward substitution with the
+// stored reciprocal pivots, X[r][q] = (delta_rq - sum_{k<r} L[r][k] X[k][q]) / L[r][r].
+// Returns the local column of the first non-positive pivot, or 32.  After a
+// failure the failed pivot and the columns after it keep their updated values
+// (LAPACK's potf2 stops there) and X's rows from the failure on are identity
+// rows.
+LNB_DEV int warp_potrf32_inv(double *S, int lds, double *X, int ldx, double *rd)
 {
     const int lane = threadIdx.x & 31;
-    double a[32], x[32];
+    double a[32];
 #pragma unroll
-    for (int c = 0; c < 32; ++c) {
-        a[c] = (c <= lane) ? S[lane * lds + c] : 0.0;
-        x[c] = (c == lane) ? 1.0 : 0.0;
-    }
+    for (int k = 0; k < 32; ++k) a[k] = (k <= lane) ? S[lane * lds + k] : 0.0;
     int fail = 32;
-#pragma unroll
+#pragma unroll 1
     for (int c = 0; c < 32; ++c) {
-        const double d = __shfl_sync(0xffffffffu, a[c], c);
-        if (fail == 32 && !(d > 0.0)) fail = c;      // warp-uniform
-        if (fail == 32) {
-            const double rs = rsqrt(d);
-            const double l = (lane == c) ? d * rs : a[c] * rs;
-            if (lane >= c) a[c] = l;
-            if (lane == c) {
+        const double d = __shfl_sync(0xffffffffu, a[0], c);
+        if (!(d > 0.0)) {                                // warp-uniform: stop here
+            fail = c;
 #pragma unroll
-                for (int q = 0; q <= c; ++q) x[q] *= rs;
-            }
-#pragma unroll
-            for (int cc = c + 1; cc < 32; ++cc) {
-                const double lcc = __shfl_sync(0xffffffffu, l, cc);
-                if (lane >= cc) a[cc] = fma(-l, lcc, a[cc]);
-            }
-#pragma unroll
-            for (int q = 0; q <= c; ++q) {
-                const double xcq = __shfl_sync(0xffffffffu, x[q], c);
-                if (lane > c) x[q] = fma(-l, xcq, x[q]);
-            }
+            for (int k = 0; k < 32; ++k)
+                if (c + k <= lane) S[lane * lds + c + k] = a[k];
+            break;
         }
-    }
-    if (lane >= fail) {
+        const double rs = rsqrt(d);
+        if (lane >= c) S[lane * lds + c] = (lane == c) ? d * rs : a[0] * rs;
+        if (lane == c) rd[c] = rs;
+        const double l = a[0] * rs;
+        __syncwarp();
 #pragma unroll
-        for (int q = 0; q < 32; ++q) x[q] = (q == lane) ? 1.0 : 0.0;
+        for (int k = 1; k < 32; ++k) {
+            const double lk = S[((c + k) & 31) * lds + c];
+            if (c + k <= lane) a[k] = fma(-l, lk, a[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < 31; ++k) a[k] = a[k + 1];
+        a[31] = 0.0;
+    }
+    __syncwarp();
+    double x[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+        double sum = (r == lane) ? 1.0 : 0.0;
+#pragma unroll
+        for (int k = 0; k < r; ++k) sum = fma(-S[r * lds + k], x[k], sum);
+        x[r] = (r < fail) ? sum * rd[r < fail ? r : 0] : ((r == lane) ? 1.0 : 0.0);
     }
 #pragma unroll
-    for (int c = 0; c < 32; ++c) {
-        if (c <= lane) S[lane * lds + c] = a[c];
-        X[lane * ldx + c] = (c <= lane) ? x[c] : 0.0;
-    }
+    for (int r = 0; r < 32; ++r) X[r * ldx + lane] = (r >= lane) ? x[r] : 0.0;
     __syncwarp();
     return fail;
 }
@@ -117,12 +120,12 @@ LNB_DEV int warp_potrf32_inv(double *S, int lds, double *X, int ldx)
 // 2 x 2 blocks of 32:  L00 = potrf(S00);  L10 = S10 W00^T;  S11 -= L10 L10^T;
 // L11 = potrf(S11);  W10 = -W11 (L10 W00).  W (row-major, ld LDS) receives
 // inv(L).  Returns the first failed local column, or 64.
-LNB_DEV int cta_potrf64_inv(double *S, double *W, int *s_fail)
+LNB_DEV int cta_potrf64_inv(double *S, double *W, int *s_fail, double *rd)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int idx = tid; idx < 32 * 32; idx += NT) W[(idx >> 5) * LDS + 32 + (idx & 31)] = 0.0;
     if (warp == 0) {
-        const int f = warp_potrf32_inv(S, LDS, W, LDS);
+        const int f = warp_potrf32_inv(S, LDS, W, LDS, rd);
         if (lane == 0) s_fail[0] = f;
     }
     __syncthreads();
@@ -169,7 +172,7 @@ LNB_DEV int cta_potrf64_inv(double *S, double *W, int *s_fail)
     }
     __syncthreads();
     if (warp == 0) {
-        const int f = warp_potrf32_inv(S + 32 * LDS + 32, LDS, W + 32 * LDS + 32, LDS);
+        const int f = warp_potrf32_inv(S + 32 * LDS + 32, LDS, W + 32 * LDS + 32, LDS, rd);
         if (lane == 0) s_fail[1] = f;
     }
     __syncthreads();
@@ -348,7 +351,7 @@ LNB_DEV bool run_tile(const Args &a, int i, int j, double *sm, int *s_ok, int *s
                     S[r * LDS + c] = v;
                 }
         __syncthreads();
-        const int f = cta_potrf64_inv(S, W, s_fail);
+        const int f = cta_potrf64_inv(S, W, s_fail, W + TS * LDS);
         if (tid == 0 && f < cols) atomicCAS(&a.st->info, 0, (int)(cj + f + 1));
         // L (lower part, valid rows/columns) and the inverse (whole 64 x 64, column-major)
         for (int idx = tid; idx < TS * TS; idx += NT) {

@@ -27,7 +27,10 @@ constexpr int SV_THREADS = 256;
 template <int NR>
 struct SvCfg {
     static constexpr int WS = NR >= 8 ? 2 : 16 / NR;
-    static constexpr int G = 4;
+    // 64 columns per item for every NR: the row sums take one atomic per row
+    // per 64 columns (with 8 columns, the atomics of 8 right-hand sides
+    // outnumbered the matrix elements and bounded the kernel)
+    static constexpr int G = 64 / WS;
     static constexpr int IW = WS * G;
     static constexpr int RPT = NR >= 8 ? 2 : NR >= 4 ? 4 : 8;
     static constexpr int SEG = SV_THREADS * RPT;

@@ -1,0 +1,471 @@
+// k_trsv_blk.cu -- triangular solves with an FP32 lower factor and few
+// right-hand sides (1..8), FP64 vectors and arithmetic, built on the inverses
+// of the factor's 512 x 512 diagonal blocks.
+//
+// Semantics of the two blocked solves of dspdsolv_main (spdsolv_main.c:15,17,
+// bblas_dltrsm bblas_trsm.h:119-160): forward L y = b walks block rows top
+// down, y_s = L_ss^-1 (b_s - sum_{j<s} L_sj y_j); backward L^T x = y walks them
+// bottom up, x_s = L_ss^-T (y_s - sum_{j>s} L_js^T x_j).  With the diagonal
+// blocks inverted beforehand every step is matrix-vector work:
+//
+//   * Work items are 64 KB slabs: 64 rows x 256 columns (forward) or 256 rows
+//     x 64 columns (backward) of a 512 x 512 block, 16 items per block, each
+//     brought into shared memory by ONE 2D TMA box issued before the item waits
+//     for its input vector.  An item multiplies its slab by a vector segment and
+//     adds the product into a target segment with FP64 atomics, then bumps a
+//     counter: the residual counter of the target block row (update items,
+//     L_sj y_j or L_js^T x_j) or the solution counter of the step (diagonal
+//     items, with L_ss^-1 or L_ss^-T).
+//   * Items are handed out by an atomic ticket in a topological order that
+//     puts the chain first: step k holds the 16 diagonal items of block s, the
+//     16 items that feed the next block row, then the bulk of the column one
+//     step behind (its remaining rows).  Every item waits only on items of
+//     earlier steps or earlier in its own step, which running CTAs hold, so the
+//     walk cannot deadlock whatever the residency.  All waits are bounded and
+//     report a site code; a CTA that gives up drains its TMA load first.
+//   * The chain is nb = n/512 steps long (64 at n = 32768), against n/64 for a
+//     substitution with 64-wide blocks, and the bulk streams the factor once.
+//
+// The block inverses come from lnb_k_trtri512_f32 (this file): FP64
+// arithmetic, FP32 storage, built column block by column block from the
+// 64 x 64 inverses of lnb_k_trtri_blocks_f32.
+#include <stdlib.h>
+#include <string.h>
+
+#include "common.cuh"
+#include "tc_sm100.cuh"
+
+namespace lnb {
+namespace blk {
+
+constexpr int HB = 512;               // diagonal block order
+constexpr int NTHR = 256;
+constexpr int SLAB = 64 * 256;        // floats per item slab (64 KB)
+constexpr int MAXR = 8;               // right-hand sides per launch
+
+struct Args {
+    int64_t n, np;          // order, padded order nb * HB
+    int nb, nrhs, fwd, nitems;
+    double *R, *Y;          // np x nrhs each (ld np): residual right-hand side, solution
+    int *ticket, *cntR, *cntY;
+    lnb_status_t *st;
+    long long wait_ns;
+};
+
+// items of step k: 16 diagonal, 16 next-row (k < nb-1), 16 per bulk row (k >= 1: nb-1-k rows)
+__host__ __device__ inline int64_t step_start(int64_t k, int64_t nb)
+{
+    const int64_t m = k < nb - 1 ? k : nb - 1;
+    const int64_t bulk = k >= 1 ? (k - 1) * (nb - 1) - (k - 1) * k / 2 : 0;
+    return 16 * (k + m + bulk);
+}
+
+struct Item {
+    int kind;     // 0 diagonal, 1 update
+    int row;      // target block row (residual for updates, solution for diagonal)
+    int col;      // source block column (its solution segment is the input of an update)
+    int part;     // 0..15
+};
+
+LNB_DEV Item decode(int64_t t, const Args &a)
+{
+    int lo = 0, hi = a.nb - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (step_start(mid, a.nb) <= t) lo = mid; else hi = mid - 1;
+    }
+    const int k = lo;
+    int64_t r = t - step_start(k, a.nb);
+    const int s = a.fwd ? k : a.nb - 1 - k;           // block solved at this step
+    Item it;
+    it.part = (int)(r & 15);
+    if (r < 16) { it.kind = 0; it.row = s; it.col = s; return it; }
+    r -= 16;
+    it.kind = 1;
+    if (k < a.nb - 1) {
+        if (r < 16) {                                 // the next block row's last update
+            it.row = a.fwd ? s + 1 : s - 1;
+            it.col = s;
+            return it;
+        }
+        r -= 16;
+    }
+    const int off = (int)(r >> 4);                    // bulk of the column one step behind
+    it.row = a.fwd ? s + 1 + off : s - 1 - off;
+    it.col = a.fwd ? s - 1 : s + 1;
+    return it;
+}
+
+// bounded wait for this CTA's own TMA load; used on the way out after a give-up
+LNB_DEV void drain(uint64_t *bar, uint32_t parity, long long wait_ns)
+{
+    const uint64_t t0 = globaltimer();
+    while (!tc::mbar_try_wait(bar, parity)) {
+        if ((long long)(globaltimer() - t0) > wait_ns) break;
+    }
+}
+
+template <int NR>
+__global__ void __launch_bounds__(NTHR, 2) k_trsm_blk(Args a, const __grid_constant__ CUtensorMap mT,
+                                                        const __grid_constant__ CUtensorMap mI)
+{
+    extern __shared__ __align__(128) float sm[];
+    float *slab = sm;                                             // 64 KB, TMA destination
+    double *vs = reinterpret_cast<double *>(sm + SLAB);           // [NR][256] input segment
+    double *red = vs + NR * 256;                                  // [4][NR][64] partial sums
+    __shared__ __align__(8) uint64_t full;
+    __shared__ int s_t, s_ok;
+    __shared__ volatile int s_abort;     // stays 0: nothing else cuts the slab wait short
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        s_abort = 0;
+        tc::mbar_init(&full, 1);
+        tc::fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    for (;;) {
+        if (tid == 0) s_t = atomicAdd(a.ticket, 1);
+        __syncthreads();
+        const int64_t t = s_t;
+        if (t >= a.nitems) break;
+        const Item it = decode(t, a);
+        const int p = it.part;
+        // source box and the vector / target segments of this item
+        //   forward : slab rows = 64 outputs (p & 7), columns = 256 inputs (p >> 3)
+        //   backward: slab rows = 256 inputs (p >> 3), columns = 64 outputs (p & 7)
+        const int64_t in0 = (int64_t)it.col * HB + 256 * (p >> 3);
+        const int64_t out0 = (int64_t)it.row * HB + 64 * (p & 7);
+        if (tid == 0) {
+            tc::mbar_arrive_expect_tx(&full, SLAB * 4);
+            if (it.kind == 0) {
+                // diagonal block s of the inverses: rows 0..511 of column block s
+                if (a.fwd) tc::tma_load_2d(slab, &mI, &full, 64 * (p & 7), it.row * HB + 256 * (p >> 3));
+                else tc::tma_load_2d(slab, &mI, &full, 256 * (p >> 3), it.row * HB + 64 * (p & 7));
+            } else {
+                // L_{row, col} (forward) or L_{col, row} (backward) of the factor
+                if (a.fwd) tc::tma_load_2d(slab, &mT, &full, (int)out0, (int)in0);
+                else tc::tma_load_2d(slab, &mT, &full, (int)in0, (int)out0);
+            }
+            // the input: a solution segment (updates) or a finished residual (diagonal)
+            bool ok;
+            if (it.kind == 1) {
+                ok = wait_geq(a.cntY + it.col, 16, a.wait_ns, a.st);
+            } else {
+                const int need = 16 * (a.fwd ? it.row : a.nb - 1 - it.row);
+                ok = wait_geq(a.cntR + it.row, need, a.wait_ns, a.st);
+            }
+            if (!ok && atomicCAS(&a.st->timeout, 0, it.kind == 0 ? 41 : 42) == 0) a.st->timeout_item = (int)t;
+            s_ok = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (!s_ok) {
+            if (tid == 0) drain(&full, phase, a.wait_ns);
+            break;
+        }
+        const double *src = it.kind == 1 ? a.Y : a.R;
+        for (int i = tid; i < NR * 256; i += NTHR) {
+            const int q = i >> 8, c = i & 255;
+            vs[i] = q < a.nrhs ? __ldcg(src + in0 + c + (int64_t)q * a.np) : 0.0;
+        }
+        if (tid == 0 && !tc::mbar_wait(&full, phase, a.wait_ns, &s_abort, a.st)) {
+            if (atomicCAS(&a.st->timeout, 0, 43) == 0) a.st->timeout_item = (int)t;
+            s_ok = 0;
+        }
+        __syncthreads();
+        phase ^= 1;
+        if (!s_ok) break;
+        double acc[NR];
+#pragma unroll
+        for (int q = 0; q < NR; ++q) acc[q] = 0.0;
+        if (a.fwd) {
+            // slab[c * 64 + r]: out[r] = sum_c slab[r][c] v[c]; thread (r, cq) takes columns cq, cq+4, ...
+            const int r = tid & 63, cq = tid >> 6;
+#pragma unroll 4
+            for (int c = cq; c < 256; c += 4) {
+                const double l = (double)slab[c * 64 + r];
+#pragma unroll
+                for (int q = 0; q < NR; ++q) acc[q] = fma(l, vs[q * 256 + c], acc[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < NR; ++q) red[(cq * NR + q) * 64 + r] = acc[q];
+            __syncthreads();
+            for (int i = tid; i < 64 * NR; i += NTHR) {
+                const int q = i >> 6, rr = i & 63;
+                const double v = red[(0 * NR + q) * 64 + rr] + red[(1 * NR + q) * 64 + rr] +
+                                 red[(2 * NR + q) * 64 + rr] + red[(3 * NR + q) * 64 + rr];
+                if (q < a.nrhs) atomicAdd((it.kind == 1 ? a.R : a.Y) + out0 + rr + (int64_t)q * a.np,
+                                          it.kind == 1 ? -v : v);
+            }
+        } else {
+            // slab[c * 256 + r]: out[c] = sum_r slab[r][c] v[r]; warp w takes columns 8w..8w+7
+            const int lane = tid & 31, w = tid >> 5;
+            for (int cc = 0; cc < 8; ++cc) {
+                const int c = 8 * w + cc;
+                double s[NR];
+#pragma unroll
+                for (int q = 0; q < NR; ++q) s[q] = 0.0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int r = lane + 32 * k;
+                    const double l = (double)slab[c * 256 + r];
+#pragma unroll
+                    for (int q = 0; q < NR; ++q) s[q] = fma(l, vs[q * 256 + r], s[q]);
+                }
+#pragma unroll
+                for (int q = 0; q < NR; ++q) {
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
+                }
+                if (lane == 0) {
+#pragma unroll
+                    for (int q = 0; q < NR; ++q)
+                        if (q < a.nrhs) atomicAdd((it.kind == 1 ? a.R : a.Y) + out0 + c + (int64_t)q * a.np,
+                                                  it.kind == 1 ? -s[q] : s[q]);
+                }
+            }
+        }
+        // publish: every thread's atomics, then one GPU-scope release of the counter
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            atomicAdd(it.kind == 1 ? a.cntR + it.row : a.cntY + it.row, 1);
+        }
+    }
+}
+
+// R = B (rows < n, zero past n), Y = 0, both np x nrhs
+__global__ void k_blk_pack(const double *B, int64_t ldb, int64_t n, int64_t np, int nrhs, double *R, double *Y)
+{
+    const int q = blockIdx.y;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < np; r += (int64_t)gridDim.x * blockDim.x) {
+        R[r + q * np] = r < n ? B[r + q * ldb] : 0.0;
+        Y[r + q * np] = 0.0;
+    }
+}
+__global__ void k_blk_unpack(const double *Y, int64_t n, int64_t np, double *B, int64_t ldb)
+{
+    const int q = blockIdx.y;
+    for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        B[r + q * ldb] = Y[r + q * np];
+}
+
+// ---- the 512 x 512 diagonal-block inverses ----------------------------------
+// CTA (cb, s): column block cb (64 wide) of inv(L_ss), s = block index.  With
+// X_a the 64 x 64 block (a, cb) of the inverse and D_a the inverse of the 64 x
+// 64 diagonal block a:  X_cb = D_cb,  X_a = -D_a sum_{c=cb}^{a-1} L_ac X_c.
+// FP64 arithmetic on operands widened once as they are staged, FP32 storage
+// (the earlier X_c are read back as stored).  Rows and columns at or past n
+// are the identity's.
+constexpr int TLD = 68;
+constexpr int TRTRI_SMEM = 3 * 64 * TLD * 8;
+
+__global__ void __launch_bounds__(256) k_trtri512(const float *__restrict__ T, int64_t ldt, int64_t n,
+                                                  const float *__restrict__ dinv64, float *Binv)
+{
+    extern __shared__ __align__(16) double tsm[];
+    double (*As)[TLD] = reinterpret_cast<double (*)[TLD]>(tsm);                 // As[k][r] = A[r][k]
+    double (*Bs)[TLD] = reinterpret_cast<double (*)[TLD]>(tsm + 64 * TLD);      // Bs[k][c] = B[k][c]
+    double (*Cs)[TLD] = reinterpret_cast<double (*)[TLD]>(tsm + 128 * TLD);     // the sum, row-major
+    const int cb = blockIdx.x, s = blockIdx.y, tid = threadIdx.x;
+    const int ty = tid >> 4, tx = tid & 15;      // rows 4 ty.., columns 4 tx..
+    const int64_t o = (int64_t)s * HB;           // first row / column of the block
+    const int64_t nb64 = (n + 63) / 64;
+    float *Xb = Binv + (int64_t)s * HB * HB;     // block s: element (r, c) at Xb[r + c * HB]
+    // blocks above the diagonal are zero
+    for (int a = 0; a < cb; ++a)
+        for (int i = tid; i < 64 * 64; i += 256) {
+            const int c = i >> 6, r = i & 63;
+            Xb[(64 * a + r) + (int64_t)(64 * cb + c) * HB] = 0.f;
+        }
+    for (int a = cb; a < 8; ++a) {
+        const int64_t q64 = (o + 64 * a) / 64;      // global 64-block index of diagonal block a
+        double acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        // sum_{c=cb}^{a-1} L_ac X_c
+        for (int c = cb; c < a; ++c) {
+            __syncthreads();
+            for (int i = tid; i < 64 * 64; i += 256) {
+                const int k = i >> 6, r = i & 63;
+                const int64_t gr = o + 64 * a + r, gc = o + 64 * c + k;
+                As[k][r] = (gr < n && gc < n) ? (double)T[gr + gc * ldt] : 0.0;
+                const int cc = i >> 6, kk = i & 63;
+                Bs[kk][cc] = (double)Xb[(64 * c + kk) + (int64_t)(64 * cb + cc) * HB];
+            }
+            __syncthreads();
+#pragma unroll 8
+            for (int k = 0; k < 64; ++k) {
+                const double2 a0 = *reinterpret_cast<const double2 *>(&As[k][4 * ty]);
+                const double2 a1 = *reinterpret_cast<const double2 *>(&As[k][4 * ty + 2]);
+                const double2 b0 = *reinterpret_cast<const double2 *>(&Bs[k][4 * tx]);
+                const double2 b1 = *reinterpret_cast<const double2 *>(&Bs[k][4 * tx + 2]);
+                const double ar[4] = {a0.x, a0.y, a1.x, a1.y}, bc[4] = {b0.x, b0.y, b1.x, b1.y};
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(ar[i], bc[j], acc[i][j]);
+            }
+        }
+        // X_a = (a == cb) ? D_a : -D_a * acc   (D_a = identity past the 64-blocks of the factor)
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                Cs[4 * ty + i][4 * tx + j] = (a == cb) ? ((4 * ty + i) == (4 * tx + j) ? 1.0 : 0.0) : acc[i][j];
+        for (int i = tid; i < 64 * 64; i += 256) {
+            const int k = i >> 6, r = i & 63;          // As[k][r] = D_a[r][k]
+            As[k][r] = q64 < nb64 ? (double)dinv64[q64 * 4096 + r + 64 * k] : (r == k ? 1.0 : 0.0);
+        }
+        __syncthreads();
+        double out[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) out[i][j] = 0.0;
+#pragma unroll 8
+        for (int k = 0; k < 64; ++k) {
+            const double2 d0 = *reinterpret_cast<const double2 *>(&As[k][4 * ty]);
+            const double2 d1 = *reinterpret_cast<const double2 *>(&As[k][4 * ty + 2]);
+            const double2 c0 = *reinterpret_cast<const double2 *>(&Cs[k][4 * tx]);
+            const double2 c1 = *reinterpret_cast<const double2 *>(&Cs[k][4 * tx + 2]);
+            const double dr[4] = {d0.x, d0.y, d1.x, d1.y}, cv[4] = {c0.x, c0.y, c1.x, c1.y};
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) out[i][j] = fma(dr[i], cv[j], out[i][j]);
+        }
+        const double sg = (a == cb) ? 1.0 : -1.0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                Xb[(64 * a + 4 * ty + i) + (int64_t)(64 * cb + 4 * tx + j) * HB] = (float)(sg * out[i][j]);
+    }
+}
+
+typedef CUresult (*EncodeTiledFnB)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// FP32 rows x cols column-major (ld elements) as a 2D tensor map with bx x by boxes
+static int map2d(CUtensorMap *m, const void *base, int64_t rows, int64_t cols, int64_t ld, int bx, int by)
+{
+    static EncodeTiledFnB fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return -1;
+        fn = (EncodeTiledFnB)p;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)rows, (cuuint64_t)cols};
+    cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+    cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by};
+    cuuint32_t estr[2] = {1, 1};
+    const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : -1;
+}
+
+template <int NR>
+static int launch(const Args &a, const CUtensorMap &mT, const CUtensorMap &mI, int sms, cudaStream_t s)
+{
+    const int smem = SLAB * 4 + NR * 256 * 8 + 4 * NR * 64 * 8;
+    cudaError_t e = cudaFuncSetAttribute(k_trsm_blk<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return (int)e;
+    const int grid = a.nitems < 2 * sms ? a.nitems : 2 * sms;
+    k_trsm_blk<NR><<<grid, NTHR, smem, s>>>(a, mT, mI);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace blk
+}  // namespace lnb
+
+extern "C" int64_t lnb_trsm_blk_ints(int64_t n)
+{
+    const int64_t nb = (n + lnb::blk::HB - 1) / lnb::blk::HB;
+    return 32 + 2 * nb;
+}
+extern "C" int64_t lnb_trsm_blk_inv_floats(int64_t n)
+{
+    const int64_t nb = (n + lnb::blk::HB - 1) / lnb::blk::HB;
+    return nb * lnb::blk::HB * lnb::blk::HB;
+}
+extern "C" int64_t lnb_trsm_blk_vec_doubles(int64_t n, int64_t nrhs)
+{
+    const int64_t nb = (n + lnb::blk::HB - 1) / lnb::blk::HB;
+    return 2 * nb * lnb::blk::HB * nrhs;
+}
+// the block solve applies: FP32 T 16-byte aligned with ld a multiple of 4, 1..8 right-hand sides
+extern "C" int lnb_trsm_blk_ok(const float *T, int64_t ldt, int64_t n, int64_t nrhs)
+{
+    const char *e = getenv("LNB_TRSM_BLK");    /* 0: substitution with 64-wide blocks instead */
+    if (e && *e && atoi(e) == 0) return 0;
+    return n >= 2 * lnb::blk::HB && nrhs >= 1 && nrhs <= lnb::blk::MAXR && (uintptr_t)T % 16 == 0 && ldt % 4 == 0;
+}
+
+// Binv: lnb_trsm_blk_inv_floats(n); dinv64: lnb_k_trtri_blocks_f32's 64 x 64 inverses of T
+extern "C" int lnb_k_trtri512_f32(const float *T, int64_t ldt, int64_t n, const float *dinv64, float *Binv,
+                                  lnb_stream_t s)
+{
+    using namespace lnb::blk;
+    if (n <= 0) return 0;
+    const int64_t nb = (n + HB - 1) / HB;
+    cudaError_t e = cudaFuncSetAttribute(k_trtri512, cudaFuncAttributeMaxDynamicSharedMemorySize, TRTRI_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    k_trtri512<<<dim3(8, (unsigned)nb), 256, TRTRI_SMEM, (cudaStream_t)s>>>(T, ldt, n, dinv64, Binv);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
+}
+
+// op(T) X = B in place for lower T (trans 'N': forward, 'T': backward), B n x nrhs
+// FP64 (ld ldb); vec: lnb_trsm_blk_vec_doubles(n, nrhs) doubles; sync:
+// lnb_trsm_blk_ints(n) ints (zeroed here)
+extern "C" int lnb_k_trsm_blk_f32(char trans, int64_t n, int64_t nrhs, const float *T, int64_t ldt, const float *Binv,
+                                  double *B, int64_t ldb, double *vec, int *sync, lnb_status_t *st, long long wait_ns,
+                                  int sms, lnb_stream_t s)
+{
+    using namespace lnb::blk;
+    if (n <= 0 || nrhs <= 0) return 0;
+    if (nrhs > MAXR) return (int)cudaErrorInvalidValue;
+    Args a;
+    a.n = n;
+    a.nb = (int)((n + HB - 1) / HB);
+    a.np = (int64_t)a.nb * HB;
+    a.nrhs = (int)nrhs;
+    a.fwd = trans == 'N';
+    a.nitems = (int)step_start(a.nb, a.nb);
+    a.R = vec;
+    a.Y = vec + a.np * nrhs;
+    a.ticket = sync;
+    a.cntR = sync + 32;
+    a.cntY = sync + 32 + a.nb;
+    a.st = st;
+    a.wait_ns = wait_ns;
+    CUtensorMap mT, mI;
+    memset(&mT, 0, sizeof mT);
+    memset(&mI, 0, sizeof mI);
+    // forward items read 64 x 256 boxes, backward 256 x 64
+    const int bx = a.fwd ? 64 : 256, by = a.fwd ? 256 : 64;
+    if (map2d(&mT, T, n, n, ldt, bx, by) || map2d(&mI, Binv, HB, a.np, HB, bx, by)) return (int)cudaErrorInvalidValue;
+    cudaStream_t cs = (cudaStream_t)s;
+    cudaError_t e = cudaMemsetAsync(sync, 0, (size_t)lnb_trsm_blk_ints(n) * sizeof(int), cs);
+    if (e != cudaSuccess) return (int)e;
+    const dim3 vg((unsigned)((a.np + 255) / 256 < 256 ? (a.np + 255) / 256 : 256), (unsigned)nrhs);
+    k_blk_pack<<<vg, 256, 0, cs>>>(B, ldb, n, a.np, (int)nrhs, a.R, a.Y);
+    int err;
+    if (nrhs <= 1) err = launch<1>(a, mT, mI, sms, cs);
+    else if (nrhs <= 2) err = launch<2>(a, mT, mI, sms, cs);
+    else if (nrhs <= 4) err = launch<4>(a, mT, mI, sms, cs);
+    else err = launch<8>(a, mT, mI, sms, cs);
+    if (err) return err;
+    k_blk_unpack<<<vg, 256, 0, cs>>>(a.Y, n, a.np, B, ldb);
+    lnb_prof_count(3);
+    return (int)cudaGetLastError();
+}

@@ -540,6 +540,15 @@ int ompss_schol_hll(int mt, int b, int t, float **Ah) { (void)t; return schol_hy
 #define TRSV_H 64
 int lnb_k_f64_to_f32(const double *D, int64_t ldd, int64_t m, int64_t k, float *X, int64_t ldx, cudaStream_t st);
 
+int64_t lnb_trsm_blk_ints(int64_t n);
+int64_t lnb_trsm_blk_inv_floats(int64_t n);
+int64_t lnb_trsm_blk_vec_doubles(int64_t n, int64_t nrhs);
+int lnb_trsm_blk_ok(const float *T, int64_t ldt, int64_t n, int64_t nrhs);
+int lnb_k_trtri512_f32(const float *T, int64_t ldt, int64_t n, const float *dinv64, float *Binv, lnb_stream_t s);
+int lnb_k_trsm_blk_f32(char trans, int64_t n, int64_t nrhs, const float *T, int64_t ldt, const float *Binv, double *B,
+                       int64_t ldb, double *vec, int *sync, lnb_status_t *st, long long wait_ns, int sms,
+                       lnb_stream_t s);
+
 static int spotrs_run(lnb_ctx *c, int64_t n, int64_t nrhs, const float *dL, int64_t lda, float *dB, int64_t ldb,
                       char which, lnb_arena *ar, cudaStream_t s)
 {
@@ -550,6 +559,22 @@ static int spotrs_run(lnb_ctx *c, int64_t n, int64_t nrhs, const float *dL, int6
     if (!sync) return lnb_set_error(LNB_ENOMEM, "spotrs workspace");
     CK(lnb_k_trtri_blocks_f32(dL, lda, n, TRSV_H, 'L', 0, dinv, s), "trtri");
     CK(lnb_k_f32_to_f64(dB, ldb, n, nrhs, Z, n, s), "widen");
+    if (lnb_trsm_blk_ok(dL, lda, n, nrhs)) {
+        /* few right-hand sides: the solves on the 512 x 512 diagonal-block inverses */
+        float *binv = lnb_arena_take(ar, (size_t)lnb_trsm_blk_inv_floats(n) * 4);
+        double *vec = lnb_arena_take(ar, (size_t)lnb_trsm_blk_vec_doubles(n, nrhs) * 8);
+        int *bsync = lnb_arena_take(ar, (size_t)lnb_trsm_blk_ints(n) * 4);
+        if (!bsync) return lnb_set_error(LNB_ENOMEM, "spotrs workspace");
+        CK(lnb_k_trtri512_f32(dL, lda, n, dinv, binv, s), "trtri 512");
+        if (which == 'N' || which == 'B')
+            CK(lnb_k_trsm_blk_f32('N', n, nrhs, dL, lda, binv, Z, n, vec, bsync, c->st, lnb_wait_ns(), c->sms, s),
+               "forward");
+        if (which == 'T' || which == 'B')
+            CK(lnb_k_trsm_blk_f32('T', n, nrhs, dL, lda, binv, Z, n, vec, bsync, c->st, lnb_wait_ns(), c->sms, s),
+               "backward");
+        CK(lnb_k_f64_to_f32(Z, n, n, nrhs, dB, ldb, s), "round");
+        return 0;
+    }
     if (which == 'N' || which == 'B')
         CK(lnb_k_trsm_left_f32('L', 'N', n, nrhs, 1.0, dL, lda, dinv, TRSV_H, Z, n, sync, c->st, lnb_wait_ns(), 0, s),
            "forward");
@@ -564,7 +589,9 @@ static size_t spotrs_ws_bytes(int64_t n, int64_t nrhs)
 {
     const int64_t nb = (n + TRSV_H - 1) / TRSV_H;
     return lnb_align256((size_t)nb * TRSV_H * TRSV_H * 8) + lnb_align256((size_t)n * nrhs * 8) +
-           lnb_align256((size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4) + 1024;
+           lnb_align256((size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4) + lnb_align256((size_t)lnb_trsm_blk_inv_floats(n) * 4) +
+           lnb_align256((size_t)lnb_trsm_blk_vec_doubles(n, nrhs) * 8) + lnb_align256((size_t)lnb_trsm_blk_ints(n) * 4) +
+           1024;
 }
 
 int lnb_spotrs_dev(int n, int nrhs, const float *dL, int lda, float *dB, int ldb, char which, void *stream)

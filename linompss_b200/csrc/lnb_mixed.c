@@ -34,6 +34,14 @@
 #define TRSV_H 64
 #define LAPACK_EPS (DBL_EPSILON / 2.0)
 
+int64_t lnb_trsm_blk_ints(int64_t n);
+int64_t lnb_trsm_blk_inv_floats(int64_t n);
+int64_t lnb_trsm_blk_vec_doubles(int64_t n, int64_t nrhs);
+int lnb_trsm_blk_ok(const float *T, int64_t ldt, int64_t n, int64_t nrhs);
+int lnb_k_trtri512_f32(const float *T, int64_t ldt, int64_t n, const float *dinv64, float *Binv, lnb_stream_t s);
+int lnb_k_trsm_blk_f32(char trans, int64_t n, int64_t nrhs, const float *T, int64_t ldt, const float *Binv, double *B,
+                       int64_t ldb, double *vec, int *sync, lnb_status_t *st, long long wait_ns, int sms,
+                       lnb_stream_t s);
 int lnb_k_coldot_f64(int64_t n, int64_t nrhs, const double *U, const double *V, double *out, lnb_stream_t s);
 int lnb_k_pcg_xr_f64(int64_t n, int64_t nrhs, const double *num, const double *den, const double *P,
                      const double *Q, double *X, int64_t ldx, double *R, lnb_stream_t s);
@@ -56,6 +64,11 @@ typedef struct {
     float *A32;
     double *S, *dinv, *R, *Z, *Y, *P, *Q, *ones, *scal; /* scal: 8 * nrhs scalars */
     int *sync;
+    /* solves on the 512 x 512 diagonal-block inverses (k_trsv_blk.cu), when they apply */
+    float *binv;
+    double *bvec;
+    int *bsync;
+    int sms;
 } irws;
 
 static size_t ir_ws_bytes(int64_t n, int64_t nrhs, int b, int mode, int streamed)
@@ -66,6 +79,8 @@ static size_t ir_ws_bytes(int64_t n, int64_t nrhs, int b, int mode, int streamed
                lnb_align256((size_t)nb * TRSV_H * TRSV_H * 8) + 5 * lnb_align256((size_t)n * nrhs * 8) +
                lnb_align256((size_t)8 * (nrhs + 1) * 8) +
                lnb_align256((size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4) + 4096;
+    s += lnb_align256((size_t)lnb_trsm_blk_inv_floats(n) * 4) +
+         lnb_align256((size_t)lnb_trsm_blk_vec_doubles(n, nrhs) * 8) + lnb_align256((size_t)lnb_trsm_blk_ints(n) * 4);
     return s + (streamed ? lnb_chol_f32_stream_ws_bytes((int)n, b, mode) : lnb_chol_f32_ws_bytes((int)n, b, mode)) +
            lnb_refactor_ws_bytes(b);
 }
@@ -74,6 +89,14 @@ static size_t ir_ws_bytes(int64_t n, int64_t nrhs, int b, int mode, int streamed
 static int precond(lnb_ctx *c, const irws *w, cudaStream_t s)
 {
     CK(lnb_k_scale_rows_f64(w->n, w->nrhs, w->S, w->R, w->Z, s), "scale");
+    if (w->binv) {
+        CK(lnb_k_trsm_blk_f32('N', w->n, w->nrhs, w->A32, w->ld32, w->binv, w->Z, w->n, w->bvec, w->bsync, c->st,
+                              lnb_wait_ns(), w->sms, s), "forward solve");
+        CK(lnb_k_trsm_blk_f32('T', w->n, w->nrhs, w->A32, w->ld32, w->binv, w->Z, w->n, w->bvec, w->bsync, c->st,
+                              lnb_wait_ns(), w->sms, s), "backward solve");
+        CK(lnb_k_scale_rows_f64(w->n, w->nrhs, w->S, w->Z, w->Z, s), "scale");
+        return 0;
+    }
     CK(lnb_k_trsm_left_f32('L', 'N', w->n, w->nrhs, 1.0, w->A32, w->ld32, (const float *)w->dinv, TRSV_H, w->Z, w->n, w->sync,
                            c->st, lnb_wait_ns(), 0, s), "forward solve");
     CK(lnb_k_trsm_left_f32('L', 'T', w->n, w->nrhs, 1.0, w->A32, w->ld32, (const float *)w->dinv, TRSV_H, w->Z, w->n, w->sync,
@@ -174,6 +197,16 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
     w.scal = lnb_arena_take(&ar, (size_t)8 * (nrhs + 1) * 8);
     w.sync = lnb_arena_take(&ar, (size_t)lnb_trsm_sync_ints(n, TRSV_H) * 4);
     if (!w.sync) return lnb_set_error(LNB_ENOMEM, "dsposv_ir workspace");
+    w.sms = c->sms;
+    w.binv = NULL;
+    w.bvec = NULL;
+    w.bsync = NULL;
+    if (lnb_trsm_blk_ok(w.A32, w.ld32, n, nrhs)) {
+        w.binv = lnb_arena_take(&ar, (size_t)lnb_trsm_blk_inv_floats(n) * 4);
+        w.bvec = lnb_arena_take(&ar, (size_t)lnb_trsm_blk_vec_doubles(n, nrhs) * 8);
+        w.bsync = lnb_arena_take(&ar, (size_t)lnb_trsm_blk_ints(n) * 4);
+        if (!w.bsync) return lnb_set_error(LNB_ENOMEM, "dsposv_ir workspace");
+    }
     const double tol = opts.tol > 0 ? opts.tol : 10.0 * n * LAPACK_EPS;
 
     /* ---- factor ---- */
@@ -200,6 +233,7 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
         return e > 0 ? lnb_set_error(e, "low-precision factor: tile at row %d could not be refactored", e) : e;
     }
     CK(lnb_k_trtri_blocks_f32(w.A32, w.ld32, n, TRSV_H, 'L', 0, (float *)w.dinv, s), "trtri");
+    if (w.binv) CK(lnb_k_trtri512_f32(w.A32, w.ld32, n, (const float *)w.dinv, w.binv, s), "trtri 512");
     CK(cudaEventRecord(c->t1, s), "event");
     int info = lnb_status_read(c, s);
     if (info < 0) return info;
