@@ -1,6 +1,6 @@
 // k_trsv_blk.cu -- triangular solves with an FP32 lower factor and few
 // right-hand sides (1..8), FP64 vectors and arithmetic, built on the inverses
-// of the factor's 512 x 512 diagonal blocks.
+// of the factor's HB x HB diagonal blocks (HB = 1024 from n = 8192, else 512).
 //
 // Semantics of the two blocked solves of dspdsolv_main (spdsolv_main.c:15,17,
 // bblas_dltrsm bblas_trsm.h:119-160): forward L y = b walks block rows top
@@ -9,7 +9,7 @@
 // blocks inverted beforehand every step is matrix-vector work:
 //
 //   * Work items are 64 KB slabs: 64 rows x 256 columns (forward) or 256 rows
-//     x 64 columns (backward) of a 512 x 512 block, 16 items per block, each
+//     x 64 columns (backward) of an HB x HB block (16 or 64 items per block), each
 //     brought into shared memory by ONE 2D TMA box issued before the item waits
 //     for its input vector.  An item multiplies its slab by a vector segment and
 //     adds the product into a target segment with FP64 atomics, then bumps a
@@ -17,16 +17,16 @@
 //     L_sj y_j or L_js^T x_j) or the solution counter of the step (diagonal
 //     items, with L_ss^-1 or L_ss^-T).
 //   * Items are handed out by an atomic ticket in a topological order that
-//     puts the chain first: step k holds the 16 diagonal items of block s, the
-//     16 items that feed the next block row, then the bulk of the column one
+//     puts the chain first: step k holds the diagonal items of block s, the
+//     items that feed the next block row, then the bulk of the column one
 //     step behind (its remaining rows).  Every item waits only on items of
 //     earlier steps or earlier in its own step, which running CTAs hold, so the
 //     walk cannot deadlock whatever the residency.  All waits are bounded and
 //     report a site code; a CTA that gives up drains its TMA load first.
-//   * The chain is nb = n/512 steps long (64 at n = 32768), against n/64 for a
+//   * The chain is nb = n/HB steps long (32 at n = 32768), against n/64 for a
 //     substitution with 64-wide blocks, and the bulk streams the factor once.
 //
-// The block inverses come from lnb_k_trtri512_f32 (this file): FP64
+// The block inverses come from lnb_k_trtri_hb_f32 (this file): FP64
 // arithmetic, FP32 storage, built column block by column block from the
 // 64 x 64 inverses of lnb_k_trtri_blocks_f32.
 #include <stdlib.h>
@@ -38,7 +38,6 @@
 namespace lnb {
 namespace blk {
 
-constexpr int HB = 512;               // diagonal block order
 constexpr int NTHR = 256;
 constexpr int SLAB = 64 * 256;        // floats per item slab (64 KB)
 constexpr int MAXR = 8;               // right-hand sides per launch
@@ -46,25 +45,26 @@ constexpr int MAXR = 8;               // right-hand sides per launch
 struct Args {
     int64_t n, np;          // order, padded order nb * HB
     int nb, nrhs, fwd, nitems;
+    int hb, ipb;            // diagonal block order HB, items per block (HB / 64) (HB / 256)
     double *R, *Y;          // np x nrhs each (ld np): residual right-hand side, solution
     int *ticket, *cntR, *cntY;
     lnb_status_t *st;
     long long wait_ns;
 };
 
-// items of step k: 16 diagonal, 16 next-row (k < nb-1), 16 per bulk row (k >= 1: nb-1-k rows)
-__host__ __device__ inline int64_t step_start(int64_t k, int64_t nb)
+// items of step k: ipb diagonal, ipb next-row (k < nb-1), ipb per bulk row (k >= 1: nb-1-k rows)
+__host__ __device__ inline int64_t step_start(int64_t k, int64_t nb, int64_t ipb)
 {
     const int64_t m = k < nb - 1 ? k : nb - 1;
     const int64_t bulk = k >= 1 ? (k - 1) * (nb - 1) - (k - 1) * k / 2 : 0;
-    return 16 * (k + m + bulk);
+    return ipb * (k + m + bulk);
 }
 
 struct Item {
     int kind;     // 0 diagonal, 1 update
     int row;      // target block row (residual for updates, solution for diagonal)
     int col;      // source block column (its solution segment is the input of an update)
-    int part;     // 0..15
+    int part;     // 0 .. ipb-1
 };
 
 LNB_DEV Item decode(int64_t t, const Args &a)
@@ -72,25 +72,25 @@ LNB_DEV Item decode(int64_t t, const Args &a)
     int lo = 0, hi = a.nb - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (step_start(mid, a.nb) <= t) lo = mid; else hi = mid - 1;
+        if (step_start(mid, a.nb, a.ipb) <= t) lo = mid; else hi = mid - 1;
     }
     const int k = lo;
-    int64_t r = t - step_start(k, a.nb);
+    int64_t r = t - step_start(k, a.nb, a.ipb);
     const int s = a.fwd ? k : a.nb - 1 - k;           // block solved at this step
     Item it;
-    it.part = (int)(r & 15);
-    if (r < 16) { it.kind = 0; it.row = s; it.col = s; return it; }
-    r -= 16;
+    it.part = (int)(r % a.ipb);
+    if (r < a.ipb) { it.kind = 0; it.row = s; it.col = s; return it; }
+    r -= a.ipb;
     it.kind = 1;
     if (k < a.nb - 1) {
-        if (r < 16) {                                 // the next block row's last update
+        if (r < a.ipb) {                              // the next block row's last update
             it.row = a.fwd ? s + 1 : s - 1;
             it.col = s;
             return it;
         }
-        r -= 16;
+        r -= a.ipb;
     }
-    const int off = (int)(r >> 4);                    // bulk of the column one step behind
+    const int off = (int)(r / a.ipb);                 // bulk of the column one step behind
     it.row = a.fwd ? s + 1 + off : s - 1 - off;
     it.col = a.fwd ? s - 1 : s + 1;
     return it;
@@ -130,18 +130,19 @@ __global__ void __launch_bounds__(NTHR, 2) k_trsm_blk(Args a, const __grid_const
         const int64_t t = s_t;
         if (t >= a.nitems) break;
         const Item it = decode(t, a);
-        const int p = it.part;
-        // source box and the vector / target segments of this item
-        //   forward : slab rows = 64 outputs (p & 7), columns = 256 inputs (p >> 3)
-        //   backward: slab rows = 256 inputs (p >> 3), columns = 64 outputs (p & 7)
-        const int64_t in0 = (int64_t)it.col * HB + 256 * (p >> 3);
-        const int64_t out0 = (int64_t)it.row * HB + 64 * (p & 7);
+        // source box and the vector / target segments of this item: 64-wide
+        // output slab po, 256-wide input slab pi
+        //   forward : slab rows = 64 outputs, columns = 256 inputs
+        //   backward: slab rows = 256 inputs, columns = 64 outputs
+        const int po = it.part % (a.hb / 64), pi = it.part / (a.hb / 64);
+        const int64_t in0 = (int64_t)it.col * a.hb + 256 * pi;
+        const int64_t out0 = (int64_t)it.row * a.hb + 64 * po;
         if (tid == 0) {
             tc::mbar_arrive_expect_tx(&full, SLAB * 4);
             if (it.kind == 0) {
-                // diagonal block s of the inverses: rows 0..511 of column block s
-                if (a.fwd) tc::tma_load_2d(slab, &mI, &full, 64 * (p & 7), it.row * HB + 256 * (p >> 3));
-                else tc::tma_load_2d(slab, &mI, &full, 256 * (p >> 3), it.row * HB + 64 * (p & 7));
+                // diagonal block s of the inverses: rows 0..HB-1 of column block s
+                if (a.fwd) tc::tma_load_2d(slab, &mI, &full, 64 * po, it.row * a.hb + 256 * pi);
+                else tc::tma_load_2d(slab, &mI, &full, 256 * pi, it.row * a.hb + 64 * po);
             } else {
                 // L_{row, col} (forward) or L_{col, row} (backward) of the factor
                 if (a.fwd) tc::tma_load_2d(slab, &mT, &full, (int)out0, (int)in0);
@@ -150,9 +151,9 @@ __global__ void __launch_bounds__(NTHR, 2) k_trsm_blk(Args a, const __grid_const
             // the input: a solution segment (updates) or a finished residual (diagonal)
             bool ok;
             if (it.kind == 1) {
-                ok = wait_geq(a.cntY + it.col, 16, a.wait_ns, a.st);
+                ok = wait_geq(a.cntY + it.col, a.ipb, a.wait_ns, a.st);
             } else {
-                const int need = 16 * (a.fwd ? it.row : a.nb - 1 - it.row);
+                const int need = a.ipb * (a.fwd ? it.row : a.nb - 1 - it.row);
                 ok = wait_geq(a.cntR + it.row, need, a.wait_ns, a.st);
             }
             if (!ok && atomicCAS(&a.st->timeout, 0, it.kind == 0 ? 41 : 42) == 0) a.st->timeout_item = (int)t;
@@ -250,7 +251,7 @@ __global__ void k_blk_unpack(const double *Y, int64_t n, int64_t np, double *B, 
         B[r + q * ldb] = Y[r + q * np];
 }
 
-// ---- the 512 x 512 diagonal-block inverses ----------------------------------
+// ---- the HB x HB diagonal-block inverses -------------------------------------
 // CTA (cb, s): column block cb (64 wide) of inv(L_ss), s = block index.  With
 // X_a the 64 x 64 block (a, cb) of the inverse and D_a the inverse of the 64 x
 // 64 diagonal block a:  X_cb = D_cb,  X_a = -D_a sum_{c=cb}^{a-1} L_ac X_c.
@@ -260,7 +261,8 @@ __global__ void k_blk_unpack(const double *Y, int64_t n, int64_t np, double *B, 
 constexpr int TLD = 68;
 constexpr int TRTRI_SMEM = 3 * 64 * TLD * 8;
 
-__global__ void __launch_bounds__(256) k_trtri512(const float *__restrict__ T, int64_t ldt, int64_t n,
+template <int HB>
+__global__ void __launch_bounds__(256) k_trtri_hb(const float *__restrict__ T, int64_t ldt, int64_t n,
                                                   const float *__restrict__ dinv64, float *Binv)
 {
     extern __shared__ __align__(16) double tsm[];
@@ -278,7 +280,7 @@ __global__ void __launch_bounds__(256) k_trtri512(const float *__restrict__ T, i
             const int c = i >> 6, r = i & 63;
             Xb[(64 * a + r) + (int64_t)(64 * cb + c) * HB] = 0.f;
         }
-    for (int a = cb; a < 8; ++a) {
+    for (int a = cb; a < HB / 64; ++a) {
         const int64_t q64 = (o + 64 * a) / 64;      // global 64-block index of diagonal block a
         double acc[4][4];
 #pragma unroll
@@ -387,39 +389,50 @@ static int launch(const Args &a, const CUtensorMap &mT, const CUtensorMap &mI, i
 }  // namespace blk
 }  // namespace lnb
 
+// diagonal block order of the block solve: 1024 from n = 8192 (half the
+// chain steps; the inverses cost twice the work), 512 below
+static inline int64_t hb_of(int64_t n) { return n >= 8192 ? 1024 : 512; }
+
 extern "C" int64_t lnb_trsm_blk_ints(int64_t n)
 {
-    const int64_t nb = (n + lnb::blk::HB - 1) / lnb::blk::HB;
+    const int64_t nb = (n + hb_of(n) - 1) / hb_of(n);
     return 32 + 2 * nb;
 }
 extern "C" int64_t lnb_trsm_blk_inv_floats(int64_t n)
 {
-    const int64_t nb = (n + lnb::blk::HB - 1) / lnb::blk::HB;
-    return nb * lnb::blk::HB * lnb::blk::HB;
+    const int64_t hb = hb_of(n), nb = (n + hb - 1) / hb;
+    return nb * hb * hb;
 }
 extern "C" int64_t lnb_trsm_blk_vec_doubles(int64_t n, int64_t nrhs)
 {
-    const int64_t nb = (n + lnb::blk::HB - 1) / lnb::blk::HB;
-    return 2 * nb * lnb::blk::HB * nrhs;
+    const int64_t hb = hb_of(n), nb = (n + hb - 1) / hb;
+    return 2 * nb * hb * nrhs;
 }
 // the block solve applies: FP32 T 16-byte aligned with ld a multiple of 4, 1..8 right-hand sides
 extern "C" int lnb_trsm_blk_ok(const float *T, int64_t ldt, int64_t n, int64_t nrhs)
 {
     const char *e = getenv("LNB_TRSM_BLK");    /* 0: substitution with 64-wide blocks instead */
     if (e && *e && atoi(e) == 0) return 0;
-    return n >= 2 * lnb::blk::HB && nrhs >= 1 && nrhs <= lnb::blk::MAXR && (uintptr_t)T % 16 == 0 && ldt % 4 == 0;
+    return n >= 1024 && nrhs >= 1 && nrhs <= lnb::blk::MAXR && (uintptr_t)T % 16 == 0 && ldt % 4 == 0;
 }
 
 // Binv: lnb_trsm_blk_inv_floats(n); dinv64: lnb_k_trtri_blocks_f32's 64 x 64 inverses of T
-extern "C" int lnb_k_trtri512_f32(const float *T, int64_t ldt, int64_t n, const float *dinv64, float *Binv,
+extern "C" int lnb_k_trtri_hb_f32(const float *T, int64_t ldt, int64_t n, const float *dinv64, float *Binv,
                                   lnb_stream_t s)
 {
     using namespace lnb::blk;
     if (n <= 0) return 0;
-    const int64_t nb = (n + HB - 1) / HB;
-    cudaError_t e = cudaFuncSetAttribute(k_trtri512, cudaFuncAttributeMaxDynamicSharedMemorySize, TRTRI_SMEM);
-    if (e != cudaSuccess) return (int)e;
-    k_trtri512<<<dim3(8, (unsigned)nb), 256, TRTRI_SMEM, (cudaStream_t)s>>>(T, ldt, n, dinv64, Binv);
+    const int64_t hb = hb_of(n), nb = (n + hb - 1) / hb;
+    cudaError_t e;
+    if (hb == 1024) {
+        e = cudaFuncSetAttribute(k_trtri_hb<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRTRI_SMEM);
+        if (e != cudaSuccess) return (int)e;
+        k_trtri_hb<1024><<<dim3(16, (unsigned)nb), 256, TRTRI_SMEM, (cudaStream_t)s>>>(T, ldt, n, dinv64, Binv);
+    } else {
+        e = cudaFuncSetAttribute(k_trtri_hb<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRTRI_SMEM);
+        if (e != cudaSuccess) return (int)e;
+        k_trtri_hb<512><<<dim3(8, (unsigned)nb), 256, TRTRI_SMEM, (cudaStream_t)s>>>(T, ldt, n, dinv64, Binv);
+    }
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }
@@ -436,11 +449,13 @@ extern "C" int lnb_k_trsm_blk_f32(char trans, int64_t n, int64_t nrhs, const flo
     if (nrhs > MAXR) return (int)cudaErrorInvalidValue;
     Args a;
     a.n = n;
-    a.nb = (int)((n + HB - 1) / HB);
-    a.np = (int64_t)a.nb * HB;
+    a.hb = (int)hb_of(n);
+    a.ipb = (a.hb / 64) * (a.hb / 256);
+    a.nb = (int)((n + a.hb - 1) / a.hb);
+    a.np = (int64_t)a.nb * a.hb;
     a.nrhs = (int)nrhs;
     a.fwd = trans == 'N';
-    a.nitems = (int)step_start(a.nb, a.nb);
+    a.nitems = (int)step_start(a.nb, a.nb, a.ipb);
     a.R = vec;
     a.Y = vec + a.np * nrhs;
     a.ticket = sync;
@@ -453,7 +468,8 @@ extern "C" int lnb_k_trsm_blk_f32(char trans, int64_t n, int64_t nrhs, const flo
     memset(&mI, 0, sizeof mI);
     // forward items read 64 x 256 boxes, backward 256 x 64
     const int bx = a.fwd ? 64 : 256, by = a.fwd ? 256 : 64;
-    if (map2d(&mT, T, n, n, ldt, bx, by) || map2d(&mI, Binv, HB, a.np, HB, bx, by)) return (int)cudaErrorInvalidValue;
+    if (map2d(&mT, T, n, n, ldt, bx, by) || map2d(&mI, Binv, a.hb, a.np, a.hb, bx, by))
+        return (int)cudaErrorInvalidValue;
     cudaStream_t cs = (cudaStream_t)s;
     cudaError_t e = cudaMemsetAsync(sync, 0, (size_t)lnb_trsm_blk_ints(n) * sizeof(int), cs);
     if (e != cudaSuccess) return (int)e;

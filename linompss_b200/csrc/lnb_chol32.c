@@ -214,7 +214,7 @@ int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode,
         const int64_t mrem = n - k0 - bs;
         const int slot = k & 1;
         { int _e = lnb_potrf_tile_f32(Akk, lda, bs, k0, dinv, c->st, crit); if (_e) return _e; }
-        if (rf) {
+        if (rf && rf->check) {
             /* the refinement driver wants a usable factor: check this tile now */
             int info = lnb_status_read(c, crit);
             if (info < 0) return info;
@@ -356,6 +356,7 @@ int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, in
     if (!u) return lnb_set_error(LNB_ENOMEM, "streamed factor: host memory");
     cudaStream_t crit = c->crit;
     cudaEvent_t ev_start = c->ev[0], ev_trsm = c->ev[1], ev_next = c->ev[2], ev_done = c->ev[3];
+    cudaEvent_t ev_pace = c->ev[4];
     int e = 0;
 #define RUN(x)                   \
     do {                         \
@@ -376,10 +377,16 @@ int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, in
         float *Akk = dA + k0 + k0 * lda;
         const int64_t mrem = n - k0 - bs;
         RUN(lnb_potrf_tile_f32(Akk, lda, bs, k0, dinv, c->st, crit));
-        if (rf) {
+        if (rf && rf->check) {
             const int info = lnb_status_read(c, crit);
             if (info < 0) { e = info; goto out; }
             if (info > 0) RUN(refactor_tile(c, rf, dA, lda, k0, bs, b, dinv, ar, crit));
+        } else if (in) {
+            /* keep the host within a step of the device, so the arrival checks
+             * below see what has landed, without stalling this step: wait for
+             * the previous step's diagonal factor, then queue this step */
+            if (k > 0) RUN(ck_cuda(cudaEventSynchronize(ev_pace), "pace"));
+            RUN(ck_cuda(cudaEventRecord(ev_pace, crit), "event"));
         }
         if (mrem <= 0) break;
         float *hk = HA + (k0 + bs) * ldk + k0, *lk = LA ? LA + (k0 + bs) * ldk + k0 : NULL;
@@ -544,7 +551,7 @@ int64_t lnb_trsm_blk_ints(int64_t n);
 int64_t lnb_trsm_blk_inv_floats(int64_t n);
 int64_t lnb_trsm_blk_vec_doubles(int64_t n, int64_t nrhs);
 int lnb_trsm_blk_ok(const float *T, int64_t ldt, int64_t n, int64_t nrhs);
-int lnb_k_trtri512_f32(const float *T, int64_t ldt, int64_t n, const float *dinv64, float *Binv, lnb_stream_t s);
+int lnb_k_trtri_hb_f32(const float *T, int64_t ldt, int64_t n, const float *dinv64, float *Binv, lnb_stream_t s);
 int lnb_k_trsm_blk_f32(char trans, int64_t n, int64_t nrhs, const float *T, int64_t ldt, const float *Binv, double *B,
                        int64_t ldb, double *vec, int *sync, lnb_status_t *st, long long wait_ns, int sms,
                        lnb_stream_t s);
@@ -560,12 +567,12 @@ static int spotrs_run(lnb_ctx *c, int64_t n, int64_t nrhs, const float *dL, int6
     CK(lnb_k_trtri_blocks_f32(dL, lda, n, TRSV_H, 'L', 0, dinv, s), "trtri");
     CK(lnb_k_f32_to_f64(dB, ldb, n, nrhs, Z, n, s), "widen");
     if (lnb_trsm_blk_ok(dL, lda, n, nrhs)) {
-        /* few right-hand sides: the solves on the 512 x 512 diagonal-block inverses */
+        /* few right-hand sides: the solves on the inverses of the large diagonal blocks */
         float *binv = lnb_arena_take(ar, (size_t)lnb_trsm_blk_inv_floats(n) * 4);
         double *vec = lnb_arena_take(ar, (size_t)lnb_trsm_blk_vec_doubles(n, nrhs) * 8);
         int *bsync = lnb_arena_take(ar, (size_t)lnb_trsm_blk_ints(n) * 4);
         if (!bsync) return lnb_set_error(LNB_ENOMEM, "spotrs workspace");
-        CK(lnb_k_trtri512_f32(dL, lda, n, dinv, binv, s), "trtri 512");
+        CK(lnb_k_trtri_hb_f32(dL, lda, n, dinv, binv, s), "block inverses");
         if (which == 'N' || which == 'B')
             CK(lnb_k_trsm_blk_f32('N', n, nrhs, dL, lda, binv, Z, n, vec, bsync, c->st, lnb_wait_ns(), c->sms, s),
                "forward");

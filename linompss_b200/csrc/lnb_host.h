@@ -88,6 +88,10 @@ typedef struct {
     int64_t lda;
     const double *S;
     int refactored, shifted;
+    /* 1: read the status after every diagonal tile and refactor a failed one
+     * at once (a host round trip per step); 0: no per-step reads -- the caller
+     * checks the final status and reruns with 1 if a pivot failed */
+    int check;
 } lnb_refactor_ctx;
 size_t lnb_refactor_ws_bytes(int b);
 int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_refactor_ctx *rf,

@@ -38,7 +38,7 @@ int64_t lnb_trsm_blk_ints(int64_t n);
 int64_t lnb_trsm_blk_inv_floats(int64_t n);
 int64_t lnb_trsm_blk_vec_doubles(int64_t n, int64_t nrhs);
 int lnb_trsm_blk_ok(const float *T, int64_t ldt, int64_t n, int64_t nrhs);
-int lnb_k_trtri512_f32(const float *T, int64_t ldt, int64_t n, const float *dinv64, float *Binv, lnb_stream_t s);
+int lnb_k_trtri_hb_f32(const float *T, int64_t ldt, int64_t n, const float *dinv64, float *Binv, lnb_stream_t s);
 int lnb_k_trsm_blk_f32(char trans, int64_t n, int64_t nrhs, const float *T, int64_t ldt, const float *Binv, double *B,
                        int64_t ldb, double *vec, int *sync, lnb_status_t *st, long long wait_ns, int sms,
                        lnb_stream_t s);
@@ -64,7 +64,7 @@ typedef struct {
     float *A32;
     double *S, *dinv, *R, *Z, *Y, *P, *Q, *ones, *scal; /* scal: 8 * nrhs scalars */
     int *sync;
-    /* solves on the 512 x 512 diagonal-block inverses (k_trsv_blk.cu), when they apply */
+    /* solves on the inverses of the large diagonal blocks (k_trsv_blk.cu), when they apply */
     float *binv;
     double *bvec;
     int *bsync;
@@ -211,7 +211,13 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
 
     /* ---- factor ---- */
     CK(cudaEventRecord(c->t0, s), "event");
-    lnb_refactor_ctx rf = {dA, lda, w.S, 0, 0};
+    /* First pass without per-step status reads: the host queues the steps
+     * while the device runs them.  A low-precision pivot that is not positive
+     * shows in the final status; then the factor is rebuilt from the FP64 A on
+     * the checking path, which refactors that tile in FP64 (rare: only very
+     * ill-conditioned tiles fail). */
+    lnb_refactor_ctx rf = {dA, lda, w.S, 0, 0, 0};
+    const lnb_arena ar_factor = ar;   /* a rerun carves the same workspace again */
     int e;
     if (in) {
         /* the matrix is converted block column by block column as it arrives */
@@ -227,13 +233,32 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
         else
             e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &rf, &ar, s);
     }
+    if (!e) {
+        const int info0 = lnb_status_read(c, s);
+        if (info0 < 0) return info0;
+        if (info0 > 0) {
+            if (in) {
+                /* every block column of A has landed before it is read again */
+                const int nblk = (n + b - 1) / b;
+                for (int j = 0; j < nblk; ++j) CK(cudaStreamWaitEvent(s, in->arr[j], 0), "arrival wait");
+            }
+            rf.check = 1;
+            ar = ar_factor;
+            CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
+            CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, s), "convert");
+            if (lnb_chol_f32_stream_ok(n, b, mode))
+                e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, NULL, &ar, s);
+            else
+                e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &rf, &ar, s);
+        }
+    }
     rr.refactored_tiles = rf.refactored;
     if (e) {
         if (e > 0 && res) { rr.info = e; *res = rr; }
         return e > 0 ? lnb_set_error(e, "low-precision factor: tile at row %d could not be refactored", e) : e;
     }
     CK(lnb_k_trtri_blocks_f32(w.A32, w.ld32, n, TRSV_H, 'L', 0, (float *)w.dinv, s), "trtri");
-    if (w.binv) CK(lnb_k_trtri512_f32(w.A32, w.ld32, n, (const float *)w.dinv, w.binv, s), "trtri 512");
+    if (w.binv) CK(lnb_k_trtri_hb_f32(w.A32, w.ld32, n, (const float *)w.dinv, w.binv, s), "block inverses");
     CK(cudaEventRecord(c->t1, s), "event");
     int info = lnb_status_read(c, s);
     if (info < 0) return info;
