@@ -1,6 +1,6 @@
 // k_trsv_blk.cu -- triangular solves with an FP32 lower factor and few
 // right-hand sides (1..8), FP64 vectors and arithmetic, built on the inverses
-// of the factor's HB x HB diagonal blocks (HB = 1024 from n = 8192, else 512).
+// of the factor's HB x HB diagonal blocks (HB = 512).
 //
 // Semantics of the two blocked solves of dspdsolv_main (spdsolv_main.c:15,17,
 // bblas_dltrsm bblas_trsm.h:119-160): forward L y = b walks block rows top
@@ -9,7 +9,7 @@
 // blocks inverted beforehand every step is matrix-vector work:
 //
 //   * Work items are 64 KB slabs: 64 rows x 256 columns (forward) or 256 rows
-//     x 64 columns (backward) of an HB x HB block (16 or 64 items per block), each
+//     x 64 columns (backward) of an HB x HB block (16 items per block), each
 //     brought into shared memory by ONE 2D TMA box issued before the item waits
 //     for its input vector.  An item multiplies its slab by a vector segment and
 //     adds the product into a target segment with FP64 atomics, then bumps a
@@ -23,7 +23,7 @@
 //     earlier steps or earlier in its own step, which running CTAs hold, so the
 //     walk cannot deadlock whatever the residency.  All waits are bounded and
 //     report a site code; a CTA that gives up drains its TMA load first.
-//   * The chain is nb = n/HB steps long (32 at n = 32768), against n/64 for a
+//   * The chain is nb = n/HB steps long (64 at n = 32768), against n/64 for a
 //     substitution with 64-wide blocks, and the bulk streams the factor once.
 //
 // The block inverses come from lnb_k_trtri_hb_f32 (this file): FP64
@@ -389,9 +389,10 @@ static int launch(const Args &a, const CUtensorMap &mT, const CUtensorMap &mI, i
 }  // namespace blk
 }  // namespace lnb
 
-// diagonal block order of the block solve: 1024 from n = 8192 (half the
-// chain steps; the inverses cost twice the work), 512 below
-static inline int64_t hb_of(int64_t n) { return n >= 8192 ? 1024 : 512; }
+// diagonal block order of the block solve.  512: with 1024 the chain halves
+// but the solve was measured only 5 % faster (its bulk streaming, not the
+// chain, sets the time) while the inverses cost 4x the time.
+static inline int64_t hb_of(int64_t n) { (void)n; return 512; }
 
 extern "C" int64_t lnb_trsm_blk_ints(int64_t n)
 {
@@ -423,16 +424,10 @@ extern "C" int lnb_k_trtri_hb_f32(const float *T, int64_t ldt, int64_t n, const 
     using namespace lnb::blk;
     if (n <= 0) return 0;
     const int64_t hb = hb_of(n), nb = (n + hb - 1) / hb;
-    cudaError_t e;
-    if (hb == 1024) {
-        e = cudaFuncSetAttribute(k_trtri_hb<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRTRI_SMEM);
-        if (e != cudaSuccess) return (int)e;
-        k_trtri_hb<1024><<<dim3(16, (unsigned)nb), 256, TRTRI_SMEM, (cudaStream_t)s>>>(T, ldt, n, dinv64, Binv);
-    } else {
-        e = cudaFuncSetAttribute(k_trtri_hb<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRTRI_SMEM);
-        if (e != cudaSuccess) return (int)e;
-        k_trtri_hb<512><<<dim3(8, (unsigned)nb), 256, TRTRI_SMEM, (cudaStream_t)s>>>(T, ldt, n, dinv64, Binv);
-    }
+    cudaError_t e = cudaFuncSetAttribute(k_trtri_hb<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, TRTRI_SMEM);
+    if (e != cudaSuccess) return (int)e;
+    k_trtri_hb<512><<<dim3((unsigned)(hb / 64), (unsigned)nb), 256, TRTRI_SMEM, (cudaStream_t)s>>>(T, ldt, n, dinv64,
+                                                                                                  Binv);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }

@@ -125,8 +125,8 @@ def test_schol_not_spd(lnb, mode, n, b, bad):
 def test_spotrs_chain_matches_fp64_solve(lnb, cuda, n, nrhs):
     """FP32-stored factor, FP64 right-hand sides and arithmetic: the solve
     equals an FP64 triangular solve with the same (FP32-valued) factor.  From
-    n = 1024 the solve runs on the inverses of 512-wide diagonal blocks, from
-    n = 8192 of 1024-wide ones (9000: a ragged last block)."""
+    n = 1024 the solve runs on the inverses of 512-wide diagonal blocks (9000:
+    a ragged last block)."""
     import torch
     rng = np.random.default_rng(n + nrhs)
     L = np.tril(rng.uniform(-1, 1, (n, n)) / np.sqrt(n)).astype(np.float32)
