@@ -27,8 +27,6 @@
 
 namespace lnb {
 
-constexpr int BMAXR = 8;
-
 struct BatchArgs {
     int count;
     const int *n, *nrhs;
@@ -58,97 +56,6 @@ struct BSmem {
     static constexpr size_t RED = sizeof(double) * (NT / 32) * BP * BMAXR;
     static constexpr size_t total = P + LI + RD + CS + XS + RS + RED;
 };
-
-// z <- inv(L) z, then z <- inv(L^T) z, for nr columns of z in shared memory
-// (z[q * BMAXN + i]); L in F, the block inverses in Dv.
-template <typename TF, int NT>
-__device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double *z, double *red)
-{
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int NW = NT / 32;
-    static_assert(BMAXR <= NW, "one warp per right-hand side in the block-inverse steps");
-    const int nblk = (n + BP - 1) / BP;
-    // forward
-    for (int kb = 0; kb < nblk; ++kb) {
-        const int k0 = kb * BP, kn = min(BP, n - k0);
-        if (k0 > 0) {
-            double acc[BMAXR];
-#pragma unroll
-            for (int q = 0; q < BMAXR; ++q) acc[q] = 0.0;
-            if (lane < kn) {
-#pragma unroll 4
-                for (int c = warp; c < k0; c += NW) {
-                    const double f = (double)__ldcg(F + (k0 + lane) + (int64_t)c * ldF);
-#pragma unroll
-                    for (int q = 0; q < BMAXR; ++q)
-                        if (q < nr) acc[q] = fma(f, z[q * BMAXN + c], acc[q]);
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < BMAXR; ++q) red[(q * NW + warp) * BP + lane] = acc[q];   // lanes contiguous
-            __syncthreads();
-            for (int t = tid; t < kn * nr; t += NT) {
-                const int q = t / kn, i = t - q * kn;
-                double s = 0.0;
-                for (int w = 0; w < NW; ++w) s += red[(q * NW + w) * BP + i];
-                z[q * BMAXN + k0 + i] -= s;
-            }
-            __syncthreads();
-        }
-        // z_blk = inv(L_kk) z_blk: thread (j, q), j = row of the block, q = rhs
-        const TF *Dk = Dv + (int64_t)kb * BP * BP;
-        const int j = tid & 31, q = tid >> 5;
-        const bool act = j < kn && q < nr;
-        double v = 0.0;
-        if (act)
-            for (int p = 0; p <= j; ++p) v = fma((double)__ldcg(Dk + j + BP * p), z[q * BMAXN + k0 + p], v);
-        __syncthreads();
-        if (act) z[q * BMAXN + k0 + j] = v;
-        __syncthreads();
-    }
-    // backward
-    for (int kb = nblk - 1; kb >= 0; --kb) {
-        const int k0 = kb * BP, kn = min(BP, n - k0), r0 = k0 + kn;
-        if (r0 < n) {
-            for (int jc = warp; jc < kn; jc += NW) {
-                double acc[BMAXR];
-#pragma unroll
-                for (int q = 0; q < BMAXR; ++q) acc[q] = 0.0;
-                const TF *col = F + (int64_t)(k0 + jc) * ldF;
-#pragma unroll 4
-                for (int r = r0 + lane; r < n; r += 32) {
-                    const double f = (double)__ldcg(col + r);
-#pragma unroll
-                    for (int q = 0; q < BMAXR; ++q)
-                        if (q < nr) acc[q] = fma(f, z[q * BMAXN + r], acc[q]);
-                }
-#pragma unroll
-                for (int q = 0; q < BMAXR; ++q) {
-                    double v = acc[q];
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-                    if (lane == 0) red[q * BP + jc] = v;
-                }
-            }
-            __syncthreads();
-            for (int t = tid; t < kn * nr; t += NT) {
-                const int q = t / kn, i = t - q * kn;
-                z[q * BMAXN + k0 + i] -= red[q * BP + i];
-            }
-            __syncthreads();
-        }
-        // z_blk = inv(L_kk)^T z_blk
-        const TF *Dk = Dv + (int64_t)kb * BP * BP;
-        const int j = tid & 31, q = tid >> 5;
-        const bool act = j < kn && q < nr;
-        double v = 0.0;
-        if (act)
-            for (int p = j; p < kn; ++p) v = fma((double)__ldcg(Dk + p + BP * j), z[q * BMAXN + k0 + p], v);
-        __syncthreads();
-        if (act) z[q * BMAXN + k0 + j] = v;
-        __syncthreads();
-    }
-}
 
 // r = b - A x (A full symmetric n x n, FP64) for nr columns; returns the max
 // over columns of ||r||_inf / (anorm ||x||_inf + ||b||_inf), same in every thread

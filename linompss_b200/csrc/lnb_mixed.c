@@ -211,12 +211,14 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
 
     /* ---- factor ---- */
     CK(cudaEventRecord(c->t0, s), "event");
-    /* First pass without per-step status reads: the host queues the steps
-     * while the device runs them.  A low-precision pivot that is not positive
-     * shows in the final status; then the factor is rebuilt from the FP64 A on
-     * the checking path, which refactors that tile in FP64 (rare: only very
-     * ill-conditioned tiles fail). */
-    lnb_refactor_ctx rf = {dA, lda, w.S, 0, 0, 0};
+    /* TF32 and FP32 factors: a first pass without per-step status reads (the
+     * host queues the steps while the device runs them); a pivot that is not
+     * positive shows in the final status, and the factor is then rebuilt from
+     * the FP64 A on the checking path, which refactors that tile in FP64.
+     * BF16 factors of ill-conditioned matrices fail often enough that the
+     * rebuild would cost more than the per-step reads, so they check every
+     * diagonal tile at once. */
+    lnb_refactor_ctx rf = {dA, lda, w.S, 0, 0, mode == LNB_FACTOR_BF16};
     const lnb_arena ar_factor = ar;   /* a rerun carves the same workspace again */
     int e;
     if (in) {
@@ -233,7 +235,7 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
         else
             e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &rf, &ar, s);
     }
-    if (!e) {
+    if (!e && !rf.check) {
         const int info0 = lnb_status_read(c, s);
         if (info0 < 0) return info0;
         if (info0 > 0) {

@@ -421,6 +421,167 @@ int orc_ditref(int64_t n, int64_t bm, const double *A, const double *rhs, double
 }
 
 /* ------------------------------------------------------------------------ */
+/* Sparse refinement (itref.c built with USE_SPARSE)                           */
+/* ------------------------------------------------------------------------ */
+/* CSR matrices as hbmat_t holds them (hb.h:27-59): row pointers vptr[n+1],
+ * column indices vpos and values vval, zero- or one-based (base = vptr[0],
+ * the offset one2zero removes, itref_config.c:228-241). */
+
+/* y = alpha A x + beta y.  The reference calls SBLAS_csrmv (bsblas_csrmm.h:
+ * 214-232, one task per row block) which is MKL's mkl_dcsrmv with the
+ * descriptor "GLNC" (general, zero-based): each row's products summed in
+ * storage order, then scaled. */
+void orc_csrmv(int64_t n, int base, const int *vptr, const int *vpos, const double *vval, const double *x,
+               double alpha, double beta, double *y)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (int64_t p = vptr[i] - base; p < vptr[i + 1] - base; ++p) s += vval[p] * x[vpos[p] - base];
+        y[i] = (beta == 0.0 ? 0.0 : beta * y[i]) + alpha * s;
+    }
+}
+
+/* Block-Jacobi preconditioner of itref_setup.c:55-93: the complete bm x bm
+ * diagonal blocks of A (hb_sym_diag_block, hb.c:512-560), each factored by
+ * Cholesky with natural ordering (cs_schol(A, 0) then cs_chol).  F holds
+ * block k (order bk <= bm) dense at F + k bm bm, column-major with ld bm,
+ * L in its lower part.  Returns 0, or 1 + the first block that is not
+ * positive definite. */
+int orc_bj_setup(int64_t n, int64_t bm, int base, const int *vptr, const int *vpos, const double *vval, double *F)
+{
+    const int64_t nblk = (n + bm - 1) / bm;
+    for (int64_t k = 0; k < nblk; ++k) {
+        const int64_t r0 = k * bm, bk = min64(bm, n - r0);
+        double *D = F + k * bm * bm;
+        for (int64_t i = 0; i < bm * bm; ++i) D[i] = 0.0;
+        for (int64_t r = r0; r < r0 + bk; ++r)
+            for (int64_t p = vptr[r] - base; p < vptr[r + 1] - base; ++p) {
+                const int64_t c = vpos[p] - base;
+                if (c >= r0 && c < r0 + bk) D[(r - r0) + (c - r0) * bm] += vval[p];
+            }
+        for (int64_t j = 0; j < bk; ++j) {
+            double d = D[j + j * bm];
+            for (int64_t q = 0; q < j; ++q) d -= D[j + q * bm] * D[j + q * bm];
+            if (!(d > 0.0)) return (int)(1 + k);
+            d = sqrt(d);
+            D[j + j * bm] = d;
+            for (int64_t i = j + 1; i < bk; ++i) {
+                double v = D[i + j * bm];
+                for (int64_t q = 0; q < j; ++q) v -= D[i + q * bm] * D[j + q * bm];
+                D[i + j * bm] = v / d;
+            }
+        }
+    }
+    return 0;
+}
+
+/* z = M^-1 r block by block: L L^T z_k = r_k (bsblas_dcholsolv2,
+ * bsblas_csrmm.h:498-513, and cs_cholsol2 with the identity permutation) */
+void orc_bj_apply(int64_t n, int64_t bm, const double *F, const double *r, double *z)
+{
+    const int64_t nblk = (n + bm - 1) / bm;
+    for (int64_t k = 0; k < nblk; ++k) {
+        const int64_t r0 = k * bm, bk = min64(bm, n - r0);
+        const double *L = F + k * bm * bm;
+        double *x = z + r0;
+        for (int64_t i = 0; i < bk; ++i) x[i] = r[r0 + i];
+        for (int64_t j = 0; j < bk; ++j) {           /* cs_lsolve: column-oriented */
+            x[j] /= L[j + j * bm];
+            for (int64_t i = j + 1; i < bk; ++i) x[i] -= L[i + j * bm] * x[j];
+        }
+        for (int64_t j = bk - 1; j >= 0; --j) {      /* cs_ltsolve */
+            for (int64_t i = j + 1; i < bk; ++i) x[j] -= L[i + j * bm] * x[i];
+            x[j] /= L[j + j * bm];
+        }
+    }
+}
+
+/* dcg_pure with the sparse matrix (itref.c:690-925, USE_SPARSE, s = 1,
+ * synchronous branch), F = NULL for the unpreconditioned form.  The
+ * recurrence as the reference executes it (every vector in slot 0, see
+ * orc_dcg): with the preconditioner alpha1 = <r, z>, the direction update
+ * is p = z then p += p (p = 2 z), and the relative test uses sqrt(alpha1). */
+int orc_dscg(int64_t n, int64_t bm, int base, const int *vptr, const int *vpos, const double *vval,
+             const double *F, const double *b, double *x, double tol, int steps, double *res_log)
+{
+    double *r = malloc(sizeof(double) * n), *p = malloc(sizeof(double) * n);
+    double *tmp = malloc(sizeof(double) * n), *z = malloc(sizeof(double) * n);
+    const double norm_b = sqrt(dot(n, n, b, b));
+    memcpy(r, b, sizeof(double) * n);
+    orc_csrmv(n, base, vptr, vpos, vval, x, -1.0, 1.0, r);     /* r = b - A x */
+    double alpha1;
+    if (F) {
+        orc_bj_apply(n, bm, F, r, z);                            /* z = M^-1 r */
+        memcpy(p, z, sizeof(double) * n);
+        alpha1 = dot(n, bm, r, z);
+    } else {
+        memcpy(p, r, sizeof(double) * n);
+        alpha1 = dot(n, bm, r, r);
+    }
+    int converged = 0, k;
+    for (k = 0; k < steps; ++k) {
+        orc_csrmv(n, base, vptr, vpos, vval, p, 1.0, 0.0, tmp);  /* tmp = A p (bsblas_dcg_comb) */
+        const double alpha2 = dot(n, bm, p, tmp);
+        const double f = alpha1 / alpha2;
+        for (int64_t i = 0; i < n; ++i) {
+            x[i] = x[i] + f * p[i];
+            r[i] = r[i] + (-1.0 * f) * tmp[i];
+        }
+        const double *y = r;
+        if (F) {
+            orc_bj_apply(n, bm, F, r, z);
+            alpha1 = dot(n, bm, r, z);
+            y = z;
+        } else {
+            alpha1 = dot(n, bm, r, r);
+        }
+        const double beta = alpha1 / alpha1;
+        for (int64_t i = 0; i < n; ++i) {
+            p[i] = y[i];
+            p[i] = p[i] + beta * p[i];
+        }
+        const double sr2norm = sqrt(alpha1) / norm_b;
+        if (res_log) res_log[k] = sr2norm;
+        if (sr2norm <= tol) { converged = 1; break; }
+    }
+    free(r); free(p); free(tmp); free(z);
+    return converged ? -1 : k;
+}
+
+/* The refinement loop of itref.c:999-1101 with the sparse matrix: the same
+ * steps as orc_ditref, the residual by the CSR product. */
+int orc_dsitref(int64_t n, int64_t bm, int base, const int *vptr, const int *vpos, const double *vval,
+                const double *F, const double *rhs, double *x, double prec, int refit, int it, double *norms)
+{
+    double *xs[2], *rs[2], *sd[2];
+    double *buf = calloc((size_t)6 * n, sizeof(double));
+    xs[0] = buf; xs[1] = buf + n; rs[0] = buf + 2 * n; rs[1] = buf + 3 * n;
+    sd[0] = buf + 4 * n; sd[1] = buf + 5 * n;
+    double r2norm[2] = {0.0, DBL_MAX};
+    orc_dscg(n, bm, base, vptr, vpos, vval, F, rhs, sd[1], prec, it, NULL);
+    memcpy(xs[1], sd[1], sizeof(double) * n);
+    memcpy(rs[1], rhs, sizeof(double) * n);
+    orc_csrmv(n, base, vptr, vpos, vval, xs[1], -1.0, 1.0, rs[1]);
+    int prevb = 1, i;
+    for (i = 0; i < refit; ++i) {
+        const int b = i & 1;
+        memset(sd[b], 0, sizeof(double) * n);
+        orc_dscg(n, bm, base, vptr, vpos, vval, F, rs[prevb], sd[b], prec, it, NULL);
+        const double sr2norm = sqrt(r2norm[prevb]);
+        if (norms) norms[i] = sr2norm;
+        if (sr2norm <= prec) { ++i; break; }
+        for (int64_t q = 0; q < n; ++q) xs[b][q] = xs[prevb][q] + 1.0 * sd[b][q];
+        memcpy(rs[b], rhs, sizeof(double) * n);
+        orc_csrmv(n, base, vptr, vpos, vval, xs[b], -1.0, 1.0, rs[b]);
+        r2norm[b] = dot(n, bm, rs[b], rs[b]);
+        prevb = b;
+    }
+    memcpy(x, xs[prevb], sizeof(double) * n);
+    free(buf);
+    return i;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Quality measures                                                           */
 /* ------------------------------------------------------------------------ */
 double orc_chol_residual(int64_t n, const double *A0, int64_t lda0, const double *L, int64_t ldl)

@@ -94,6 +94,18 @@ double orc_chol_residual(int64_t n, const double *A0, int64_t lda0, const double
 double orc_backward_error(int64_t n, int64_t nrhs, const double *A, int64_t lda,
                           const double *X, int64_t ldx, const double *B, int64_t ldb);
 
+/* ---- sparse refinement (itref.c, USE_SPARSE): CSR with base = vptr[0] ---- */
+void orc_csrmv(int64_t n, int base, const int *vptr, const int *vpos, const double *vval, const double *x,
+               double alpha, double beta, double *y);
+/* block-Jacobi factors: F[k bm bm ...] = chol of diagonal block k (ld bm); 0 or 1 + failed block */
+int orc_bj_setup(int64_t n, int64_t bm, int base, const int *vptr, const int *vpos, const double *vval, double *F);
+void orc_bj_apply(int64_t n, int64_t bm, const double *F, const double *r, double *z);
+/* dcg_pure with the CSR matrix (F = NULL: no preconditioner) */
+int orc_dscg(int64_t n, int64_t bm, int base, const int *vptr, const int *vpos, const double *vval,
+             const double *F, const double *b, double *x, double tol, int steps, double *res_log);
+int orc_dsitref(int64_t n, int64_t bm, int base, const int *vptr, const int *vpos, const double *vval,
+                const double *F, const double *rhs, double *x, double prec, int refit, int it, double *norms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,7 +35,7 @@ DBL := itref/itref.c itref/itref_config.c itref/itref_setup.c fp/fptype.c \
        blocked_blas/task_dot_async.c blocked_blas/task_gemv.c util/as_man.c util/async_struct.c \
        util/task_log.c util/prof.c util/file_log.c util/strutil.c util/ompss_apps.c \
        util/ompss_options.c matutil/matfprint.c matutil/matfread.c matutil/genmat.c \
-       matutil/genmat_config.c matutil/densutil.c csparse/dcsparse.c
+       matutil/genmat_config.c matutil/densutil.c csparse/dcsparse.c matutil/hb.c
 # precision-independent sources
 COM := fp/fpmatr.c cholesky/dense/ompss_dense_chol.c trsm/ompss_trsm.c syrk/ompss_syrk.c
 

@@ -17,10 +17,11 @@
 #include <string.h>
 
 #include "async_struct.h"
+#include "dcsparse.h"
+#include "hb.h"
 
-struct cs_sparse;
-struct css_s;
-struct csn_s;
+/* dcsparse.c defines cs_cholsol2 as cs_cholsol2_double; the header declares only the short name */
+int cs_cholsol2_double(int n, css *S, csn *N, double *b, double *x);
 
 int dcg_pure(int bm, int bn, int n, void *A, int s, void *b, void *xbuff, int *offs, double tol,
              int steps, void *work, unsigned long works, int async, double profile, int warmup,
@@ -63,4 +64,47 @@ int lnbref_dcg(int n, int bm, double *A, double *b, double *x, double tol, int s
 int lnbref_itref_main(int argc, char **argv)
 {
     return linompss_ref_itref_main(argc, argv);
+}
+
+/* The reference's block-Jacobi preconditioner of the sparse refinement,
+ * built exactly as itref_setup.c:55-93 builds it and applied as
+ * bsblas_dcholsolv2 (bsblas_csrmm.h:498-513) applies it: the complete bm x bm
+ * diagonal blocks of the zero-based CSR matrix (hb_sym_diag_block, hb.c:512),
+ * each handed to CSparse as a compressed matrix, analysed with natural
+ * ordering (cs_schol(A, 0)), factored (cs_chol) and solved
+ * (cs_cholsol2: z = L^-T L^-1 r).  Returns 0, or 1 + the first block whose
+ * factor failed. */
+int lnbref_bj_apply(int n, int bm, int *vptr, int *vpos, double *vval, const double *r, double *z)
+{
+    hbmat_t A;
+    memset(&A, 0, sizeof A);
+    A.m = A.n = n;
+    A.elemc = vptr[n];
+    A.vptr = vptr;
+    A.vpos = vpos;
+    A.vval = vval;
+    const int bs = (n + bm - 1) / bm;
+    hbmat_t *blocks = calloc((size_t)bs, sizeof(hbmat_t));
+    hb_sym_diag_block_double(&A, bm, blocks);
+    int rc = 0;
+    for (int i = 0, i0 = 0; i < bs; ++i, i0 += bm) {
+        hbmat_t *d = &blocks[i];
+        cs c;
+        c.nz = -1;
+        c.nzmax = d->elemc;
+        c.n = c.m = d->m;
+        c.p = d->vptr;
+        c.i = d->vpos;
+        c.x = d->vval;
+        css *S = cs_schol_double(&c, 0);
+        csn *N = S ? cs_chol_double(&c, S) : NULL;
+        if (!N) {
+            if (!rc) rc = 1 + i;
+        } else {
+            cs_cholsol2_double(d->m, S, N, (double *)r + i0, z + i0);
+        }
+        free(d->vptr); free(d->vpos); free(d->vval);
+    }
+    free(blocks);
+    return rc;
 }
