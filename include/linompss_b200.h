@@ -151,6 +151,35 @@ LNB_EXPORT int ompss_dcg(int n, int bm, const double *A, int lda, const double *
 LNB_EXPORT int ompss_ditref(int n, int bm, const double *A, int lda, const double *b,
                             double *x, double prec, int refit, int it, double *norms);
 
+/* Sparse refinement: itref.c built with USE_SPARSE (the refinement loop of
+ * itref.c:999-1101 and dcg_pure itref.c:690-925 over a sparse matrix).  A is
+ * n x n, symmetric positive definite, in CSR with both triangles stored (the
+ * reference's hbmat_t after dhb_sym_expand, hb.h:27-59): row pointers
+ * vptr[n+1], column indices vpos, values vval, zero- or one-based (the base
+ * is vptr[0], as the reference's one2zero reads it).  is_precond != 0: the
+ * inner solver uses the reference's block-Jacobi preconditioner
+ * (itref_setup.c:55-93): Cholesky, natural ordering, of every complete
+ * bm x bm diagonal block, applied as z = L^-T L^-1 r (bsblas_dcholsolv2,
+ * bsblas_csrmm.h:498); bm <= 512 here.  The recurrence is the reference's as
+ * it executes (see ompss_dcg): alpha1 = <r, z>, direction update p = 2 z,
+ * stop at sqrt(alpha1)/||b||_2 <= tol.  ompss_dscg: x is the start vector on
+ * entry and the iterate on exit; returns -1 if converged, else the steps.
+ * ompss_dsitref: arguments and return as ompss_ditref.  A diagonal block that
+ * is not positive definite returns LNB_EINVAL naming the block. */
+LNB_EXPORT int ompss_dscg(int n, int bm, const int *vptr, const int *vpos, const double *vval,
+                          const double *b, double *x, double tol, int steps, int is_precond);
+LNB_EXPORT int ompss_dsitref(int n, int bm, const int *vptr, const int *vpos, const double *vval,
+                             const double *b, double *x, double prec, int refit, int it,
+                             int is_precond, double *norms);
+/* MatrixMarket coordinate file ("real" or "integer", "general" or
+ * "symmetric") to zero-based CSR with ascending columns in every row; a
+ * symmetric file's off-diagonal entries appear in both triangles (the input
+ * the sparse refinement wants; the reference reads Harwell-Boeing files with
+ * readHB_newmat_double, itref_config.c:228-241).  The arrays are allocated
+ * here; release them with lnb_mm_free.  Returns 0 or LNB_E*. */
+LNB_EXPORT int lnb_mm_read_csr(const char *path, int *n, int **vptr, int **vpos, double **vval);
+LNB_EXPORT void lnb_mm_free(int *vptr, int *vpos, double *vval);
+
 /* ======================================================================== */
 /* 2. Device-pointer entry points (run on `stream`, asynchronous)            */
 /* ======================================================================== */

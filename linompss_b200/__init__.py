@@ -244,6 +244,47 @@ def ompss_ditref(n, bm, A, lda, b, x, prec, refit, it, norms=None) -> int:
     return _chk(f(n, bm, _p(A), lda, _p(b), _p(x), prec, refit, it, _p(norms)))
 
 
+def _csr(vptr, vpos, vval):
+    return (np.ascontiguousarray(vptr, dtype=np.int32), np.ascontiguousarray(vpos, dtype=np.int32),
+            np.ascontiguousarray(vval, dtype=np.float64))
+
+
+def ompss_dscg(n, bm, vptr, vpos, vval, b, x, tol, steps, is_precond=1) -> int:
+    """Sparse dcg_pure (x: start vector in, iterate out).  Returns -1 if converged, else the steps."""
+    vptr, vpos, vval = _csr(vptr, vpos, vval)
+    f = lib().ompss_dscg
+    f.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                  C.c_int, C.c_int]
+    rc = f(n, bm, _p(vptr), _p(vpos), _p(vval), _p(b), _p(x), tol, steps, is_precond)
+    if rc < -1:
+        raise LinompssError(rc, last_error())
+    return rc
+
+
+def ompss_dsitref(n, bm, vptr, vpos, vval, b, x, prec, refit, it, is_precond=1, norms=None) -> int:
+    vptr, vpos, vval = _csr(vptr, vpos, vval)
+    f = lib().ompss_dsitref
+    f.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                  C.c_int, C.c_int, C.c_int, C.c_void_p]
+    return _chk(f(n, bm, _p(vptr), _p(vpos), _p(vval), _p(b), _p(x), prec, refit, it, is_precond, _p(norms)))
+
+
+def mm_read_csr(path: str):
+    """MatrixMarket coordinate file -> (n, vptr, vpos, vval) zero-based CSR (numpy copies)."""
+    L = lib()
+    L.lnb_mm_read_csr.argtypes = [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.POINTER(C.c_int)),
+                                  C.POINTER(C.POINTER(C.c_int)), C.POINTER(C.POINTER(C.c_double))]
+    L.lnb_mm_free.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    n = C.c_int()
+    vp, vq, vv = C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_double)()
+    _chk(L.lnb_mm_read_csr(path.encode(), C.byref(n), C.byref(vp), C.byref(vq), C.byref(vv)))
+    nnz = vp[n.value]
+    out = (n.value, np.ctypeslib.as_array(vp, (n.value + 1,)).copy(),
+           np.ctypeslib.as_array(vq, (max(nnz, 1),))[:nnz].copy(), np.ctypeslib.as_array(vv, (max(nnz, 1),))[:nnz].copy())
+    L.lnb_mm_free(vp, vq, vv)
+    return out
+
+
 # --------------------------------------------------------------------------
 # device entry points (torch CUDA tensors, column-major as (ncols, ld))
 # --------------------------------------------------------------------------

@@ -247,3 +247,102 @@ def ref_cg(A: np.ndarray, rhs: np.ndarray, bm: int, tol: float, steps: int):
     rc = ref().lnbref_dcg(C.c_int(n), C.c_int(bm), _ptr(A), _ptr(np.ascontiguousarray(rhs)),
                           _ptr(x), C.c_double(tol), C.c_int(steps))
     return rc, x
+
+
+# --------------------------------------------------------------------------
+# sparse refinement (itref.c built with USE_SPARSE); CSR with base = vptr[0]
+# --------------------------------------------------------------------------
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def csr_from_dense(A: np.ndarray, base: int = 0):
+    """CSR (vptr, vpos, vval) of the nonzeros of A, rows in order, columns
+    ascending within a row; base 0 or 1 (the reference's one2zero offset)."""
+    n = A.shape[0]
+    vptr, vpos, vval = [base], [], []
+    for i in range(n):
+        cols = np.nonzero(A[i])[0]
+        vpos.extend(cols + base)
+        vval.extend(A[i, cols])
+        vptr.append(vptr[-1] + len(cols))
+    return _i32(vptr), _i32(vpos), np.ascontiguousarray(vval, dtype=np.float64)
+
+
+def csrmv(vptr, vpos, vval, x, alpha=1.0, beta=0.0, y=None):
+    n = len(vptr) - 1
+    y = np.zeros(n) if y is None else np.ascontiguousarray(y, dtype=np.float64).copy()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    lib().orc_csrmv(_i64(n), C.c_int(int(vptr[0])), _ptr(vptr), _ptr(vpos), _ptr(vval), _ptr(x),
+                    C.c_double(alpha), C.c_double(beta), _ptr(y))
+    return y
+
+
+def bj_setup(vptr, vpos, vval, bm: int):
+    """block-Jacobi factors (n/bm blocks of bm x bm, column-major); returns (rc, F)"""
+    n = len(vptr) - 1
+    nblk = (n + bm - 1) // bm
+    F = np.zeros(nblk * bm * bm)
+    rc = lib().orc_bj_setup(_i64(n), _i64(bm), C.c_int(int(vptr[0])), _ptr(vptr), _ptr(vpos), _ptr(vval), _ptr(F))
+    return rc, F
+
+
+def bj_apply(F, bm: int, r):
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    z = np.zeros_like(r)
+    lib().orc_bj_apply(_i64(len(r)), _i64(bm), _ptr(F), _ptr(r), _ptr(z))
+    return z
+
+
+def scg(vptr, vpos, vval, rhs, bm: int, tol: float, steps: int, precond: bool):
+    n = len(vptr) - 1
+    F = bj_setup(vptr, vpos, vval, bm)[1] if precond else None
+    x = np.zeros(n)
+    log = np.zeros(max(steps, 1))
+    rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+    rc = lib().orc_dscg(_i64(n), _i64(bm), C.c_int(int(vptr[0])), _ptr(vptr), _ptr(vpos), _ptr(vval),
+                        _ptr(F) if F is not None else None, _ptr(rhs), _ptr(x), C.c_double(tol), C.c_int(steps),
+                        _ptr(log))
+    return rc, x, log
+
+
+def sitref(vptr, vpos, vval, rhs, bm: int, prec: float, refit: int, it: int, precond: bool):
+    n = len(vptr) - 1
+    F = bj_setup(vptr, vpos, vval, bm)[1] if precond else None
+    x = np.zeros(n)
+    norms = np.zeros(max(refit, 1))
+    rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+    k = lib().orc_dsitref(_i64(n), _i64(bm), C.c_int(int(vptr[0])), _ptr(vptr), _ptr(vpos), _ptr(vval),
+                          _ptr(F) if F is not None else None, _ptr(rhs), _ptr(x), C.c_double(prec), C.c_int(refit),
+                          C.c_int(it), _ptr(norms))
+    return k, x, norms[:k]
+
+
+def ref_bj_apply(vptr, vpos, vval, bm: int, r):
+    """the reference's own block-Jacobi preconditioner (CSparse, itref_setup.c:55-93)
+    applied to r; zero-based CSR.  Returns (rc, z)."""
+    n = len(vptr) - 1
+    vptr, vpos = _i32(vptr).copy(), _i32(vpos).copy()
+    vval = np.ascontiguousarray(vval, dtype=np.float64).copy()
+    r = np.ascontiguousarray(r, dtype=np.float64)
+    z = np.zeros(n)
+    rc = ref().lnbref_bj_apply(C.c_int(n), C.c_int(bm), _ptr(vptr), _ptr(vpos), _ptr(vval), _ptr(r), _ptr(z))
+    return rc, z
+
+
+def spd_sparse(n: int, seed: int = 0, density: float = 0.02, shift: float = 1.0) -> np.ndarray:
+    """a sparse SPD test matrix: the 5-point Laplacian of a near-square grid plus
+    a symmetric random sparse perturbation, made diagonally dominant"""
+    rng = np.random.default_rng(seed)
+    m = int(np.ceil(np.sqrt(n)))
+    A = np.zeros((n, n))
+    for i in range(n):
+        A[i, i] = 4.0
+        for j in (i - 1, i + 1, i - m, i + m):
+            if 0 <= j < n and (abs(i - j) != 1 or (i // m) == (j // m)):
+                A[i, j] = -1.0
+    R = (rng.random((n, n)) < density) * rng.uniform(-0.5, 0.5, (n, n))
+    R = np.triu(R, 1)
+    A += R + R.T
+    A[np.diag_indices(n)] += np.abs(A).sum(axis=1) - np.abs(np.diag(A)) + shift - np.diag(A) + 4.0
+    return A

@@ -21,6 +21,12 @@ scaled down to a few hundred KB in total:
   dcg_*       itref.c dcg_pure on a G G^T/n + I matrix
   itref_*     the refinement loop of itref.c main(), driven through its argv
               with A and RHS passed as files (itref_config.c:130-222)
+  sparse_bj_* the block-Jacobi preconditioner of the sparse refinement, built
+              by the reference's own code (hb_sym_diag_block + CSparse
+              cs_schol/cs_chol/cs_cholsol2, itref_setup.c:55-93) on a sparse
+              SPD matrix in zero-based CSR, applied to a vector
+
+    python tests/golden/make_golden.py [group ...]   (default: every group)
 """
 from __future__ import annotations
 
@@ -174,9 +180,23 @@ def itref_cases():
              it=np.int64(it), prec=np.float64(prec), bm=np.int64(bm))
 
 
+def sparse_bj_cases():
+    for n, bm, seed in ((150, 32, 1), (200, 48, 2)):
+        A = O.spd_sparse(n, seed=seed)
+        vptr, vpos, vval = O.csr_from_dense(A)
+        r = np.random.default_rng(seed + 50).standard_normal(n)
+        rc, z = O.ref_bj_apply(vptr, vpos, vval, bm, r)
+        assert rc == 0
+        save(f"sparse_bj_n{n}_bm{bm}", A=A, vptr=vptr, vpos=vpos, vval=vval, r=r, z=z, bm=np.int64(bm))
+
+
 if __name__ == "__main__":
     if not O.ref_available():
         sys.exit("build the reference first: make -C oracle ref")
+    if len(sys.argv) > 1:
+        for group in sys.argv[1:]:
+            globals()[group + "_cases"]()
+        sys.exit(0)
     chol_cases()
     schol_case()
     spdsolv_cases()

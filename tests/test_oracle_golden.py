@@ -155,3 +155,62 @@ def test_blocked_ssyrk(golden_dir):
     O.syrk("L", "N", n, k, float(d["alpha"]), np.asfortranarray(d["A"]), float(d["beta"]), Cm)
     tol = 4 * k * np.finfo(np.float32).eps * np.abs(d["out"]).max()
     np.testing.assert_allclose(Cm, d["out"], rtol=0, atol=tol)
+
+
+# ---------------------------------------------------------------- sparse refinement
+# The reference's sparse matrix product is MKL's mkl_dcsrmv (fpsblas.h defines
+# SBLAS_csrmv empty without MKL, and task_csrmm.c does not compile in the
+# non-MKL configuration), so the sparse restatement is pinned piece by piece:
+# its block-Jacobi against the reference's own CSparse preconditioner, and its
+# recurrence against the reference's dense dcg_pure on the same matrix as CSR.
+@pytest.mark.parametrize("name", ["sparse_bj_n150_bm32", "sparse_bj_n200_bm48"])
+def test_oracle_block_jacobi_matches_reference(golden_dir, name):
+    d = np.load(os.path.join(golden_dir, name + ".npz"))
+    bm = int(d["bm"])
+    rc, F = O.bj_setup(d["vptr"], d["vpos"], d["vval"], bm)
+    assert rc == 0
+    z = O.bj_apply(F, bm, d["r"])
+    np.testing.assert_allclose(z, d["z"], rtol=1e-13, atol=1e-15 * np.abs(d["z"]).max())
+
+
+@pytest.mark.parametrize("name", ["dcg_n64_bm16_s8", "dcg_n64_bm16_s200", "dcg_n100_bm32_s300"])
+@pytest.mark.parametrize("base", [0, 1])
+def test_oracle_sparse_cg_reproduces_reference_dense_cg(golden_dir, name, base):
+    """a dense matrix given as CSR: the sparse dcg_pure takes the reference's dense iterates"""
+    d = np.load(os.path.join(golden_dir, name + ".npz"))
+    vptr, vpos, vval = O.csr_from_dense(d["A"], base)
+    rc, x, _ = O.scg(vptr, vpos, vval, d["rhs"], int(d["bm"]), float(d["tol"]), int(d["steps"]), False)
+    assert rc == int(d["rc"])
+    np.testing.assert_allclose(x, d["x"], rtol=1e-12, atol=1e-14)
+
+
+def test_oracle_sparse_refinement_converges_with_block_jacobi():
+    A = O.spd_sparse(300, seed=3)
+    vptr, vpos, vval = O.csr_from_dense(A)
+    x_true = np.random.default_rng(3).standard_normal(300)
+    k, x, norms = O.sitref(vptr, vpos, vval, A @ x_true, 64, 1e-12, 10, 300, True)
+    assert 1 <= k <= 10
+    np.testing.assert_allclose(x, x_true, rtol=0, atol=1e-10)
+
+
+def test_mm_reader_matches_scipy(tmp_path):
+    """the library's MatrixMarket reader (host code, no device needed)"""
+    import scipy.io
+    import scipy.sparse
+
+    import linompss_b200 as lnb
+    A = O.spd_sparse(80, seed=4)
+    for kind in ("symmetric", "general"):
+        path = str(tmp_path / f"a_{kind}.mtx")
+        M = scipy.sparse.coo_matrix(np.tril(A) if kind == "symmetric" else A)
+        scipy.io.mmwrite(path, M, symmetry=kind)
+        n, vptr, vpos, vval = lnb.mm_read_csr(path)
+        assert n == 80
+        ref = scipy.sparse.csr_matrix(scipy.io.mmread(path)).toarray()
+        got = np.zeros((n, n))
+        for i in range(n):
+            for p in range(vptr[i], vptr[i + 1]):
+                got[i, vpos[p]] += vval[p]
+            assert np.all(np.diff(vpos[vptr[i]:vptr[i + 1]]) > 0)
+        np.testing.assert_allclose(got, A, rtol=0, atol=1e-15)
+        np.testing.assert_allclose(ref if kind == "general" else A, A)
