@@ -242,6 +242,14 @@ LNB_EXPORT int lnb_dposv_dev(int n, int nrhs, int b, double *dA, int lda, double
 LNB_EXPORT int lnb_dtrsm_dev(char uplo, char trans, char diag, int m, int n, double alpha,
                              const double *dA, int lda, double *dB, int ldb, void *stream);
 
+/* The refinement's matrix product Y = A X for symmetric A given by its lower
+ * triangle (the strict upper part of dA is not read), FP64.  Replaces the
+ * reference's bblas_dgemm matvec over the full stored A (itref.c:1086,1094),
+ * which reads both triangles.  dX, dY: n x nrhs with ld = n; the columns of Y
+ * are sums in an unspecified order (atomic accumulation). */
+LNB_EXPORT int lnb_dsymv_dev(int n, int nrhs, const double *dA, int lda, const double *dX, double *dY,
+                             void *stream);
+
 /* ======================================================================== */
 /* 3. Mixed precision: low-precision factor + FP64 iterative refinement       */
 /* ======================================================================== */

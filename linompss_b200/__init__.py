@@ -317,6 +317,13 @@ def dpotrs_dev(Lt, Bt, n: int, nrhs: int, which: str = "B", stream=None) -> int:
                                      C.c_int(_ld(Bt)), C.c_char(which.encode()), _stream(stream)))
 
 
+def dsymv_dev(At, Xt, Yt, n: int, nrhs: int, stream=None) -> int:
+    """Y = A X from the lower triangle of A; Xt, Yt as (nrhs, n) contiguous tensors (ld n)."""
+    f = lib().lnb_dsymv_dev
+    f.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    return _chk(f(n, nrhs, _p(At), _ld(At), _p(Xt), _p(Yt), _stream(stream)))
+
+
 def dtrsm_dev(uplo: str, trans: str, diag: str, m: int, n: int, alpha: float, At, Bt, stream=None) -> int:
     f = lib().lnb_dtrsm_dev
     f.argtypes = [C.c_char, C.c_char, C.c_char, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int,

@@ -12,6 +12,8 @@
 // group and keeps per-column partials for the transposed contribution, which
 // are reduced across the CTA once per strip.  Accumulation into y uses double
 // atomics (summation order is not fixed).
+#include <stdlib.h>
+
 #include "common.cuh"
 
 namespace lnb {
@@ -117,6 +119,173 @@ __global__ void __launch_bounds__(SV_THREADS, 2) k_symv_lower(int64_t n, const d
     }
 }
 
+// ---- several right-hand sides on the FP64 tensor cores ---------------------
+//
+// With 2..8 right-hand sides each stored element costs 2 nr FMAs, as many as
+// the HBM stream can feed, so both products go to DMMA (m16n8k4, N = 8 = the
+// right-hand-side pass).  A work item is a 256 x 256 block of the lower
+// triangle (4 x 4 tiles of 64 x 64); tiles stream through shared memory by
+// cp.async, double-buffered, two CTAs per SM.  Per tile, warps 0-3 form
+// y_I += T x_J (one 16-row slab each) and warps 4-7 form y_J += T^T x_I (one
+// 16-column slab each).  y_I builds up in registers over the item's tile row
+// and y_J over the whole item, so Y takes (4 + 4) x 64 x 8 atomic adds per 16
+// tiles.  A diagonal tile holds only its lower triangle: the row warps read
+// the mirrored element above the diagonal and the column warps skip it.
+namespace symtc {
+constexpr int TS = 64, LD = 68, RB = 4, NT = 256, STAGES = 2;
+constexpr int BR = RB * TS;                       // rows of an item's block
+struct Smem {
+    double t[STAGES][TS * LD];
+    double xi[BR * 8];                            // x rows of the item's row block, 8 per row (swizzled)
+    double xj[BR * 8];                            // and of its column block
+};
+// element (row, q) of a staged x block; the swizzle keeps the B-fragment
+// loads (rows 4kk + t, column g) free of bank conflicts
+LNB_DEV int xoff(int row, int q) { return row * 8 + (q ^ (((row >> 1) & 1) << 2)); }
+
+LNB_DEV void load_tile(double *dst, const double *A, int64_t lda, int64_t n, int64_t R, int64_t Cc, bool diag,
+                       int tid)
+{
+#pragma unroll
+    for (int k = 0; k < (TS * TS / 2) / NT; ++k) {
+        const int ch = tid + k * NT;
+        const int c = ch >> 5, rp = (ch & 31) * 2;
+        if (diag && rp + 1 < c) continue;         // strictly above the diagonal: never read
+        const int64_t gr = R + rp, gc = Cc + c;
+        int bytes = 0;
+        if (gc < n && gr < n) bytes = (n - gr) >= 2 ? 16 : 8;
+        const double *src = bytes ? A + gr + gc * lda : A;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst + c * LD + rp)),
+                     "l"(src), "r"(bytes));
+    }
+}
+
+__global__ void __launch_bounds__(NT, 2) k_symv_tc(int64_t n, int64_t nB, const double *__restrict__ A, int64_t lda,
+                                                   const double *__restrict__ X, int nr, double *Y)
+{
+    extern __shared__ __align__(16) unsigned char smraw[];
+    Smem &S = *reinterpret_cast<Smem *>(smraw);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
+    // item -> (bi, bj), bi >= bj, row-major over the lower triangle of the block grid
+    const int64_t idx = blockIdx.x;
+    int64_t bi = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+    while (bi * (bi + 1) / 2 > idx) --bi;
+    while ((bi + 1) * (bi + 2) / 2 <= idx) ++bi;
+    const int64_t bj = idx - bi * (bi + 1) / 2;
+    (void)nB;
+    const bool diag = bi == bj;
+    const int64_t r0 = bi * BR, c0 = bj * BR;
+    const int nti = (int)min((int64_t)RB, (n - r0 + TS - 1) / TS);
+    const int ntj = (int)min((int64_t)RB, (n - c0 + TS - 1) / TS);
+    const int ntiles = diag ? nti * (nti + 1) / 2 : nti * ntj;
+
+    auto decode = [&](int i, int &ii, int &jj) {
+        if (diag) {
+            ii = 0;
+            while ((ii + 1) * (ii + 2) / 2 <= i) ++ii;
+            jj = i - ii * (ii + 1) / 2;
+        } else {
+            ii = i / ntj;
+            jj = i - ii * ntj;
+        }
+    };
+    auto issue = [&](int i) {
+        if (i < ntiles) {
+            int ii, jj;
+            decode(i, ii, jj);
+            load_tile(S.t[i % STAGES], A, lda, n, r0 + ii * TS, c0 + jj * TS, diag && ii == jj, tid);
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) issue(s);
+
+    for (int e = tid; e < BR * 8; e += NT) {
+        const int q = e / BR, row = e - q * BR;
+        const int64_t ri = r0 + row, rj = c0 + row;
+        S.xi[xoff(row, q)] = (q < nr && ri < n) ? X[ri + (int64_t)q * n] : 0.0;
+        S.xj[xoff(row, q)] = (q < nr && rj < n) ? X[rj + (int64_t)q * n] : 0.0;
+    }
+
+    const bool roww = warp < 4;
+    const int m16 = (warp & 3) * 16;
+    double accC[RB][4];
+#pragma unroll
+    for (int j = 0; j < RB; ++j)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) accC[j][v] = 0.0;
+    int tc = 0;
+    for (int ii = 0; ii < nti; ++ii) {
+        double accR[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int jj = 0; jj < RB; ++jj) {
+            if (jj >= ntj || (diag && jj > ii)) continue;
+            issue(tc + STAGES - 1);
+            cp_async_wait<STAGES - 1>();
+            __syncthreads();
+            const double *T = S.t[tc % STAGES];
+            const bool dt = diag && jj == ii;
+            if (roww) {
+                const double *xb = S.xj + jj * TS * 8;
+                if (!dt) {
+#pragma unroll
+                    for (int kk = 0; kk < TS / 4; ++kk) {
+                        const int c = 4 * kk + t4;
+                        dmma16x8x4(accR, T[c * LD + m16 + g], T[c * LD + m16 + g + 8], xb[xoff(c, g)]);
+                    }
+                } else {
+#pragma unroll
+                    for (int kk = 0; kk < TS / 4; ++kk) {
+                        const int c = 4 * kk + t4, ra = m16 + g, rb = ra + 8;
+                        const double a0 = ra >= c ? T[c * LD + ra] : T[ra * LD + c];
+                        const double a1 = rb >= c ? T[c * LD + rb] : T[rb * LD + c];
+                        dmma16x8x4(accR, a0, a1, xb[xoff(c, g)]);
+                    }
+                }
+            } else if (!dt) {
+                const double *xb = S.xi + ii * TS * 8;
+#pragma unroll
+                for (int kk = 0; kk < TS / 4; ++kk) {
+                    const int r = 4 * kk + t4;
+                    dmma16x8x4(accC[jj], T[(m16 + g) * LD + r], T[(m16 + g + 8) * LD + r], xb[xoff(r, g)]);
+                }
+            }
+            __syncthreads();
+            ++tc;
+        }
+        if (roww) {
+            const int64_t ra = r0 + ii * TS + m16 + g, rb = ra + 8;
+            const int q0 = 2 * t4, q1 = q0 + 1;
+            if (ra < n) {
+                if (q0 < nr) atomicAdd(Y + ra + (int64_t)q0 * n, accR[0]);
+                if (q1 < nr) atomicAdd(Y + ra + (int64_t)q1 * n, accR[1]);
+            }
+            if (rb < n) {
+                if (q0 < nr) atomicAdd(Y + rb + (int64_t)q0 * n, accR[2]);
+                if (q1 < nr) atomicAdd(Y + rb + (int64_t)q1 * n, accR[3]);
+            }
+        }
+    }
+    if (!roww) {
+#pragma unroll
+        for (int jj = 0; jj < RB; ++jj) {
+            if (jj >= ntj || (diag && jj == nti - 1)) continue;   // the last diagonal column has no tile below
+            const int64_t ca = c0 + jj * TS + m16 + g, cb = ca + 8;
+            const int q0 = 2 * t4, q1 = q0 + 1;
+            if (ca < n) {
+                if (q0 < nr) atomicAdd(Y + ca + (int64_t)q0 * n, accC[jj][0]);
+                if (q1 < nr) atomicAdd(Y + ca + (int64_t)q1 * n, accC[jj][1]);
+            }
+            if (cb < n) {
+                if (q0 < nr) atomicAdd(Y + cb + (int64_t)q0 * n, accC[jj][2]);
+                if (q1 < nr) atomicAdd(Y + cb + (int64_t)q1 * n, accC[jj][3]);
+            }
+        }
+    }
+    cp_async_wait<0>();
+}
+}  // namespace symtc
+
 LNB_DEV void atomic_max_nonneg(double *addr, double v)
 {
     // non-negative doubles order like their bit patterns as signed 64-bit ints
@@ -207,19 +376,49 @@ static void launch_symv(int64_t n, const double *A, int64_t lda, const double *X
     lnb_prof_count(1);
 }
 
-// nrhs columns are processed in passes of 8 / 4 / 2 / 1 (X, Y with ld n)
+static bool symv_tc_enabled()
+{
+    static int v = -1;
+    if (v < 0) {
+        const char *e = getenv("LNB_SYMV_TC");      /* 0: the strip kernel for every right-hand-side count */
+        v = (e && e[0] == '0') ? 0 : 1;
+    }
+    return v == 1;
+}
+
+// nrhs columns are processed in passes of 8 (tensor cores, 2..8 columns per
+// pass) or, on the strip kernel, of 8 / 4 / 2 / 1 (X, Y with ld n)
 extern "C" int lnb_k_symv_lower_f64(int64_t n, int64_t nrhs, const double *A, int64_t lda, const double *X,
                                     double *Y, int absval, lnb_stream_t s)
 {
     if (n <= 0 || nrhs <= 0) return 0;
     cudaError_t e = cudaMemsetAsync(Y, 0, sizeof(double) * n * nrhs, s);
     if (e != cudaSuccess) return (int)e;
+    /* the tensor-core pass stages A by 16-byte copies: A 16-byte aligned, lda even */
+    const bool use_tc = !absval && symv_tc_enabled() && (lda % 2) == 0 && ((uintptr_t)A % 16) == 0;
+    if (use_tc) {
+        static int attr_set = 0;
+        if (!attr_set) {
+            e = cudaFuncSetAttribute(symtc::k_symv_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(symtc::Smem));
+            if (e != cudaSuccess) return (int)e;
+            attr_set = 1;
+        }
+    }
     int64_t q = 0;
     while (q < nrhs) {
         const int64_t left = nrhs - q;
         const double *Xq = X + q * n;
         double *Yq = Y + q * n;
-        if (left >= 8) { launch_symv<8>(n, A, lda, Xq, Yq, absval, s); q += 8; }
+        if (left >= 2 && use_tc) {
+            const int nr = left >= 8 ? 8 : (int)left;
+            const int64_t nB = (n + symtc::BR - 1) / symtc::BR;
+            symtc::k_symv_tc<<<(unsigned)(nB * (nB + 1) / 2), symtc::NT, sizeof(symtc::Smem), s>>>(n, nB, A, lda, Xq,
+                                                                                                 nr, Yq);
+            lnb_prof_count(1);
+            q += nr;
+        }
+        else if (left >= 8) { launch_symv<8>(n, A, lda, Xq, Yq, absval, s); q += 8; }
         else if (left >= 4) { launch_symv<4>(n, A, lda, Xq, Yq, absval, s); q += 4; }
         else if (left >= 2) { launch_symv<2>(n, A, lda, Xq, Yq, absval, s); q += 2; }
         else { launch_symv<1>(n, A, lda, Xq, Yq, absval, s); q += 1; }

@@ -100,6 +100,17 @@ int lnb_dtrsm_dev(char uplo, char trans, char diag, int m, int n, double alpha, 
     return lnb_trsm_f64_run(c, uplo, trans, diag, m, n, alpha, dA, lda, dB, ldb, &ar, s, NULL);
 }
 
+int lnb_dsymv_dev(int n, int nrhs, const double *dA, int lda, const double *dX, double *dY, void *stream)
+{
+    if (n < 0 || nrhs < 0 || lda < (n > 1 ? n : 1)) return lnb_set_error(LNB_EINVAL, "dsymv sizes");
+    if (n == 0 || nrhs == 0) return 0;
+    if (!dA || !dX || !dY) return lnb_set_error(LNB_EINVAL, "dsymv: NULL argument");
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    CK(lnb_k_symv_lower_f64(n, nrhs, dA, lda, dX, dY, 0, (cudaStream_t)stream), "dsymv");
+    return 0;
+}
+
 int lnb_dpotrs_dev(int n, int nrhs, const double *dL, int lda, double *dB, int ldb, char which,
                    void *stream)
 {
