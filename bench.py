@@ -748,6 +748,133 @@ def config_records(args, world, rank, dev, peaks):
     return out
 
 
+def blas_records(args, world, rank, dev, peaks):
+    """The stand-alone BLAS-3 drivers at the reference's own chart sizes
+    (tests/dsyrk.cfg: lower, transposed, n = k = 16000, alpha 13.44, beta
+    -9.877, b in {550, 1032, 2898, 5988}; tests/dtrsm.cfg: left lower, no
+    transpose, m = n = 1500, alpha 13.44, b in {121, 256, 350, 550}), each timed
+    on the device (DMMA kernels), end to end through the reference-named host
+    entry point (host arrays in, result back), and, on rank 0 of a 1-GPU run,
+    the reference build's own call on the same arrays (OpenBLAS on every host
+    thread; b only changes the reference's tiling)."""
+    import numpy as np
+    import torch
+
+    import linompss_b200 as lnb
+    cores = os.cpu_count() or 1
+    os.environ["OPENBLAS_NUM_THREADS"] = str(cores)
+    s = torch.cuda.current_stream()
+    reps = max(1, min(args.steps, 3))
+    out = {}
+    with_ref = rank == 0 and world == 1 and not args.no_cpu_baseline
+    if with_ref:
+        from oracle import oracle as O
+        with_ref = O.ref_available()
+
+    # ---- dsyrk ----
+    n = k = 16000
+    alpha, beta = 13.44, -9.877
+    g = torch.Generator(device=dev)
+    g.manual_seed(16000 + rank)
+    At = torch.randn(n, k, dtype=torch.float64, device=dev, generator=g)    # A stored k x n (trans = 'T')
+    C0 = torch.randn(n, n, dtype=torch.float64, device=dev, generator=g)
+    Ct = torch.empty_like(C0)
+    run = lambda: lnb.dsyrk_dev("L", "T", n, k, alpha, At, beta, Ct, stream=s)
+    prep = lambda: Ct.copy_(C0)
+    time_events(run, 1, s, prep)
+    ms = allmax(world, time_events(run, reps, s, prep))
+    fl = float(n) * (n + 1) * k
+    ref = torch.addmm(C0.t(), At, At.t(), beta=beta, alpha=alpha)          # cuBLAS FP64, full matrix
+    got = Ct.t()
+    lo = torch.tril(torch.ones(n, n, dtype=torch.bool, device=dev))
+    err = float(((got - ref).abs() * lo).max() / ref.abs().max())
+    assert err < 1e-12, err
+    rec = {"n": n, "k": k, "uplo": "L", "trans": "T", "alpha": alpha, "beta": beta,
+           "device_ms": round(ms, 3), "device_tflops": round(world * fl / ms / 1e9, 3),
+           "frac_of_fp64_dgemm_peak": round(fl / ms / 1e9 / peaks["fp64"], 4),
+           "max_rel_err_vs_cublas_dgemm": err, "kernel": "k_gemm_dmma (DMMA, 64x64 tiles, lower tiles only)"}
+    del ref, got, lo
+    Ah = torch.empty((n, k), dtype=torch.float64, pin_memory=True)
+    Ah.copy_(At)
+    Ch0 = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+    Ch0.copy_(C0)
+    del At, C0, Ct
+    torch.cuda.empty_cache()
+    A_np = Ah.numpy().T          # column-major k x n view
+    Ch = torch.empty_like(Ch0, pin_memory=True)
+    times = []
+    for i in range(2):
+        Ch.copy_(Ch0)
+        C_np = Ch.numpy().T
+        t0 = time.perf_counter()
+        lnb.ompss_dsyrk("L", "T", 550, n, k, alpha, A_np, k, C_np, n, beta=beta)
+        times.append(time.perf_counter() - t0)
+    rec["e2e_ms"] = round(allmax(world, times[-1]) * 1e3, 3)
+    rec["e2e_tflops"] = round(world * fl / (rec["e2e_ms"] / 1e3) / 1e12, 3)
+    rec["e2e_api"] = "ompss_dsyrk (host arrays, pinned): A and C in, C out (6.1 GB over PCIe)"
+    if with_ref:
+        rref = {}
+        for bb in (550, 5988):
+            Ch.copy_(Ch0)
+            C_np = Ch.numpy().T
+            t0 = time.perf_counter()
+            O.ref_dsyrk("L", "T", bb, n, k, alpha, A_np, k, beta, C_np, n)
+            rref[f"b{bb}_s"] = round(time.perf_counter() - t0, 3)
+        rref["cores"] = cores
+        rref["tflops_best"] = round(fl / min(v for kk, v in rref.items() if kk.endswith("_s")) / 1e12, 4)
+        rec["reference"] = rref
+        rec["e2e_speedup_vs_reference_best"] = round(min(rref["b550_s"], rref["b5988_s"]) / (rec["e2e_ms"] / 1e3), 2)
+    out["dsyrk_n16000_k16000"] = rec
+    del Ah, Ch0, Ch
+    # ---- dtrsm ----
+    m = nn = 1500
+    alpha = 13.44
+    rng = np.random.default_rng(1500 + rank)
+    Lm = np.tril(rng.standard_normal((m, m))) + m * np.eye(m)
+    Lm = np.asfortranarray(Lm)
+    B0 = np.asfortranarray(rng.standard_normal((m, nn)))
+    Ld = torch.tensor(np.ascontiguousarray(Lm.T), device=dev)
+    Bd0 = torch.tensor(np.ascontiguousarray(B0.T), device=dev)
+    Bd = torch.empty_like(Bd0)
+    run = lambda: lnb.dtrsm_dev("L", "N", "N", m, nn, alpha, Ld, Bd, stream=s)
+    prep = lambda: Bd.copy_(Bd0)
+    time_events(run, 1, s, prep)
+    ms = allmax(world, time_events(run, reps, s, prep))
+    fl = float(m) * m * nn
+    X = Bd.cpu().numpy().T
+    err = float(np.abs(Lm @ X - alpha * B0).max() / (np.abs(Lm).sum(1).max() * np.abs(X).max()))
+    rec = {"m": m, "n": nn, "side": "L", "uplo": "L", "trans": "N", "diag": "N", "alpha": alpha,
+           "device_ms": round(ms, 4), "device_tflops": round(world * fl / ms / 1e9, 4), "backward_error": err}
+    assert err < 10 * m * np.finfo(float).eps, err
+    e2e = {}
+    for bb in (121, 256, 350, 550):
+        t = []
+        for _ in range(3):
+            B = B0.copy(order="F")
+            t0 = time.perf_counter()
+            lnb.ompss_dtrsm("L", "L", "N", "N", m, nn, bb, alpha, Lm, m, B, m)
+            t.append(time.perf_counter() - t0)
+        e2e[f"b{bb}_ms"] = round(min(t) * 1e3, 3)
+    rec["e2e"] = e2e
+    rec["e2e_api"] = "ompss_dtrsm (host arrays): L and B in, X out"
+    if with_ref:
+        rref = {}
+        for bb in (121, 256, 350, 550):
+            t = []
+            for _ in range(3):
+                B = B0.copy(order="F")
+                t0 = time.perf_counter()
+                O.ref_dtrsm("L", "L", "N", "N", m, nn, bb, alpha, Lm, m, B, m)
+                t.append(time.perf_counter() - t0)
+            rref[f"b{bb}_ms"] = round(min(t) * 1e3, 3)
+        rref["cores"] = cores
+        rec["reference"] = rref
+    out["dtrsm_m1500_n1500"] = rec
+    del Ld, Bd0, Bd
+    torch.cuda.empty_cache()
+    return out
+
+
 def ours_arm(args, world, rank, local):
     import numpy as np
     import torch
@@ -944,6 +1071,7 @@ def ours_arm(args, world, rank, local):
         del A0, B0, X
         torch.cuda.empty_cache()
         line["configs"] = config_records(args, world, rank, dev, peaks)
+        line["blas"] = blas_records(args, world, rank, dev, peaks)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ns = min(n, 8192)

@@ -242,6 +242,16 @@ LNB_EXPORT int lnb_dposv_dev(int n, int nrhs, int b, double *dA, int lda, double
 LNB_EXPORT int lnb_dtrsm_dev(char uplo, char trans, char diag, int m, int n, double alpha,
                              const double *dA, int lda, double *dB, int ldb, void *stream);
 
+/* Device forms of the tile BLAS-3 tasks on the FP64 tensor cores (DMMA):
+ * C = alpha op(A) op(B) + beta C (task_dgemm, task_gemm.c:55-58) and
+ * C = alpha op(A) op(A)^T + beta C on triangle uplo of C (task_dsyrk,
+ * tasks_syrk.c:19-21).  Options as characters ('N'/'T', 'L'/'U'); beta == 0
+ * does not read C.  Asynchronous on `stream`. */
+LNB_EXPORT int lnb_dgemm_dev(char transa, char transb, int m, int n, int k, double alpha, const double *dA,
+                             int lda, const double *dB, int ldb, double beta, double *dC, int ldc, void *stream);
+LNB_EXPORT int lnb_dsyrk_dev(char uplo, char trans, int n, int k, double alpha, const double *dA, int lda,
+                             double beta, double *dC, int ldc, void *stream);
+
 /* The refinement's matrix product Y = A X for symmetric A given by its lower
  * triangle (the strict upper part of dA is not read), FP64.  Replaces the
  * reference's bblas_dgemm matvec over the full stored A (itref.c:1086,1094),

@@ -317,6 +317,25 @@ def dpotrs_dev(Lt, Bt, n: int, nrhs: int, which: str = "B", stream=None) -> int:
                                      C.c_int(_ld(Bt)), C.c_char(which.encode()), _stream(stream)))
 
 
+def dgemm_dev(transa: str, transb: str, m: int, n: int, k: int, alpha: float, At, Bt, beta: float, Ct,
+              stream=None) -> int:
+    """C = alpha op(A) op(B) + beta C on device tensors (column-major as (cols, ld))."""
+    f = lib().lnb_dgemm_dev
+    f.argtypes = [C.c_char, C.c_char, C.c_int, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_void_p,
+                  C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_void_p]
+    return _chk(f(transa.encode(), transb.encode(), m, n, k, alpha, _p(At), _ld(At), _p(Bt), _ld(Bt), beta, _p(Ct),
+                  _ld(Ct), _stream(stream)))
+
+
+def dsyrk_dev(uplo: str, trans: str, n: int, k: int, alpha: float, At, beta: float, Ct, stream=None) -> int:
+    """C = alpha op(A) op(A)^T + beta C on triangle `uplo` of the device tensor Ct."""
+    f = lib().lnb_dsyrk_dev
+    f.argtypes = [C.c_char, C.c_char, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_double, C.c_void_p,
+                  C.c_int, C.c_void_p]
+    return _chk(f(uplo.encode(), trans.encode(), n, k, alpha, _p(At), _ld(At), beta, _p(Ct), _ld(Ct),
+                  _stream(stream)))
+
+
 def dsymv_dev(At, Xt, Yt, n: int, nrhs: int, stream=None) -> int:
     """Y = A X from the lower triangle of A; Xt, Yt as (nrhs, n) contiguous tensors (ld n)."""
     f = lib().lnb_dsymv_dev

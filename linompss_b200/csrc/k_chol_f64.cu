@@ -297,54 +297,136 @@ __global__ void __launch_bounds__(128) k_trsm_rlt_f64(const double *__restrict__
 }
 
 // ========================================================================
-// Generic FP64 GEMM for the tile-task ABI (task_dgemm / task_dsyrk)
+// FP64 GEMM of the tile-task ABI (task_dgemm / task_dsyrk / ompss_dsyrk)
 // ========================================================================
 // C = alpha op(A) op(B) + beta C, optionally restricted to a triangle of C
-// (tri = 'L' or 'U').  SIMT, 64x64 tiles, 4x4 per thread.
-__global__ void __launch_bounds__(256) k_gemm_f64(char ta, char tb, int64_t M, int64_t N, int64_t K,
-                                                  double alpha, const double *A, int64_t lda,
-                                                  const double *Bm, int64_t ldb, double beta,
-                                                  double *C, int64_t ldc, char tri)
+// (tri = 'L' or 'U'), on DMMA: 64 x 64 CTA tiles, 4 warps of 32 x 32, BK = 16,
+// 4-stage cp.async pipeline, two CTAs per SM.  Each operand is staged in the
+// orientation its memory is contiguous in, so every copy is a 16-byte
+// cp.async along a column: op(A) = A and op(B) = B^T are stored k-major
+// (S[k][m], row stride 68), op(A) = A^T and op(B) = B m-major (S[m][k], row
+// stride 20).  Both strides spread a half-warp's fragment reads over all 32
+// banks.  beta == 0 does not read C (BLAS semantics).
+namespace gm {
+constexpr int BM = 64, BN = 64, BK = 16, ST = 4, THREADS = 128;
+constexpr int LDKM = BM + 4;                  // k-major row stride (doubles)
+constexpr int LDMK = BK + 4;                  // m-major row stride
+constexpr int STAGE = (BM * LDMK > BK * LDKM) ? BM * LDMK : BK * LDKM;
+constexpr int SMEM = ST * 2 * STAGE * (int)sizeof(double);
+
+// two consecutive elements src[0], src[1] (nv of them valid) -> dst[0..1]
+LNB_DEV void load2(double *dst, const double *src, int nv)
 {
-    __shared__ double As[16][65], Bs[16][65];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int64_t m0 = (int64_t)blockIdx.y * 64, n0 = (int64_t)blockIdx.x * 64;
-    double acc[4][4] = {};
-    for (int64_t k0 = 0; k0 < K; k0 += 16) {
-        for (int idx = threadIdx.x; idx < 16 * 64; idx += 256) {
-            const int kk = idx / 64, mm = idx % 64;
-            const int64_t k = k0 + kk, i = m0 + mm, j = n0 + mm;
-            double av = 0.0, bv = 0.0;
-            if (k < K && i < M) av = (ta == 'N') ? A[i + k * lda] : A[k + i * lda];
-            if (k < K && j < N) bv = (tb == 'N') ? Bm[k + j * ldb] : Bm[j + k * ldb];
-            As[kk][mm] = av;
-            Bs[kk][mm] = bv;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-            double a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) { a[i] = As[kk][ty + 16 * i]; b[i] = Bs[kk][tx + 16 * i]; }
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
+    if (nv == 2 && ((uintptr_t)src & 15) == 0) {
+        cp_async16(dst, src, true);
+    } else {
+        cp_async8(dst, nv > 0 ? src : dst, nv > 0);
+        cp_async8(dst + 1, nv > 1 ? src + 1 : dst, nv > 1);
     }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int64_t r = m0 + ty + 16 * i, c = n0 + tx + 16 * j;
-            if (r >= M || c >= N) continue;
-            if (tri == 'L' && r < c) continue;
-            if (tri == 'U' && r > c) continue;
-            double *cp = &C[r + c * ldc];
-            *cp = (beta == 0.0 ? 0.0 : beta * *cp) + alpha * acc[i][j];
-        }
 }
+
+// rows x BK tile of an operand whose element (r, k) is X[r + k ldx] (KM:
+// contiguous in r -> k-major smem) or X[k + r ldx] (!KM: contiguous in k ->
+// r-major smem); rows [r0, r0 + 64) of nr, k in [k0, k0 + BK) of nk
+template <bool KM>
+LNB_DEV void load_op(double *dst, const double *X, int64_t ldx, int64_t r0, int64_t nr, int64_t k0, int64_t nk,
+                     int tid)
+{
+#pragma unroll
+    for (int it = 0; it < (BM * BK / 2) / THREADS; ++it) {
+        const int idx = tid + it * THREADS;
+        if (KM) {
+            const int kk = idx / (BM / 2), rr = (idx % (BM / 2)) * 2;
+            const int64_t r = r0 + rr, k = k0 + kk;
+            const int nv = k < nk ? (int)(r + 1 < nr ? 2 : (r < nr ? 1 : 0)) : 0;
+            load2(dst + kk * LDKM + rr, X + (nv ? r + k * ldx : 0), nv);
+        } else {
+            const int rr = idx / (BK / 2), kk = (idx % (BK / 2)) * 2;
+            const int64_t r = r0 + rr, k = k0 + kk;
+            const int nv = r < nr ? (int)(k + 1 < nk ? 2 : (k < nk ? 1 : 0)) : 0;
+            load2(dst + rr * LDMK + kk, X + (nv ? k + r * ldx : 0), nv);
+        }
+    }
+}
+
+// AKM: op(A) = A (k-major staging); BKM: op(B) = B^T (k-major staging)
+template <bool AKM, bool BKM>
+__global__ void __launch_bounds__(THREADS, 2) k_gemm_dmma(int64_t M, int64_t N, int64_t K, double alpha,
+                                                          const double *__restrict__ A, int64_t lda,
+                                                          const double *__restrict__ B, int64_t ldb, double beta,
+                                                          double *C, int64_t ldc, char tri)
+{
+    const int64_t m0 = (int64_t)blockIdx.y * BM, n0 = (int64_t)blockIdx.x * BN;
+    if (tri == 'L' && m0 + BM <= n0) return;
+    if (tri == 'U' && n0 + BN <= m0) return;
+    extern __shared__ __align__(16) double gsm[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp >> 1, wn = warp & 1, g = lane >> 2, t = lane & 3;
+    const int ktiles = (int)((K + BK - 1) / BK);
+    auto stage = [&](int s, int kt) {
+        double *as = gsm + (2 * s) * STAGE, *bs = gsm + (2 * s + 1) * STAGE;
+        load_op<AKM>(as, A, lda, m0, M, (int64_t)kt * BK, K, tid);
+        load_op<BKM>(bs, B, ldb, n0, N, (int64_t)kt * BK, K, tid);
+    };
+    double acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.0;
+#pragma unroll
+    for (int s = 0; s < ST - 1; ++s) {
+        if (s < ktiles) stage(s, s);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < ktiles; ++kt) {
+        cp_async_wait<ST - 2>();
+        __syncthreads();
+        {
+            const int nk = kt + ST - 1;
+            if (nk < ktiles) stage(nk % ST, nk);
+            cp_async_commit();
+        }
+        const double *as = gsm + (2 * (kt % ST)) * STAGE, *bs = gsm + (2 * (kt % ST) + 1) * STAGE;
+#pragma unroll
+        for (int kq = 0; kq < BK / 4; ++kq) {
+            const int k = kq * 4 + t;
+            double a0[2], a1[2], b0[4];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi) {
+                const int r = wm * 32 + mi * 16 + g;
+                a0[mi] = AKM ? as[k * LDKM + r] : as[r * LDMK + k];
+                a1[mi] = AKM ? as[k * LDKM + r + 8] : as[(r + 8) * LDMK + k];
+            }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) {
+                const int c = wn * 32 + ni * 8 + g;
+                b0[ni] = BKM ? bs[k * LDKM + c] : bs[c * LDMK + k];
+            }
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma16x8x4(acc[mi][ni], a0[mi], a1[mi], b0[ni]);
+        }
+    }
+    cp_async_wait<0>();
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int64_t r = m0 + wm * 32 + mi * 16 + g + (q >> 1) * 8;
+                const int64_t c = n0 + wn * 32 + ni * 8 + 2 * t + (q & 1);
+                if (r >= M || c >= N) continue;
+                if (tri == 'L' && r < c) continue;
+                if (tri == 'U' && r > c) continue;
+                double *cp = &C[r + c * ldc];
+                *cp = (beta == 0.0 ? 0.0 : beta * *cp) + alpha * acc[mi][ni][q];
+            }
+}
+}  // namespace gm
 
 }  // namespace lnb
 
@@ -416,13 +498,30 @@ extern "C" int lnb_k_syrk_lower_f64(const double *P, int64_t ldp, double *C, int
     }
 }
 
+template <bool AKM, bool BKM>
+static void launch_gemm(int64_t m, int64_t n, int64_t k, double alpha, const double *A, int64_t lda,
+                        const double *B, int64_t ldb, double beta, double *C, int64_t ldc, char tri, lnb_stream_t s)
+{
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(gm::k_gemm_dmma<AKM, BKM>, cudaFuncAttributeMaxDynamicSharedMemorySize, gm::SMEM);
+        attr = true;
+    }
+    dim3 grid((unsigned)((n + gm::BN - 1) / gm::BN), (unsigned)((m + gm::BM - 1) / gm::BM));
+    gm::k_gemm_dmma<AKM, BKM><<<grid, gm::THREADS, gm::SMEM, s>>>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc,
+                                                                  tri);
+}
+
 extern "C" int lnb_k_gemm_tri_f64(char ta, char tb, int64_t m, int64_t n, int64_t k, double alpha,
                                   const double *A, int64_t lda, const double *B, int64_t ldb,
                                   double beta, double *C, int64_t ldc, char tri, lnb_stream_t s)
 {
     if (m <= 0 || n <= 0) return 0;
-    dim3 grid((unsigned)((n + 63) / 64), (unsigned)((m + 63) / 64));
-    k_gemm_f64<<<grid, 256, 0, s>>>(ta, tb, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri);
+    const bool akm = ta == 'N', bkm = tb == 'T';
+    if (akm && bkm) launch_gemm<true, true>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri, s);
+    else if (akm) launch_gemm<true, false>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri, s);
+    else if (bkm) launch_gemm<false, true>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri, s);
+    else launch_gemm<false, false>(m, n, k, alpha, A, lda, B, ldb, beta, C, ldc, tri, s);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }

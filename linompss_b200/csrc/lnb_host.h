@@ -115,7 +115,7 @@ int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, in
                             const lnb_stream_in *in, lnb_arena *ar, cudaStream_t s);
 
 /* ---- FP64 triangular solves on device memory (lnb_solve.c) --------------- */
-size_t lnb_trsm_f64_ws_bytes(int64_t n);
+size_t lnb_trsm_f64_ws_bytes(int64_t n, int64_t nrhs);
 int lnb_trsm_f64_run(lnb_ctx *c, char uplo, char trans, char diag, int64_t n, int64_t nrhs,
                      double alpha, const double *dT, int64_t ldt, double *dB, int64_t ldb,
                      lnb_arena *ar, cudaStream_t s, const double *dinv_given);

@@ -6,8 +6,10 @@
  * (spdsolv_main.c:10-20) runs it twice, L Y = B then L^T X = Y.  Here each
  * solve is one persistent DAG-walking launch (k_trsv.cu) after one launch
  * that inverts the 64 x 64 diagonal blocks; the forward and the backward
- * solve share the inverses.
+ * solve share the inverses.  With many right-hand sides the solve is instead
+ * a sequence of DMMA GEMMs over 64-row blocks (trsm_gemm).
  */
+#include <stdlib.h>
 #include <string.h>
 
 #include "lnb_host.h"
@@ -22,11 +24,65 @@
 
 static inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
-size_t lnb_trsm_f64_ws_bytes(int64_t n)
+/* Two schedules for a solve: one persistent launch that walks the tile DAG,
+ * or a sequence of DMMA GEMMs over 64-row blocks.  The DAG walk costs about
+ * linearly in the right-hand sides; the GEMM sequence about 10 us per launch
+ * plus full-rate tiles.  Measured on B200 (m = 1024 .. 16384), the GEMM
+ * sequence wins from 128 - 256 columns on; auto switches at 192.  The GEMM
+ * path needs at least TRSM_GEMM_MIN_NRHS columns (its workspace). */
+#define TRSM_GEMM_MIN_NRHS 32
+#define TRSM_GEMM_AUTO_NRHS 192
+
+size_t lnb_trsm_f64_ws_bytes(int64_t n, int64_t nrhs)
 {
     const int64_t nb = ceil_div(n, TRSV_H);
     return lnb_align256((size_t)nb * TRSV_H * TRSV_H * sizeof(double)) +
-           lnb_align256((size_t)lnb_trsm_sync_ints(n, TRSV_H) * sizeof(int)) + 512;
+           lnb_align256((size_t)lnb_trsm_sync_ints(n, TRSV_H) * sizeof(int)) +
+           (nrhs >= TRSM_GEMM_MIN_NRHS ? lnb_align256((size_t)TRSV_H * nrhs * sizeof(double)) : 0) + 512;
+}
+
+static int trsm_use_gemm(int64_t n, int64_t nrhs)
+{
+    static int mode = -2;
+    if (mode == -2) {
+        const char *e = getenv("LNB_TRSM_GEMM");    /* 0: always the DAG walk, 1: the GEMM path from 32 columns */
+        mode = e ? atoi(e) : -1;
+    }
+    if (nrhs < TRSM_GEMM_MIN_NRHS || mode == 0) return 0;
+    return mode == 1 || nrhs >= TRSM_GEMM_AUTO_NRHS;
+}
+
+/* op(T) X = alpha B by 64-row blocks in dependency order, the blocked solve of
+ * bblas_dltrsm (bblas_trsm.h:119-160) with each TRSM task replaced by a
+ * product with the inverted diagonal block:
+ *     X_j = op(D_j) B_j                    (into tmp, then back into B_j)
+ *     B_r = B_r - op(T)_{r,j} X_j          (every block row r still to come)
+ * alpha enters through the first step: its diagonal product is scaled by
+ * alpha and its update scales the rows still to come (beta = alpha), so
+ * every later block already holds alpha B. */
+static int trsm_gemm(char uplo, char trans, int64_t n, int64_t nrhs, double alpha, const double *T, int64_t ldt,
+                     const double *dinv, double *B, int64_t ldb, double *tmp, cudaStream_t s)
+{
+    const int fwd = (uplo == 'L') == (trans == 'N');
+    const int64_t nb = ceil_div(n, TRSV_H);
+    for (int64_t q = 0; q < nb; ++q) {
+        const int64_t j = fwd ? q : nb - 1 - q;
+        const int64_t j0 = j * TRSV_H, jb = n - j0 < TRSV_H ? n - j0 : TRSV_H;
+        CK(lnb_k_gemm_tri_f64(trans, 'N', jb, nrhs, jb, q == 0 ? alpha : 1.0, dinv + j * TRSV_H * TRSV_H, TRSV_H,
+                              B + j0, ldb, 0.0, tmp, TRSV_H, 0, s), "diagonal block");
+        CK(cudaMemcpy2DAsync(B + j0, (size_t)ldb * 8, tmp, TRSV_H * 8, (size_t)jb * 8, nrhs, cudaMemcpyDeviceToDevice,
+                             s), "block back");
+        const int64_t r0 = fwd ? j0 + jb : 0, nr = fwd ? n - j0 - jb : j0;
+        if (nr <= 0) continue;
+        /* op(T)_{r,j}: stored at rows r, columns j (below the diagonal block
+         * for (L,N), above it for (U,N)); for trans 'T' it is the transpose of
+         * the block at rows j, columns r (left of the diagonal block for
+         * (L,T), right of it for (U,T)) */
+        const double *Ap = trans == 'N' ? T + r0 + j0 * ldt : T + j0 + r0 * ldt;
+        CK(lnb_k_gemm_tri_f64(trans, 'N', nr, nrhs, jb, -1.0, Ap, ldt, tmp, TRSV_H, q == 0 ? alpha : 1.0, B + r0, ldb,
+                              0, s), "update");
+    }
+    return 0;
 }
 
 /* op(T) X = alpha B with T triangular (uplo as stored), left side */
@@ -35,12 +91,21 @@ int lnb_trsm_f64_run(lnb_ctx *c, char uplo, char trans, char diag, int64_t n, in
                      lnb_arena *ar, cudaStream_t s, const double *dinv_given)
 {
     if (n <= 0 || nrhs <= 0) return 0;
+    if (alpha == 0.0) {                /* BLAS: B = 0, T not read */
+        CK(cudaMemset2DAsync(dB, (size_t)ldb * 8, 0, (size_t)n * 8, nrhs, s), "zero");
+        return 0;
+    }
     const int64_t nb = ceil_div(n, TRSV_H);
     double *dinv = (double *)dinv_given;
     if (!dinv) {
         dinv = (double *)lnb_arena_take(ar, (size_t)nb * TRSV_H * TRSV_H * sizeof(double));
         if (!dinv) return lnb_set_error(LNB_ENOMEM, "trsm workspace");
         CK(lnb_k_trtri_blocks_f64(dT, ldt, n, TRSV_H, uplo, diag == 'U', dinv, s), "trtri");
+    }
+    if (trsm_use_gemm(n, nrhs)) {
+        double *tmp = (double *)lnb_arena_take(ar, (size_t)TRSV_H * nrhs * sizeof(double));
+        if (!tmp) return lnb_set_error(LNB_ENOMEM, "trsm workspace");
+        return trsm_gemm(uplo, trans, n, nrhs, alpha, dT, ldt, dinv, dB, ldb, tmp, s);
     }
     int *sync = (int *)lnb_arena_take(ar, (size_t)lnb_trsm_sync_ints(n, TRSV_H) * sizeof(int));
     if (!sync) return lnb_set_error(LNB_ENOMEM, "trsm sync workspace");
@@ -57,7 +122,7 @@ int lnb_selftest_wait_timeout(long long wait_us)
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
     const int64_t n = 1024;
-    void *ws = lnb_ws(c, lnb_align256(n * n * 8) + lnb_align256(n * 8) + lnb_trsm_f64_ws_bytes(n));
+    void *ws = lnb_ws(c, lnb_align256(n * n * 8) + lnb_align256(n * 8) + lnb_trsm_f64_ws_bytes(n, 1));
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     double *T = lnb_arena_take(&ar, n * n * 8), *B = lnb_arena_take(&ar, n * 8);
@@ -92,7 +157,7 @@ int lnb_dtrsm_dev(char uplo, char trans, char diag, int m, int n, double alpha, 
     if (m == 0 || n == 0) return 0;
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
-    void *ws = lnb_ws(c, lnb_trsm_f64_ws_bytes(m));
+    void *ws = lnb_ws(c, lnb_trsm_f64_ws_bytes(m, n));
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     cudaStream_t s = (cudaStream_t)stream;
@@ -120,7 +185,7 @@ int lnb_dpotrs_dev(int n, int nrhs, const double *dL, int lda, double *dB, int l
     if (n == 0 || nrhs == 0) return 0;
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
-    void *ws = lnb_ws(c, lnb_trsm_f64_ws_bytes(n) + lnb_trsm_f64_ws_bytes(n));
+    void *ws = lnb_ws(c, 2 * lnb_trsm_f64_ws_bytes(n, nrhs));
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     cudaStream_t s = (cudaStream_t)stream;
@@ -145,7 +210,7 @@ int lnb_dposv_dev(int n, int nrhs, int b, double *dA, int lda, double *dB, int l
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
     const int64_t nb = ceil_div(n, TRSV_H);
-    void *ws = lnb_ws(c, lnb_chol_f64_ws_bytes(n, b) + 2 * lnb_trsm_f64_ws_bytes(n));
+    void *ws = lnb_ws(c, lnb_chol_f64_ws_bytes(n, b) + 2 * lnb_trsm_f64_ws_bytes(n, nrhs));
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     cudaStream_t s = (cudaStream_t)stream;
@@ -180,7 +245,7 @@ int dspdsolv_main(int m, int nrhs, int b, double *A, double *B)
     const int64_t ldd = ld_dev(m);
     const size_t abytes = (size_t)ldd * m * sizeof(double), bbytes = (size_t)ldd * (nrhs ? nrhs : 1) * sizeof(double);
     void *ws = lnb_ws(c, lnb_align256(abytes) + lnb_align256(bbytes) + lnb_chol_f64_ws_bytes(m, b) +
-                             2 * lnb_trsm_f64_ws_bytes(m));
+                             2 * lnb_trsm_f64_ws_bytes(m, nrhs));
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     double *dA = (double *)lnb_arena_take(&ar, abytes);
@@ -239,7 +304,7 @@ int ompss_dtrsm(ompssblas_t side, ompssblas_t uplo, ompssblas_t trans, ompssblas
     if (!c) return LNB_ENODEV;
     const int64_t ldd = ld_dev(m);
     const size_t abytes = (size_t)ldd * m * sizeof(double), bbytes = (size_t)ldd * n * sizeof(double);
-    void *ws = lnb_ws(c, lnb_align256(abytes) + lnb_align256(bbytes) + lnb_trsm_f64_ws_bytes(m));
+    void *ws = lnb_ws(c, lnb_align256(abytes) + lnb_align256(bbytes) + lnb_trsm_f64_ws_bytes(m, n));
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     double *dA = (double *)lnb_arena_take(&ar, abytes);

@@ -20,6 +20,8 @@
         if (_e != 0) return lnb_cuda_error(_e, where);             \
     } while (0)
 
+#define EVEN(m) ((((int64_t)(m)) + 1) & ~(int64_t)1)
+
 static int opt(const char *s, const char *allowed, char *out, const char *what)
 {
     if (!s || !s[0] || !strchr(allowed, s[0])) return lnb_set_error(LNB_EINVAL, "bad %s option", what);
@@ -97,18 +99,21 @@ int task_dgemm(ompssblas_t transa, ompssblas_t transb, int bm, int bn, int bk, d
         return lnb_set_error(LNB_EINVAL, "gemm leading dimensions");
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
-    const size_t sa = lnb_align256((size_t)am * (an ? an : 1) * 8), sb = lnb_align256((size_t)bmr * (bnc ? bnc : 1) * 8);
-    const size_t sc = lnb_align256((size_t)bm * bn * 8);
+    /* device copies with even leading dimensions: every column starts on a
+     * 16-byte boundary, as the kernel's 16-byte copies want */
+    const int64_t lda_d = EVEN(am), ldb_d = EVEN(bmr), ldc_d = EVEN(bm);
+    const size_t sa = lnb_align256((size_t)lda_d * (an ? an : 1) * 8), sb = lnb_align256((size_t)ldb_d * (bnc ? bnc : 1) * 8);
+    const size_t sc = lnb_align256((size_t)ldc_d * bn * 8);
     void *ws = lnb_ws(c, sa + sb + sc + 1024);
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     double *dA = lnb_arena_take(&ar, sa), *dB = lnb_arena_take(&ar, sb), *dC = lnb_arena_take(&ar, sc);
     cudaStream_t s = c->main;
-    if ((e = put(dA, am, A, lda, am, an, s)) || (e = put(dB, bmr, B, ldb, bmr, bnc, s)) ||
-        (e = put(dC, bm, C, ldc, bm, bn, s)))
+    if ((e = put(dA, lda_d, A, lda, am, an, s)) || (e = put(dB, ldb_d, B, ldb, bmr, bnc, s)) ||
+        (beta != 0.0 && (e = put(dC, ldc_d, C, ldc, bm, bn, s))))
         return e;
-    CK(lnb_k_gemm_tri_f64(ta, tb, bm, bn, bk, alpha, dA, am, dB, bmr, beta, dC, bm, 0, s), "gemm");
-    if ((e = get(C, ldc, dC, bm, bm, bn, s))) return e;
+    CK(lnb_k_gemm_tri_f64(ta, tb, bm, bn, bk, alpha, dA, lda_d, dB, ldb_d, beta, dC, ldc_d, 0, s), "gemm");
+    if ((e = get(C, ldc, dC, ldc_d, bm, bn, s))) return e;
     CK(cudaStreamSynchronize(s), "gemm sync");
     return 0;
 }
@@ -128,7 +133,8 @@ static int syrk_host(char u, char t, int n, int k, double alpha, const void *A, 
     if (!A || !C) return lnb_set_error(LNB_EINVAL, "syrk: NULL argument");
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
-    const size_t sa = lnb_align256((size_t)am * (an ? an : 1) * 8), sc = lnb_align256((size_t)n * n * 8);
+    const int64_t lda_d = EVEN(am), ldc_d = EVEN(n);    /* 16-byte aligned device columns */
+    const size_t sa = lnb_align256((size_t)lda_d * (an ? an : 1) * 8), sc = lnb_align256((size_t)ldc_d * n * 8);
     const size_t sa4 = single ? lnb_align256((size_t)am * (an ? an : 1) * 4) : 0;
     const size_t sc4 = single ? lnb_align256((size_t)n * n * 4) : 0;
     void *ws = lnb_ws(c, sa + sc + sa4 + sc4 + 1024);
@@ -140,24 +146,25 @@ static int syrk_host(char u, char t, int n, int k, double alpha, const void *A, 
     cudaStream_t s = c->main;
     int e;
     if (!single) {
-        if ((e = put(dA, am, (const double *)A, lda, am, an, s)) || (e = put(dC, n, (const double *)C, ldc, n, n, s)))
+        if ((e = put(dA, lda_d, (const double *)A, lda, am, an, s)) ||
+            (e = put(dC, ldc_d, (const double *)C, ldc, n, n, s)))
             return e;
     } else {
         if (am > 0 && an > 0) {
             CK(cudaMemcpy2DAsync(fA, (size_t)am * 4, A, (size_t)lda * 4, (size_t)am * 4, an, cudaMemcpyHostToDevice, s),
                "syrk A in");
-            CK(lnb_k_f32_to_f64(fA, am, am, an, dA, am, s), "widen A");
+            CK(lnb_k_f32_to_f64(fA, am, am, an, dA, lda_d, s), "widen A");
         }
         CK(cudaMemcpy2DAsync(fC, (size_t)n * 4, C, (size_t)ldc * 4, (size_t)n * 4, n, cudaMemcpyHostToDevice, s),
            "syrk C in");
-        CK(lnb_k_f32_to_f64(fC, n, n, n, dC, n, s), "widen C");
+        CK(lnb_k_f32_to_f64(fC, n, n, n, dC, ldc_d, s), "widen C");
     }
-    CK(lnb_k_gemm_tri_f64(t == 'N' ? 'N' : 'T', t == 'N' ? 'T' : 'N', n, n, k, alpha, dA, am, dA, am, beta, dC, n, u,
-                          s), "syrk");
+    CK(lnb_k_gemm_tri_f64(t == 'N' ? 'N' : 'T', t == 'N' ? 'T' : 'N', n, n, k, alpha, dA, lda_d, dA, lda_d, beta, dC,
+                          ldc_d, u, s), "syrk");
     if (!single) {
-        if ((e = get((double *)C, ldc, dC, n, n, n, s))) return e;
+        if ((e = get((double *)C, ldc, dC, ldc_d, n, n, s))) return e;
     } else {
-        CK(lnb_k_f64_to_f32(dC, n, n, n, fC, n, s), "narrow C");
+        CK(lnb_k_f64_to_f32(dC, ldc_d, n, n, fC, n, s), "narrow C");
         CK(cudaMemcpy2DAsync(C, (size_t)ldc * 4, fC, (size_t)n * 4, (size_t)n * 4, n, cudaMemcpyDeviceToHost, s),
            "syrk C out");
     }
@@ -211,7 +218,7 @@ int task_dtrsm(ompssblas_t side, ompssblas_t uplo, ompssblas_t trans, ompssblas_
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
     const size_t sa = lnb_align256((size_t)na * na * 8), sb = lnb_align256((size_t)bm * bn * 8);
-    void *ws = lnb_ws(c, sa + sb + lnb_trsm_f64_ws_bytes(na) + 1024);
+    void *ws = lnb_ws(c, sa + sb + lnb_trsm_f64_ws_bytes(na, sd == 'L' ? bn : bm) + 1024);
     if (!ws) return LNB_ENOMEM;
     lnb_arena ar = {(char *)ws, 0, c->ws_size};
     double *dA = lnb_arena_take(&ar, sa), *dB = lnb_arena_take(&ar, sb);
@@ -240,4 +247,39 @@ int task_dtrsm(ompssblas_t side, ompssblas_t uplo, ompssblas_t trans, ompssblas_
     }
     e = lnb_status_read(c, s);
     return e < 0 ? e : 0;
+}
+
+int lnb_dgemm_dev(char transa, char transb, int m, int n, int k, double alpha, const double *dA, int lda,
+                  const double *dB, int ldb, double beta, double *dC, int ldc, void *stream)
+{
+    if ((transa != 'N' && transa != 'T') || (transb != 'N' && transb != 'T'))
+        return lnb_set_error(LNB_EINVAL, "dgemm options");
+    if (m < 0 || n < 0 || k < 0) return lnb_set_error(LNB_EINVAL, "dgemm sizes");
+    const int am = transa == 'N' ? m : k, br = transb == 'N' ? k : n;
+    if (lda < (am > 1 ? am : 1) || ldb < (br > 1 ? br : 1) || ldc < (m > 1 ? m : 1))
+        return lnb_set_error(LNB_EINVAL, "dgemm leading dimensions");
+    if (m == 0 || n == 0) return 0;
+    if (!dC || (k > 0 && (!dA || !dB))) return lnb_set_error(LNB_EINVAL, "dgemm: NULL argument");
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    CK(lnb_k_gemm_tri_f64(transa, transb, m, n, k, alpha, dA, lda, dB, ldb, beta, dC, ldc, 0,
+                          (cudaStream_t)stream), "dgemm");
+    return 0;
+}
+
+int lnb_dsyrk_dev(char uplo, char trans, int n, int k, double alpha, const double *dA, int lda, double beta,
+                  double *dC, int ldc, void *stream)
+{
+    if ((uplo != 'L' && uplo != 'U') || (trans != 'N' && trans != 'T'))
+        return lnb_set_error(LNB_EINVAL, "dsyrk options");
+    if (n < 0 || k < 0) return lnb_set_error(LNB_EINVAL, "dsyrk sizes");
+    const int am = trans == 'N' ? n : k;
+    if (lda < (am > 1 ? am : 1) || ldc < (n > 1 ? n : 1)) return lnb_set_error(LNB_EINVAL, "dsyrk leading dimensions");
+    if (n == 0) return 0;
+    if (!dC || (k > 0 && !dA)) return lnb_set_error(LNB_EINVAL, "dsyrk: NULL argument");
+    lnb_ctx *c = lnb_ctx_get();
+    if (!c) return LNB_ENODEV;
+    CK(lnb_k_gemm_tri_f64(trans == 'N' ? 'N' : 'T', trans == 'N' ? 'T' : 'N', n, n, k, alpha, dA, lda, dA, lda, beta,
+                          dC, ldc, uplo, (cudaStream_t)stream), "dsyrk");
+    return 0;
 }
