@@ -10,8 +10,10 @@
 //
 //   * Work items are 64 KB slabs: 64 rows x 256 columns (forward) or 256 rows
 //     x 64 columns (backward) of an HB x HB block (16 items per block), each
-//     brought into shared memory by ONE 2D TMA box issued before the item waits
-//     for its input vector.  An item multiplies its slab by a vector segment and
+//     brought into shared memory by 2 (forward) or 8 (backward) 2D TMA boxes
+//     of 128-byte swizzled rows on one mbarrier, issued before the item waits
+//     for its input vector.  An item multiplies its slab by a segment of up to
+//     8 vectors on the FP64 tensor cores (DMMA, FP32 widened as it loads) and
 //     adds the product into a target segment with FP64 atomics, then bumps a
 //     counter: the residual counter of the target block row (update items,
 //     L_sj y_j or L_js^T x_j) or the solution counter of the step (diagonal
@@ -105,18 +107,42 @@ LNB_DEV void drain(uint64_t *bar, uint32_t parity, long long wait_ns)
     }
 }
 
-template <int NR>
-__global__ void __launch_bounds__(NTHR, 2) k_trsm_blk(Args a, const __grid_constant__ CUtensorMap mT,
-                                                        const __grid_constant__ CUtensorMap mI)
+// Slab layout.  The slab arrives as boxes of 32 floats along its contiguous
+// (inner) index r, written by TMA with the 128-byte swizzle: box r / 32,
+// then one 128-byte row per outer index c, 16-byte chunk (r % 32) / 4 stored
+// at chunk position ((r % 32) / 4) ^ (c % 8).  OUTER = 256 (forward: r = the
+// 64 outputs, c = the 256 inputs) or 64 (backward: r = the 256 inputs, c =
+// the 64 outputs).  With the swizzle the backward A fragments are free of
+// bank conflicts and the forward ones 2-way.
+template <int OUTER>
+LNB_DEV int soff(int r, int c)
 {
-    extern __shared__ __align__(128) float sm[];
-    float *slab = sm;                                             // 64 KB, TMA destination
-    double *vs = reinterpret_cast<double *>(sm + SLAB);           // [NR][256] input segment
-    double *red = vs + NR * 256;                                  // [4][NR][64] partial sums
+    return (r >> 5) * (32 * OUTER) + c * 32 + ((((r & 31) >> 2) ^ (c & 7)) << 2) + (r & 3);
+}
+// x segment element (k, q), 8 columns per row, swizzled so that the B
+// fragment loads (rows 4kk + t, column g) are free of bank conflicts
+LNB_DEV int voff(int k, int q) { return k * 8 + (q ^ (((k >> 1) & 1) << 2)); }
+
+constexpr int RED_DOUBLES = 64 * 8;
+constexpr int BLK_SMEM = 1024 + SLAB * 4 + 256 * 8 * 8 + RED_DOUBLES * 8;
+
+// Item product on the FP64 tensor cores: out (64 x 8) = S (64 x 256) v (256 x 8),
+// S = the slab (forward) or its transpose (backward), FP32 widened as the
+// fragments load.  Warp w takes output rows 16 (w % 4) .. +15 over inputs
+// 128 (w / 4) .. +127 (32 DMMAs); the two input halves meet in shared memory.
+__global__ void __launch_bounds__(NTHR, 2) k_trsm_blk(Args a, const __grid_constant__ CUtensorMap mT,
+                                                      const __grid_constant__ CUtensorMap mI)
+{
+    extern __shared__ __align__(16) unsigned char smb[];
+    // TMA with the 128-byte swizzle writes to 1024-byte aligned boxes
+    const uint32_t base = smem_u32(smb);
+    float *slab = reinterpret_cast<float *>(smb + (((base + 1023u) & ~1023u) - base));
+    double *vs = reinterpret_cast<double *>(slab + SLAB);          // [256][8] input segment (voff)
+    double *red = vs + 256 * 8;                                    // [64][8] partial sums
     __shared__ __align__(8) uint64_t full;
     __shared__ int s_t, s_ok;
     __shared__ volatile int s_abort;     // stays 0: nothing else cuts the slab wait short
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, t4 = lane & 3;
     if (tid == 0) {
         s_abort = 0;
         tc::mbar_init(&full, 1);
@@ -139,14 +165,21 @@ __global__ void __launch_bounds__(NTHR, 2) k_trsm_blk(Args a, const __grid_const
         const int64_t out0 = (int64_t)it.row * a.hb + 64 * po;
         if (tid == 0) {
             tc::mbar_arrive_expect_tx(&full, SLAB * 4);
+            const CUtensorMap *m = it.kind == 0 ? &mI : &mT;
+            // diagonal items read block s of the inverses (rows 0..HB-1 of
+            // column block s), updates L_{row, col} (forward) or L_{col, row}
+            int x0, y0;
             if (it.kind == 0) {
-                // diagonal block s of the inverses: rows 0..HB-1 of column block s
-                if (a.fwd) tc::tma_load_2d(slab, &mI, &full, 64 * po, it.row * a.hb + 256 * pi);
-                else tc::tma_load_2d(slab, &mI, &full, 256 * pi, it.row * a.hb + 64 * po);
+                x0 = a.fwd ? 64 * po : 256 * pi;
+                y0 = it.row * a.hb + (a.fwd ? 256 * pi : 64 * po);
             } else {
-                // L_{row, col} (forward) or L_{col, row} (backward) of the factor
-                if (a.fwd) tc::tma_load_2d(slab, &mT, &full, (int)out0, (int)in0);
-                else tc::tma_load_2d(slab, &mT, &full, (int)in0, (int)out0);
+                x0 = a.fwd ? (int)out0 : (int)in0;
+                y0 = a.fwd ? (int)in0 : (int)out0;
+            }
+            if (a.fwd) {
+                for (int b = 0; b < 2; ++b) tc::tma_load_2d(slab + b * 32 * 256, m, &full, x0 + 32 * b, y0);
+            } else {
+                for (int b = 0; b < 8; ++b) tc::tma_load_2d(slab + b * 32 * 64, m, &full, x0 + 32 * b, y0);
             }
             // the input: a solution segment (updates) or a finished residual (diagonal)
             bool ok;
@@ -165,9 +198,9 @@ __global__ void __launch_bounds__(NTHR, 2) k_trsm_blk(Args a, const __grid_const
             break;
         }
         const double *src = it.kind == 1 ? a.Y : a.R;
-        for (int i = tid; i < NR * 256; i += NTHR) {
+        for (int i = tid; i < 8 * 256; i += NTHR) {
             const int q = i >> 8, c = i & 255;
-            vs[i] = q < a.nrhs ? __ldcg(src + in0 + c + (int64_t)q * a.np) : 0.0;
+            vs[voff(c, q)] = q < a.nrhs ? __ldcg(src + in0 + c + (int64_t)q * a.np) : 0.0;
         }
         if (tid == 0 && !tc::mbar_wait(&full, phase, a.wait_ns, &s_abort, a.st)) {
             if (atomicCAS(&a.st->timeout, 0, 43) == 0) a.st->timeout_item = (int)t;
@@ -176,54 +209,44 @@ __global__ void __launch_bounds__(NTHR, 2) k_trsm_blk(Args a, const __grid_const
         __syncthreads();
         phase ^= 1;
         if (!s_ok) break;
-        double acc[NR];
-#pragma unroll
-        for (int q = 0; q < NR; ++q) acc[q] = 0.0;
+        const int m16 = (warp & 3) * 16, k00 = (warp >> 2) * 128;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
         if (a.fwd) {
-            // slab[c * 64 + r]: out[r] = sum_c slab[r][c] v[c]; thread (r, cq) takes columns cq, cq+4, ...
-            const int r = tid & 63, cq = tid >> 6;
-#pragma unroll 4
-            for (int c = cq; c < 256; c += 4) {
-                const double l = (double)slab[c * 64 + r];
-#pragma unroll
-                for (int q = 0; q < NR; ++q) acc[q] = fma(l, vs[q * 256 + c], acc[q]);
-            }
-#pragma unroll
-            for (int q = 0; q < NR; ++q) red[(cq * NR + q) * 64 + r] = acc[q];
-            __syncthreads();
-            for (int i = tid; i < 64 * NR; i += NTHR) {
-                const int q = i >> 6, rr = i & 63;
-                const double v = red[(0 * NR + q) * 64 + rr] + red[(1 * NR + q) * 64 + rr] +
-                                 red[(2 * NR + q) * 64 + rr] + red[(3 * NR + q) * 64 + rr];
-                if (q < a.nrhs) atomicAdd((it.kind == 1 ? a.R : a.Y) + out0 + rr + (int64_t)q * a.np,
-                                          it.kind == 1 ? -v : v);
+#pragma unroll 8
+            for (int kk = 0; kk < 32; ++kk) {
+                const int k = k00 + 4 * kk + t4;
+                const double a0 = (double)slab[soff<256>(m16 + g, k)];
+                const double a1 = (double)slab[soff<256>(m16 + g + 8, k)];
+                dmma16x8x4(acc, a0, a1, vs[voff(k, g)]);
             }
         } else {
-            // slab[c * 256 + r]: out[c] = sum_r slab[r][c] v[r]; warp w takes columns 8w..8w+7
-            const int lane = tid & 31, w = tid >> 5;
-            for (int cc = 0; cc < 8; ++cc) {
-                const int c = 8 * w + cc;
-                double s[NR];
-#pragma unroll
-                for (int q = 0; q < NR; ++q) s[q] = 0.0;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const int r = lane + 32 * k;
-                    const double l = (double)slab[c * 256 + r];
-#pragma unroll
-                    for (int q = 0; q < NR; ++q) s[q] = fma(l, vs[q * 256 + r], s[q]);
-                }
-#pragma unroll
-                for (int q = 0; q < NR; ++q) {
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) s[q] += __shfl_down_sync(0xffffffffu, s[q], o);
-                }
-                if (lane == 0) {
-#pragma unroll
-                    for (int q = 0; q < NR; ++q)
-                        if (q < a.nrhs) atomicAdd((it.kind == 1 ? a.R : a.Y) + out0 + c + (int64_t)q * a.np,
-                                                  it.kind == 1 ? -s[q] : s[q]);
-                }
+#pragma unroll 8
+            for (int kk = 0; kk < 32; ++kk) {
+                const int k = k00 + 4 * kk + t4;
+                const double a0 = (double)slab[soff<64>(k, m16 + g)];
+                const double a1 = (double)slab[soff<64>(k, m16 + g + 8)];
+                dmma16x8x4(acc, a0, a1, vs[voff(k, g)]);
+            }
+        }
+        // C fragment: rows m16 + g (+8), columns 2 t4 (+1)
+        const int ra = m16 + g, rb = ra + 8, q0 = 2 * t4, q1 = q0 + 1;
+        if (warp >= 4) {
+            red[ra * 8 + q0] = acc[0];
+            red[ra * 8 + q1] = acc[1];
+            red[rb * 8 + q0] = acc[2];
+            red[rb * 8 + q1] = acc[3];
+        }
+        __syncthreads();
+        if (warp < 4) {
+            double *dst = (it.kind == 1 ? a.R : a.Y) + out0;
+            const double sg = it.kind == 1 ? -1.0 : 1.0;
+            if (q0 < a.nrhs) {
+                atomicAdd(dst + ra + (int64_t)q0 * a.np, sg * (acc[0] + red[ra * 8 + q0]));
+                atomicAdd(dst + rb + (int64_t)q0 * a.np, sg * (acc[2] + red[rb * 8 + q0]));
+            }
+            if (q1 < a.nrhs) {
+                atomicAdd(dst + ra + (int64_t)q1 * a.np, sg * (acc[1] + red[ra * 8 + q1]));
+                atomicAdd(dst + rb + (int64_t)q1 * a.np, sg * (acc[3] + red[rb * 8 + q1]));
             }
         }
         // publish: every thread's atomics, then one GPU-scope release of the counter
@@ -353,7 +376,8 @@ typedef CUresult (*EncodeTiledFnB)(CUtensorMap *, CUtensorMapDataType, cuuint32_
                                    const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-// FP32 rows x cols column-major (ld elements) as a 2D tensor map with bx x by boxes
+// FP32 rows x cols column-major (ld elements) as a 2D tensor map with bx x by
+// boxes (bx = 32 floats = 128 bytes), written with the 128-byte swizzle
 static int map2d(CUtensorMap *m, const void *base, int64_t rows, int64_t cols, int64_t ld, int bx, int by)
 {
     static EncodeTiledFnB fn = nullptr;
@@ -370,19 +394,17 @@ static int map2d(CUtensorMap *m, const void *base, int64_t rows, int64_t cols, i
     cuuint32_t box[2] = {(cuuint32_t)bx, (cuuint32_t)by};
     cuuint32_t estr[2] = {1, 1};
     const CUresult r = fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void *>(base), dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? 0 : -1;
 }
 
-template <int NR>
 static int launch(const Args &a, const CUtensorMap &mT, const CUtensorMap &mI, int sms, cudaStream_t s)
 {
-    const int smem = SLAB * 4 + NR * 256 * 8 + 4 * NR * 64 * 8;
-    cudaError_t e = cudaFuncSetAttribute(k_trsm_blk<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(k_trsm_blk, cudaFuncAttributeMaxDynamicSharedMemorySize, BLK_SMEM);
     if (e != cudaSuccess) return (int)e;
     const int grid = a.nitems < 2 * sms ? a.nitems : 2 * sms;
-    k_trsm_blk<NR><<<grid, NTHR, smem, s>>>(a, mT, mI);
+    k_trsm_blk<<<grid, NTHR, BLK_SMEM, s>>>(a, mT, mI);
     return (int)cudaGetLastError();
 }
 
@@ -461,8 +483,8 @@ extern "C" int lnb_k_trsm_blk_f32(char trans, int64_t n, int64_t nrhs, const flo
     CUtensorMap mT, mI;
     memset(&mT, 0, sizeof mT);
     memset(&mI, 0, sizeof mI);
-    // forward items read 64 x 256 boxes, backward 256 x 64
-    const int bx = a.fwd ? 64 : 256, by = a.fwd ? 256 : 64;
+    // forward items read 2 boxes of 32 x 256, backward 8 boxes of 32 x 64
+    const int bx = 32, by = a.fwd ? 256 : 64;
     if (map2d(&mT, T, n, n, ldt, bx, by) || map2d(&mI, Binv, a.hb, a.np, a.hb, bx, by))
         return (int)cudaErrorInvalidValue;
     cudaStream_t cs = (cudaStream_t)s;
@@ -470,11 +492,7 @@ extern "C" int lnb_k_trsm_blk_f32(char trans, int64_t n, int64_t nrhs, const flo
     if (e != cudaSuccess) return (int)e;
     const dim3 vg((unsigned)((a.np + 255) / 256 < 256 ? (a.np + 255) / 256 : 256), (unsigned)nrhs);
     k_blk_pack<<<vg, 256, 0, cs>>>(B, ldb, n, a.np, (int)nrhs, a.R, a.Y);
-    int err;
-    if (nrhs <= 1) err = launch<1>(a, mT, mI, sms, cs);
-    else if (nrhs <= 2) err = launch<2>(a, mT, mI, sms, cs);
-    else if (nrhs <= 4) err = launch<4>(a, mT, mI, sms, cs);
-    else err = launch<8>(a, mT, mI, sms, cs);
+    const int err = launch(a, mT, mI, sms, cs);
     if (err) return err;
     k_blk_unpack<<<vg, 256, 0, cs>>>(a.Y, n, a.np, B, ldb);
     lnb_prof_count(3);
