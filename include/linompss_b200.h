@@ -260,6 +260,30 @@ LNB_EXPORT int lnb_dsyrk_dev(char uplo, char trans, int n, int k, double alpha, 
 LNB_EXPORT int lnb_dsymv_dev(int n, int nrhs, const double *dA, int lda, const double *dX, double *dY,
                              void *stream);
 
+/* ---- tile LU with partial pivoting and the general solve ----------------- */
+/* ompss_dgetrf (ompss_lu.h:19, dlu_main lu_main.c:5-27): P A = L U in place,
+ * A m x n column-major (ld lda), b the panel width of the pivot convention.
+ * IPIV (min(m, n) ints) receives the reference's convention: for the b-wide
+ * panel starting at row j, IPIV[j + k] is the pivot row of column j + k,
+ * 1-based and relative to row j (LAPACK dgetrf's output for the panel).
+ * Returns 0, or the 1-based column of the first exactly zero pivot (LAPACK
+ * info; the factorization completes); < 0 on error.  The reference's
+ * functions return void.  The _ll drivers (ompss_lu.h:23-25) give the same
+ * factorization.  s*: FP32 arrays, computed in FP64 on the device. */
+LNB_EXPORT int ompss_dgetrf(int m, int n, int b, double *A, int lda, int *IPIV);
+LNB_EXPORT int ompss_sgetrf(int m, int n, int b, float *A, int lda, int *IPIV);
+LNB_EXPORT int ompss_dgetrf_ll(int m, int n, int b, double *A, int lda, int *IPIV);
+LNB_EXPORT int ompss_sgetrf_ll(int m, int n, int b, float *A, int lda, int *IPIV);
+/* dgensolv_main (gensolv_main.h, gensolv_main.c:10-25): A (m x m, ld m) -> its
+ * LU factors, B (m x n, ld m) -> A^-1 B. */
+LNB_EXPORT int dgensolv_main(int m, int n, int b, double *A, double *B);
+LNB_EXPORT int sgensolv_main(int m, int n, int b, float *A, float *B);
+/* device forms: dipiv receives LAPACK pivots (1-based, global rows);
+ * info_dev (may be NULL) the info value; asynchronous on `stream` */
+LNB_EXPORT int lnb_dgetrf_dev(int m, int n, double *dA, int lda, int *dipiv, int *info_dev, void *stream);
+LNB_EXPORT int lnb_dgetrs_dev(int n, int nrhs, const double *dLU, int lda, const int *dipiv, double *dB, int ldb,
+                              void *stream);
+
 /* ======================================================================== */
 /* 3. Mixed precision: low-precision factor + FP64 iterative refinement       */
 /* ======================================================================== */

@@ -317,6 +317,43 @@ def dpotrs_dev(Lt, Bt, n: int, nrhs: int, which: str = "B", stream=None) -> int:
                                      C.c_int(_ld(Bt)), C.c_char(which.encode()), _stream(stream)))
 
 
+def ompss_getrf(A, b: int, ll: bool = False) -> tuple:
+    """P A = L U in place (ompss_dgetrf / ompss_sgetrf by A's dtype, column-major); returns (info, IPIV) with the
+    reference's panel-relative pivots"""
+    _colmajor(A)
+    m, n = A.shape
+    single = A.dtype == np.float32
+    name = ("ompss_sgetrf" if single else "ompss_dgetrf") + ("_ll" if ll else "")
+    f = getattr(lib(), name)
+    f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+    ipiv = np.zeros(max(min(m, n), 1), dtype=np.int32)
+    info = _chk(f(m, n, b, _p(A), m, _p(ipiv)))
+    return info, ipiv[:min(m, n)]
+
+
+def gensolv(A, B, b: int) -> int:
+    """dgensolv_main / sgensolv_main: A (m x m) -> LU, B (m x n) -> A^-1 B, in place, column-major"""
+    _colmajor(A)
+    _colmajor(B)
+    m, n = B.shape
+    single = A.dtype == np.float32
+    f = lib().sgensolv_main if single else lib().dgensolv_main
+    f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    return _chk(f(m, n, b, _p(A), _p(B)))
+
+
+def dgetrf_dev(At, m: int, n: int, ipiv_dev, info=None, stream=None) -> int:
+    f = lib().lnb_dgetrf_dev
+    f.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    return _chk(f(m, n, _p(At), _ld(At), _p(ipiv_dev), _p(info), _stream(stream)))
+
+
+def dgetrs_dev(LUt, ipiv_dev, Bt, n: int, nrhs: int, stream=None) -> int:
+    f = lib().lnb_dgetrs_dev
+    f.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    return _chk(f(n, nrhs, _p(LUt), _ld(LUt), _p(ipiv_dev), _p(Bt), _ld(Bt), _stream(stream)))
+
+
 def dgemm_dev(transa: str, transb: str, m: int, n: int, k: int, alpha: float, At, Bt, beta: float, Ct,
               stream=None) -> int:
     """C = alpha op(A) op(B) + beta C on device tensors (column-major as (cols, ld))."""

@@ -309,6 +309,115 @@ int orc_dspdsolv(int64_t m, int64_t nrhs, int64_t b, double *A, double *B)
 }
 
 /* ------------------------------------------------------------------------ */
+/* Tile LU with partial pivoting (lu_main.c:5-27, lu_kernels.c:5-33) and the  */
+/* general solve (gensolv_main.c:10-25)                                      */
+/* ------------------------------------------------------------------------ */
+
+/* TASK_GETRF (lu_kernels.c:5-10) is LAPACK dgetrf on the (m-j) x dimC panel,
+ * restated unblocked (dgetf2): the pivot of column k is the first row of
+ * largest |a| at or below k; rows k and p swap across the panel; the column
+ * below the pivot is divided by it (skipped when it is exactly zero, which
+ * sets info = k + 1); the rank-1 update follows.  ipiv is 1-based and
+ * relative to the panel's first row, as dgetrf returns it for the panel. */
+static int getf2(int64_t m, int64_t n, double *A, int64_t lda, int *ipiv)
+{
+    int info = 0;
+    const int64_t mn = min64(m, n);
+    for (int64_t k = 0; k < mn; ++k) {
+        int64_t p = k;
+        double amax = fabs(A[IDX(k, k, lda)]);
+        for (int64_t i = k + 1; i < m; ++i) {
+            const double v = fabs(A[IDX(i, k, lda)]);
+            if (v > amax) { amax = v; p = i; }
+        }
+        ipiv[k] = (int)(p + 1);
+        if (A[IDX(p, k, lda)] != 0.0) {
+            if (p != k)
+                for (int64_t j = 0; j < n; ++j) {
+                    const double t = A[IDX(k, j, lda)];
+                    A[IDX(k, j, lda)] = A[IDX(p, j, lda)];
+                    A[IDX(p, j, lda)] = t;
+                }
+            for (int64_t i = k + 1; i < m; ++i) A[IDX(i, k, lda)] /= A[IDX(k, k, lda)];
+        } else if (!info) {
+            info = (int)(k + 1);
+        }
+        for (int64_t j = k + 1; j < n; ++j) {
+            const double u = A[IDX(k, j, lda)];
+            for (int64_t i = k + 1; i < m; ++i) A[IDX(i, j, lda)] -= A[IDX(i, k, lda)] * u;
+        }
+    }
+    return info;
+}
+
+/* LAPACK dlaswp on ncols columns: rows k and ipiv[k]-1 swap for k = k1..k2-1 */
+static void laswp(int64_t ncols, double *A, int64_t lda, int64_t k1, int64_t k2, const int *ipiv)
+{
+    for (int64_t k = k1; k < k2; ++k) {
+        const int64_t p = ipiv[k] - 1;
+        if (p == k) continue;
+        for (int64_t j = 0; j < ncols; ++j) {
+            const double t = A[IDX(k, j, lda)];
+            A[IDX(k, j, lda)] = A[IDX(p, j, lda)];
+            A[IDX(p, j, lda)] = t;
+        }
+    }
+}
+
+/* dlu_main (lu_main.c:5-27), m >= n: for each panel j of width dimC, getrf on
+ * rows j..m-1; its swaps applied to dimC columns of every block column on the
+ * left (TASK_LASWP: the reference passes the panel's width as the column
+ * count, so with a ragged last panel the earlier blocks' columns past dimC are
+ * not swapped); each block column on the right takes the swaps, a unit-lower
+ * TRSM with the panel's top block and a GEMM with the rest of the panel
+ * (TASK_TRSM_GEMM, lu_kernels.c:18-30).  ipiv[j..j+dimC) holds the panel's
+ * pivots, 1-based and relative to row j.  Returns the first exactly zero
+ * pivot's global column (1-based) or 0. */
+int orc_dgetrf(int64_t m, int64_t n, int64_t b, double *A, int64_t lda, int *ipiv)
+{
+    int info = 0;
+    for (int64_t j = 0; j < n; j += b) {
+        const int64_t dimC = min64(b, n - j), dimR = m - j;
+        if (dimR <= 0) break;
+        int *ip = &ipiv[j];
+        const int e = getf2(dimR, dimC, &A[IDX(j, j, lda)], lda, ip);
+        if (e && !info) info = (int)(j + e);
+        const int64_t ips = min64(dimR, dimC);
+        for (int64_t jj = 0; jj < j; jj += b) laswp(dimC, &A[IDX(j, jj, lda)], lda, 0, ips, ip);
+        for (int64_t jj = j + dimC; jj < n; jj += b) {
+            const int64_t dimM = min64(b, n - jj);
+            laswp(dimM, &A[IDX(j, jj, lda)], lda, 0, ips, ip);
+            orc_dtrsm('L', 'L', 'N', 'U', dimC, dimM, 1.0, &A[IDX(j, j, lda)], lda, &A[IDX(j, jj, lda)], lda);
+            orc_dgemm('N', 'N', dimR - dimC, dimM, dimC, -1.0, &A[IDX(j + dimC, j, lda)], lda, &A[IDX(j, jj, lda)],
+                      lda, 1.0, &A[IDX(j + dimC, jj, lda)], lda);
+        }
+    }
+    return info;
+}
+
+/* dgensolv_main (gensolv_main.c:10-25): A (m x m) = P L U by dlu_main; the
+ * panels' swaps applied to B (m x n); then the blocked unit-lower and upper
+ * solves.  As executed: the swap loop runs over i < n in steps of b and
+ * applies panel i's pivots (relative to row i) starting at row b
+ * (TASK_LASWP(b, ...)), which is where they belong only for i = b.  On the
+ * reference's matrices (a +100 diagonal) no pivot leaves its row and the
+ * swaps are all no-ops. */
+int orc_dgensolv(int64_t m, int64_t n, int64_t b, double *A, double *B)
+{
+    int *ipiv = (int *)malloc(sizeof(int) * (size_t)(m > n ? m : n));
+    if (!ipiv) return -1;
+    const int info = orc_dgetrf(m, m, b, A, m, ipiv);
+    for (int64_t i = 0; i < n; i += b) {
+        const int64_t dim = min64(b, n - i);
+        laswp(n, &B[IDX(b, 0, m)], m, 0, dim, &ipiv[i]);
+    }
+    orc_dltrsm('L', 'N', 'U', b, m, n, 1.0, A, m, B, m);
+    orc_dltrsm('U', 'N', 'N', b, m, n, 1.0, A, m, B, m);
+    free(ipiv);
+    return info;
+}
+
+/* ------------------------------------------------------------------------ */
 /* Iterative refinement (itref.c)                                             */
 /* ------------------------------------------------------------------------ */
 

@@ -69,6 +69,8 @@ void orc_dltrsm(char uplo, char trans, char diag, int64_t bm, int64_t m, int64_t
 /* dspdsolv_main (spdsolv_main.c:10-20): chol_rl then the two blocked solves.
  * A is m x m (ld = m), B is m x nrhs (ld = m). */
 int orc_dspdsolv(int64_t m, int64_t nrhs, int64_t b, double *A, double *B);
+int orc_dgetrf(int64_t m, int64_t n, int64_t b, double *A, int64_t lda, int *ipiv);
+int orc_dgensolv(int64_t m, int64_t n, int64_t b, double *A, double *B);
 
 /* Dense FP64 CG of dcg_pure (itref.c:690-925, non-preconditioned dense
  * branch, s = 1).  x holds the start vector on entry, the iterate on exit.

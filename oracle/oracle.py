@@ -135,6 +135,43 @@ def spdsolv(A: np.ndarray, B: np.ndarray, b: int) -> int:
     return lib().orc_dspdsolv(_i64(m), _i64(nrhs), _i64(b), _ptr(A), _ptr(B))
 
 
+def getrf(A: np.ndarray, b: int):
+    """dlu_main restated (orc_dgetrf), A (m x n, m >= n, column-major) in place; returns (info, ipiv) with
+    the reference's pivots: 1-based, relative to the first row of each b-wide panel"""
+    m, n = A.shape
+    ipiv = np.zeros(max(m, n), dtype=np.int32)
+    info = lib().orc_dgetrf(_i64(m), _i64(n), _i64(b), _ptr(A), _i64(m), ipiv.ctypes.data_as(C.c_void_p))
+    return info, ipiv[:min(m, n)]
+
+
+def gensolv(A: np.ndarray, B: np.ndarray, b: int) -> int:
+    """dgensolv_main restated (orc_dgensolv): A -> LU, B -> X, in place"""
+    m, n = B.shape
+    return lib().orc_dgensolv(_i64(m), _i64(n), _i64(b), _ptr(A), _ptr(B))
+
+
+def genmat_ip(m: int, n: int, seed: int, scale: float = 100.0) -> np.ndarray:
+    """GENMAT_IP (genmat.c:131-144) with a seeded generator: uniform [0, 1) entries plus `scale` on the
+    diagonal, the distribution of the reference's LU and gensolv programs"""
+    A = np.random.default_rng(seed).random((m, n))
+    k = min(m, n)
+    A[np.arange(k), np.arange(k)] += scale
+    return np.asfortranarray(A)
+
+
+def lu_unpack(LU: np.ndarray, ipiv_local: np.ndarray, b: int):
+    """(P, L, U) with P A = L U from a getrf result in the reference's pivot convention"""
+    m, n = LU.shape
+    k = min(m, n)
+    perm = np.arange(m)
+    for i in range(k):
+        p = (i // b) * b + int(ipiv_local[i]) - 1
+        perm[[i, p]] = perm[[p, i]]
+    L = np.tril(LU[:, :k], -1) + np.eye(m, k)
+    U = np.triu(LU[:k, :])
+    return perm, L, U
+
+
 def cg(A: np.ndarray, rhs: np.ndarray, bm: int, tol: float, steps: int):
     n = A.shape[0]
     x = np.zeros(n)
@@ -215,6 +252,23 @@ def ref_chol_h(variant: str, tiles: np.ndarray) -> int:
 def ref_spdsolv(A: np.ndarray, B: np.ndarray, b: int) -> int:
     m, nrhs = B.shape
     return ref().dspdsolv_main(C.c_int(m), C.c_int(nrhs), C.c_int(b), _ptr(A), _ptr(B))
+
+
+def ref_getrf(A: np.ndarray, b: int, single: bool = False) -> np.ndarray:
+    """the reference's ompss_dgetrf / ompss_sgetrf (dlu_main), A in place; returns its IPIV"""
+    m, n = A.shape
+    ipiv = np.zeros(max(m, n), dtype=np.int32)
+    f = ref().ompss_sgetrf if single else ref().ompss_dgetrf
+    f(C.c_int(m), C.c_int(n), C.c_int(b), _ptr(A), C.c_int(m), ipiv.ctypes.data_as(C.c_void_p))
+    return ipiv[:min(m, n)]
+
+
+def ref_gensolv(A: np.ndarray, B: np.ndarray, b: int, single: bool = False) -> None:
+    """the reference's dgensolv_main / sgensolv_main: A -> LU, B -> X (B has as many columns as A rows:
+    its IPIV is allocated with the column count)"""
+    m, n = B.shape
+    f = ref().sgensolv_main if single else ref().dgensolv_main
+    f(C.c_int(m), C.c_int(n), C.c_int(b), _ptr(A), _ptr(B))
 
 
 def ref_dtrsm(side, uplo, trans, diag, m, n, b, alpha, A, lda, B, ldb) -> None:

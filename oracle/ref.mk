@@ -19,7 +19,7 @@ RCFLAGS := -O2 -w -fPIC -DHAVE_CONFIG_H -I$(OUT) \
            -I$(REF_SRC)/fp -I$(REF_SRC)/blas -I$(REF_SRC)/blocked_blas -I$(REF_SRC)/matutil \
            -I$(REF_SRC)/util -I$(REF_SRC)/cholesky/dense -I$(REF_SRC)/spdsolv -I$(REF_SRC)/trsm \
            -I$(REF_SRC)/syrk \
-           -I$(REF_SRC)/csparse -I$(REF_SRC)/itref
+           -I$(REF_SRC)/csparse -I$(REF_SRC)/itref -I$(REF_SRC)/lu -I$(REF_SRC)/gensolv
 
 # precision-generic sources (built for both precisions)
 GEN := cholesky/dense/chol_rlmain.c cholesky/dense/chol_llmain.c cholesky/dense/chol_hrlmain.c \
@@ -27,7 +27,8 @@ GEN := cholesky/dense/chol_rlmain.c cholesky/dense/chol_llmain.c cholesky/dense/
        blocked_blas/tasks_potrf.c blocked_blas/tasks_trsm.c blocked_blas/tasks_syrk.c \
        blocked_blas/task_gemm.c blocked_blas/tasks_nested_potrf.c blocked_blas/tasks_nested_trsm.c \
        blocked_blas/tasks_nested_syrk.c blocked_blas/tasks_nested_gemm.c \
-       spdsolv/spdsolv_main.c trsm/trsm_main.c syrk/syrk_main.c
+       spdsolv/spdsolv_main.c trsm/trsm_main.c syrk/syrk_main.c \
+       lu/lu_main.c lu/lull_main.c lu/lu_kernels.c gensolv/gensolv_main.c
 # double-only sources: the dense itref program and what it links
 DBL := itref/itref.c itref/itref_config.c itref/itref_setup.c fp/fptype.c \
        blocked_blas/task_dot.c blocked_blas/task_axpy.c blocked_blas/task_axpy_async.c \
@@ -37,7 +38,7 @@ DBL := itref/itref.c itref/itref_config.c itref/itref_setup.c fp/fptype.c \
        util/ompss_options.c matutil/matfprint.c matutil/matfread.c matutil/genmat.c \
        matutil/genmat_config.c matutil/densutil.c csparse/dcsparse.c matutil/hb.c
 # precision-independent sources
-COM := fp/fpmatr.c cholesky/dense/ompss_dense_chol.c trsm/ompss_trsm.c syrk/ompss_syrk.c
+COM := fp/fpmatr.c cholesky/dense/ompss_dense_chol.c trsm/ompss_trsm.c syrk/ompss_syrk.c lu/ompss_lu.c
 
 GEN_D := $(patsubst %.c,$(OUT)/d/%.o,$(GEN))
 GEN_S := $(patsubst %.c,$(OUT)/s/%.o,$(GEN))

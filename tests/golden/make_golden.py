@@ -25,6 +25,11 @@ scaled down to a few hundred KB in total:
               by the reference's own code (hb_sym_diag_block + CSparse
               cs_schol/cs_chol/cs_cholsol2, itref_setup.c:55-93) on a sparse
               SPD matrix in zero-based CSR, applied to a vector
+  lu_*        the reference's ompss_dgetrf (dlu_main, lu_main.c) on GENMAT_IP
+              matrices (U[0,1) + 100 on the diagonal, as lu_test.c and the dlu
+              program), square with a ragged last panel and tall rectangular
+  gensolv_*   dgensolv_main (gensolv_main.c) on the same distribution, B ~
+              U[0,1) with as many columns as rows (its IPIV is sized by them)
 
     python tests/golden/make_golden.py [group ...]   (default: every group)
 """
@@ -190,6 +195,22 @@ def sparse_bj_cases():
         save(f"sparse_bj_n{n}_bm{bm}", A=A, vptr=vptr, vpos=vpos, vval=vval, r=r, z=z, bm=np.int64(bm))
 
 
+def lu_cases():
+    """the reference's ompss_dgetrf (dlu_main) and dgensolv_main on its own matrix distribution (GENMAT_IP:
+    uniform [0, 1) plus 100 on the diagonal, seeded here), as lu_test.c and the dlu/dgensolv programs run it"""
+    for m, n, b, seed in ((200, 200, 33, 11), (240, 160, 64, 12)):
+        A = O.genmat_ip(m, n, seed)
+        LU = A.copy(order="F")
+        ipiv = O.ref_getrf(LU, b)
+        save(f"lu_m{m}_n{n}_b{b}", A=A, LU=LU, ipiv=ipiv, b=np.int64(b))
+    m, b = 128, 48
+    A = O.genmat_ip(m, m, 13)
+    B = np.asfortranarray(np.random.default_rng(14).random((m, m)))
+    LU, X = A.copy(order="F"), B.copy(order="F")
+    O.ref_gensolv(LU, X, b)
+    save(f"gensolv_m{m}_b{b}", A=A, B=B, LU=LU, X=X, b=np.int64(b))
+
+
 if __name__ == "__main__":
     if not O.ref_available():
         sys.exit("build the reference first: make -C oracle ref")
@@ -205,3 +226,5 @@ if __name__ == "__main__":
     ssyrk_case()
     dcg_cases()
     itref_cases()
+    sparse_bj_cases()
+    lu_cases()

@@ -214,3 +214,51 @@ def test_mm_reader_matches_scipy(tmp_path):
             assert np.all(np.diff(vpos[vptr[i]:vptr[i + 1]]) > 0)
         np.testing.assert_allclose(got, A, rtol=0, atol=1e-15)
         np.testing.assert_allclose(ref if kind == "general" else A, A)
+
+
+# ---------------------------------------------------------------- LU / gensolv
+@pytest.mark.parametrize("name", ["lu_m200_n200_b33", "lu_m240_n160_b64"])
+def test_oracle_lu_matches_reference(golden_dir, name):
+    d = np.load(os.path.join(golden_dir, name + ".npz"))
+    A = d["A"].copy(order="F")
+    info, ipiv = O.getrf(A, int(d["b"]))
+    assert info == 0
+    np.testing.assert_array_equal(ipiv, d["ipiv"])
+    np.testing.assert_allclose(A, d["LU"], rtol=0, atol=1e-12 * np.abs(d["LU"]).max())
+
+
+def test_oracle_gensolv_matches_reference(golden_dir):
+    d = np.load(os.path.join(golden_dir, "gensolv_m128_b48.npz"))
+    A, B = d["A"].copy(order="F"), d["B"].copy(order="F")
+    assert O.gensolv(A, B, int(d["b"])) == 0
+    np.testing.assert_allclose(A, d["LU"], rtol=0, atol=1e-12 * np.abs(d["LU"]).max())
+    np.testing.assert_allclose(B, d["X"], rtol=0, atol=1e-13 * np.abs(d["X"]).max())
+
+
+def test_oracle_lu_with_pivoting_matches_lapack_when_panels_align():
+    """partial pivoting over every row below: the same pivots and factor as LAPACK dgetrf"""
+    import scipy.linalg as sl
+    A0 = np.asfortranarray(np.random.default_rng(5).standard_normal((300, 300)))
+    lu, piv = sl.lu_factor(A0)
+    A = A0.copy(order="F")
+    info, ipiv = O.getrf(A, 50)
+    assert info == 0
+    np.testing.assert_array_equal(np.arange(300) // 50 * 50 + ipiv, piv + 1)
+    np.testing.assert_allclose(A, lu, rtol=0, atol=1e-11)
+    perm, L, U = O.lu_unpack(A, ipiv, 50)
+    np.testing.assert_allclose(A0[perm], L @ U, rtol=0, atol=1e-12)
+
+
+def test_oracle_lu_ragged_last_panel_quirk():
+    """the reference swaps only dimC columns of the earlier blocks for a ragged last panel
+    (lu_main.c TASK_LASWP(j, dimC, ...)): with pivoting there, P A != L U.  The oracle keeps it
+    (it restates the reference); the library factors correctly (tests/test_gpu_lu.py)"""
+    A0 = np.asfortranarray(np.random.default_rng(5).standard_normal((300, 300)))
+    A = A0.copy(order="F")
+    _, ipiv = O.getrf(A, 64)
+    A2 = A0.copy(order="F")
+    if O.ref_available():
+        assert (O.ref_getrf(A2, 64) == ipiv).all()
+        np.testing.assert_allclose(A, A2, rtol=0, atol=1e-12)
+    perm, L, U = O.lu_unpack(A, ipiv, 64)
+    assert np.abs(A0[perm] - L @ U).max() > 1.0
