@@ -67,6 +67,8 @@ def parse():
     p.add_argument("--no-batched", action="store_true", help="skip the batched uneven-systems measurement")
     p.add_argument("--batch-count", type=int, default=10000)
     p.add_argument("--no-configs", action="store_true", help="skip the other configurations' records")
+    p.add_argument("--case", default=None, choices=sorted(CASES),
+                   help="run one small single-kernel case (for ncu captures) and exit")
     p.add_argument("--ref-budget-s", type=float, default=150.0,
                    help="reference arm: stop timing full-size calls once their total passes this")
     a = p.parse_args()
@@ -749,7 +751,7 @@ def config_records(args, world, rank, dev, peaks):
 
 
 def blas_records(args, world, rank, dev, peaks):
-    """The stand-alone BLAS-3 drivers at the reference's own chart sizes
+    """The stand-alone BLAS-3 drivers and the LU / general solve at the reference's own chart sizes
     (tests/dsyrk.cfg: lower, transposed, n = k = 16000, alpha 13.44, beta
     -9.877, b in {550, 1032, 2898, 5988}; tests/dtrsm.cfg: left lower, no
     transpose, m = n = 1500, alpha 13.44, b in {121, 256, 350, 550}), each timed
@@ -871,6 +873,67 @@ def blas_records(args, world, rank, dev, peaks):
         rec["reference"] = rref
     out["dtrsm_m1500_n1500"] = rec
     del Ld, Bd0, Bd
+    torch.cuda.empty_cache()
+    # ---- LU and the general solve (tests/dlu.cfg, tests/dgensolv.cfg: m = n = 1500) ----
+    m = 1500
+    bs = (121, 256, 350, 550, 1000)
+    gA = np.random.default_rng(1501 + rank).random((m, m))
+    gA[np.arange(m), np.arange(m)] += 100.0                 # GENMAT_IP: U[0,1) + 100 on the diagonal
+    A0 = np.asfortranarray(gA)
+    B0 = np.asfortranarray(np.random.default_rng(1502 + rank).random((m, m)))
+    fl_lu = 2.0 * m ** 3 / 3.0
+    fl_gs = fl_lu + 2.0 * m * m * m
+    Ad = torch.tensor(np.ascontiguousarray(A0.T), device=dev)
+    Aw = torch.empty_like(Ad)
+    piv = torch.zeros(m, dtype=torch.int32, device=dev)
+    run = lambda: lnb.dgetrf_dev(Aw, m, m, piv, stream=s)
+    prep = lambda: Aw.copy_(Ad)
+    time_events(run, 1, s, prep)
+    ms = allmax(world, time_events(run, reps, s, prep))
+    rec = {"m": m, "n": m, "matrix": "U[0,1) + 100 I (the reference's GENMAT_IP)", "device_ms": round(ms, 3),
+           "device_tflops": round(world * fl_lu / ms / 1e9, 4)}
+    e2e, e2e_gs = {}, {}
+    for bb in bs:
+        t, tg = [], []
+        for _ in range(2):
+            A = A0.copy(order="F")
+            t0 = time.perf_counter()
+            lnb.ompss_getrf(A, bb)
+            t.append(time.perf_counter() - t0)
+            A, B = A0.copy(order="F"), B0.copy(order="F")
+            t0 = time.perf_counter()
+            lnb.gensolv(A, B, bb)
+            tg.append(time.perf_counter() - t0)
+        e2e[f"b{bb}_ms"] = round(min(t) * 1e3, 3)
+        e2e_gs[f"b{bb}_ms"] = round(min(tg) * 1e3, 3)
+    berr = float(np.abs(A0 @ B - B0).max() / (np.abs(A0).sum(1).max() * np.abs(B).max() + np.abs(B0).max()))
+    assert berr < 10 * m * np.finfo(float).eps, berr
+    rec["getrf_e2e"] = e2e
+    rec["gensolv_e2e"] = e2e_gs
+    rec["gensolv_backward_error"] = berr
+    rec["e2e_api"] = "ompss_dgetrf / dgensolv_main (host arrays in and out)"
+    if with_ref:
+        rref, rgs = {}, {}
+        for bb in bs:
+            A = A0.copy(order="F")
+            t0 = time.perf_counter()
+            ip = O.ref_getrf(A, bb)
+            rref[f"b{bb}_ms"] = round((time.perf_counter() - t0) * 1e3, 3)
+            if bb == bs[0]:
+                Ag = A0.copy(order="F")
+                _, ipg = lnb.ompss_getrf(Ag, bb)
+                rec["factor_max_rel_diff_vs_reference"] = float(np.abs(Ag - A).max() / np.abs(A).max())
+                rec["pivots_equal_reference"] = bool((ipg == ip).all())
+            A, B = A0.copy(order="F"), B0.copy(order="F")
+            t0 = time.perf_counter()
+            O.ref_gensolv(A, B, bb)
+            rgs[f"b{bb}_ms"] = round((time.perf_counter() - t0) * 1e3, 3)
+        rec["reference_getrf"] = rref
+        rec["reference_gensolv"] = rgs
+        rec["reference_cores"] = cores
+        rec["gensolv_e2e_speedup_vs_reference_best"] = round(min(rgs.values()) / min(e2e_gs.values()), 2)
+    out["lu_gensolv_m1500"] = rec
+    del Ad, Aw, piv
     torch.cuda.empty_cache()
     return out
 
@@ -1086,8 +1149,63 @@ def ours_arm(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def case_symv8(n):
+    """k_symv_tc: Y = A X from the lower triangle, n x n FP64 (2 GB at n = 16384), 8 columns, 3 calls"""
+    import torch
+    import linompss_b200 as lnb
+    A = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    X = torch.randn(8, n, dtype=torch.float64, device="cuda")
+    Y = torch.empty_like(X)
+    for _ in range(3):
+        lnb.dsymv_dev(A, X, Y, n, 8)
+
+
+def case_syrk(n):
+    """k_gemm_dmma: C = A^T A + C on the lower triangle, n = k (FP64), 2 calls"""
+    import torch
+    import linompss_b200 as lnb
+    A = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    C = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        lnb.dsyrk_dev("L", "T", n, n, 1.0, A, 1.0, C)
+
+
+def case_dag(n):
+    """k_chol_dag_f64: the FP64 factorization on the device DAG walk, b = 512, 2 calls"""
+    import linompss_b200 as lnb
+    A0 = make_spd(n, 1e-2, 3, "cuda")
+    lnb.set_chol_schedule(lnb.SCHED_DAG)
+    for _ in range(2):
+        A = A0.clone()
+        lnb.dchol_dev(A, n, 512)
+
+
+def case_bf16(n):
+    """configuration 4's solver at order n: BF16 factor, 8 right-hand sides, delta 1e-4 (PCG: k_trsm_blk with 8
+    columns, k_symv_tc), one call"""
+    import torch
+    import linompss_b200 as lnb
+    A = make_spd(n, 1e-4, 7, "cuda", scaled=True)
+    B = torch.randn(8, n, dtype=torch.float64, device="cuda")
+    X = torch.zeros_like(B)
+    rc, res = lnb.dsposv_ir_dev(A, B, X, n, 8, 1024, lnb.ir_opts(factor=lnb.FACTOR_BF16, max_iter=40,
+                                                                 pcg_max_iter=400))
+    assert rc == 0, (rc, res)
+
+
+CASES = {"symv8": (case_symv8, 16384), "syrk": (case_syrk, 8192), "dag": (case_dag, 4096),
+         "bf16": (case_bf16, 16384)}
+
+
 def main():
     args = parse()
+    if args.case:
+        import torch
+        fn, n = CASES[args.case]
+        fn(args.n or n)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": args.case, "n": args.n or n, "ok": True}))
+        return
     world, rank, local = dist_init()
     try:
         if args.impl == "reference":

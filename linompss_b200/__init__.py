@@ -320,9 +320,9 @@ def dpotrs_dev(Lt, Bt, n: int, nrhs: int, which: str = "B", stream=None) -> int:
 def ompss_getrf(A, b: int, ll: bool = False) -> tuple:
     """P A = L U in place (ompss_dgetrf / ompss_sgetrf by A's dtype, column-major); returns (info, IPIV) with the
     reference's panel-relative pivots"""
-    _colmajor(A)
-    m, n = A.shape
     single = A.dtype == np.float32
+    _colmajor(A, np.float32 if single else np.float64)
+    m, n = A.shape
     name = ("ompss_sgetrf" if single else "ompss_dgetrf") + ("_ll" if ll else "")
     f = getattr(lib(), name)
     f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
@@ -333,10 +333,10 @@ def ompss_getrf(A, b: int, ll: bool = False) -> tuple:
 
 def gensolv(A, B, b: int) -> int:
     """dgensolv_main / sgensolv_main: A (m x m) -> LU, B (m x n) -> A^-1 B, in place, column-major"""
-    _colmajor(A)
-    _colmajor(B)
-    m, n = B.shape
     single = A.dtype == np.float32
+    _colmajor(A, np.float32 if single else np.float64)
+    _colmajor(B, np.float32 if single else np.float64)
+    m, n = B.shape
     f = lib().sgensolv_main if single else lib().dgensolv_main
     f.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
     return _chk(f(m, n, b, _p(A), _p(B)))

@@ -83,19 +83,22 @@ __global__ void __launch_bounds__(NT) k_lu_panel(double *A, int64_t lda, int64_t
             cand[0] = best;                                  // -1: no row of mine at or below c0+k
             cand[1] = bi == LLONG_MAX ? -1.0 : (double)bi;
         }
-        cl.sync();                                           // #1: candidates visible
-        // 2. the pivot row, the same in every CTA
-        if (tid == 0) {
+        if (ncl > 1) cl.sync(); else __syncthreads();          // #1: candidates visible
+        // 2. the pivot row, the same in every CTA: lane q of warp 0 reads CTA q's candidate
+        if (warp == 0) {
             double gb = -1.0;
             long long gi = LLONG_MAX;
-            for (int q = 0; q < ncl; ++q) {
-                const double *cq = cl.map_shared_rank(cand, q);
-                const double v = cq[0];
-                if (cq[1] < 0.0) continue;
-                const long long i = (long long)cq[1];
-                if (v > gb || (v == gb && i < gi)) { gb = v; gi = i; }
+            if (lane < ncl) {
+                const double *cq = cl.map_shared_rank(cand, lane);
+                if (cq[1] >= 0.0) { gb = cq[0]; gi = (long long)cq[1]; }
             }
-            s_p = gi;
+#pragma unroll
+            for (int o = 4; o > 0; o >>= 1) {                  // ncl <= 8
+                const double ov = __shfl_down_sync(0xffffffffu, gb, o);
+                const long long oi = __shfl_down_sync(0xffffffffu, gi, o);
+                if (ov > gb || (ov == gb && oi < gi)) { gb = ov; gi = oi; }
+            }
+            if (lane == 0) s_p = gi;
         }
         __syncthreads();
         const int64_t p = s_p;
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(NT) k_lu_panel(double *A, int64_t lda, int64_t
             double *sq = cl.map_shared_rank(swp, op);
             for (int j = tid; j < nb; j += NT) sq[j] = P[(int64_t)j * R + (gk - r0)];
         }
-        cl.sync();                                           // #2: pivot row and old row delivered
+        if (ncl > 1) cl.sync(); else __syncthreads();          // #2: pivot row and old row delivered
         if (rank == ok)
             for (int j = tid; j < nb; j += NT) P[(int64_t)j * R + (gk - r0)] = urow[j];
         if (rank == op && p != gk)
@@ -137,7 +140,7 @@ __global__ void __launch_bounds__(NT) k_lu_panel(double *A, int64_t lda, int64_t
         const int j = (int)(i / R), r = (int)(i % R);
         if (r < nr) A[(r0 + r) + (c0 + j) * lda] = P[i];
     }
-    cl.sync();                                               // no CTA leaves while its smem may be read
+    if (ncl > 1) cl.sync();                                  // no CTA leaves while its smem may be read
 }
 
 // rows k and piv[k]-1 swap, k = k0..k1-1 in order, on columns [a0, a1) and [b0, b1)
@@ -192,9 +195,15 @@ __global__ void __launch_bounds__(128) k_lu_trsm_unit(double *A, int64_t lda, in
 
 using namespace lnb::lu;
 
-// the widest panel (<= 32, a power of two) whose rows fit one cluster's shared memory; 0 if none
+// Panel width for `rows` rows.  One CTA per panel when the rows fit its shared
+// memory at 8 columns or more (barriers within the CTA only: about a
+// microsecond per column); otherwise the widest panel a cluster of up to 8
+// CTAs holds (two cluster barriers and the DSMEM exchange per column cost
+// several times more, so the cluster takes wide panels).  0 if none fits.
 extern "C" int lnb_lu_panel_width(int64_t rows)
 {
+    for (int nb = MAXNB; nb >= 8; nb >>= 1)
+        if (rows * nb * (int64_t)sizeof(double) <= (int64_t)SMEM_DATA) return nb;
     for (int nb = MAXNB; nb >= 4; nb >>= 1)
         if (rows * nb * (int64_t)sizeof(double) <= (int64_t)MAXCL * SMEM_DATA) return nb;
     return 0;
