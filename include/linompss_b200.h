@@ -345,14 +345,17 @@ LNB_EXPORT int lnb_batched_posv_dev(int count, const int *n_dev, const int *nrhs
                                     const double *dA, const double *dB, double *dX,
                                     int mode, int max_iter, int *info_dev, int *iters_dev,
                                     void *stream);
-/* Autotuner: times the candidate panel widths of the per-system factorization
- * on this batch (synchronous) and keeps the fastest for later
- * lnb_batched_posv_dev calls of the same mode.  Returns the chosen width.
- * Each system's A_s is n x n FP64 with both triangles stored. */
+/* Autotuner: times the candidate launch shapes of the persistent solver on
+ * this batch (synchronous): CTA size (256 / 512 threads), systems resident per
+ * SM (1 / 2) and processing order (largest first / largest and smallest
+ * interleaved), and keeps the fastest for later lnb_batched_posv_dev calls of
+ * the same mode.  Returns the chosen CTA size; lnb_batched_config reports the
+ * whole shape.  Each system's A_s is n x n FP64 with both triangles stored. */
 LNB_EXPORT int lnb_batched_autotune(int count, const int *n_dev, const int *nrhs_dev,
                                     const int64_t *a_off_dev, const int64_t *b_off_dev,
                                     const double *dA, const double *dB, double *dX,
                                     int mode, int max_iter, void *stream);
+LNB_EXPORT int lnb_batched_config(int mode, int *cta_threads, int *ctas_per_sm, int *interleave);
 /* Multi-GPU split of one batch (host only, no device work): the systems in
  * decreasing order of estimated cost n^3/3 + 2 n^2 nrhs (equal costs: lower
  * index first), each given to the part with the least cost so far (ties: lower

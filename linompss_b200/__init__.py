@@ -468,10 +468,18 @@ def batched_partition(ns, rs, parts: int):
 
 def batched_autotune(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode=FACTOR_FP32, max_iter=10,
                      stream=None) -> int:
-    """Times the solver's CTA sizes on this batch, keeps the fastest for later
-    calls in this process and returns it (256 or 512 threads)."""
+    """Times the solver's launch shapes on this batch (CTA size, systems per SM, order), keeps the fastest for
+    later calls in this process and returns its CTA size (256 or 512 threads)."""
     args = _batched_args(n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode, max_iter)
     return _chk(lib().lnb_batched_autotune(*args, _stream(stream)))
+
+
+def batched_config(mode=FACTOR_FP32) -> dict:
+    """the launch shape the batched solver uses for `mode` (after autotuning, the chosen one)"""
+    v = [C.c_int(), C.c_int(), C.c_int()]
+    lib().lnb_batched_config(mode, C.byref(v[0]), C.byref(v[1]), C.byref(v[2]))
+    return {"cta_threads": v[0].value, "ctas_per_sm": v[1].value, "order": "interleaved" if v[2].value else
+            "largest first"}
 
 
 def spotrs_dev(Lt, Bt, n: int, nrhs: int, which: str = "B", stream=None) -> int:

@@ -195,15 +195,12 @@ __global__ void __launch_bounds__(128) k_lu_trsm_unit(double *A, int64_t lda, in
 
 using namespace lnb::lu;
 
-// Panel width for `rows` rows.  One CTA per panel when the rows fit its shared
-// memory at 8 columns or more (barriers within the CTA only: about a
-// microsecond per column); otherwise the widest panel a cluster of up to 8
-// CTAs holds (two cluster barriers and the DSMEM exchange per column cost
-// several times more, so the cluster takes wide panels).  0 if none fits.
+// Panel width for `rows` rows: the widest (<= 32, a power of two) whose rows
+// fit a cluster of up to 8 CTAs; 0 if none fits.  Narrower panels that fit one
+// CTA were measured slower on B200 (n = 1500: 11.5 vs 10.2 ms; n = 4096: 45.7
+// vs 34.2 ms): the extra panels' launches cost more than the cluster barriers.
 extern "C" int lnb_lu_panel_width(int64_t rows)
 {
-    for (int nb = MAXNB; nb >= 8; nb >>= 1)
-        if (rows * nb * (int64_t)sizeof(double) <= (int64_t)SMEM_DATA) return nb;
     for (int nb = MAXNB; nb >= 4; nb >>= 1)
         if (rows * nb * (int64_t)sizeof(double) <= (int64_t)MAXCL * SMEM_DATA) return nb;
     return 0;

@@ -7,10 +7,15 @@
  * captured in a CUDA graph once the workspace exists (any earlier call, or
  * lnb_batched_autotune, creates it).
  *
- * Autotuning: the CTA size of the persistent solver (256 or 512 threads; 256
- * only in FP64 mode, whose shared-memory layout fills the SM) is chosen by
- * lnb_batched_autotune, which times the candidates on the caller's own batch
- * and keeps the faster one for the rest of the process.
+ * Autotuning: lnb_batched_autotune times the candidate launch shapes on the
+ * caller's own batch and keeps the fastest for the rest of the process:
+ *   - CTA size (256 or 512 threads),
+ *   - resident systems per SM (1 or 2: two 256-thread FP32 CTAs fit one SM's
+ *     shared memory and registers, so one system's latency chain hides the
+ *     other's),
+ *   - processing order (largest first, or largest/smallest interleaved).
+ * FP64 mode's panel fills the shared memory: one 256-thread CTA per SM, both
+ * orders.
  */
 #include <stdlib.h>
 #include <string.h>
@@ -21,7 +26,7 @@ size_t lnb_batched_scratch_bytes(int grid, int fp64);
 int lnb_k_batched_posv(int count, const int *n, const int *nrhs, const int64_t *a_off, const int64_t *b_off,
                        const double *A, const double *B, double *X, void *scratch, int grid, const int *order,
                        int *ticket, int *info, int *iters, int max_iter, int fp64, int variant, cudaStream_t s);
-int lnb_k_batch_order(int count, const int *n, int *order, cudaStream_t s);
+int lnb_k_batch_order(int count, const int *n, int *order, int interleave, cudaStream_t s);
 
 #define CK(call, where)                                            \
     do {                                                           \
@@ -29,11 +34,12 @@ int lnb_k_batch_order(int count, const int *n, int *order, cudaStream_t s);
         if (_e != 0) return lnb_cuda_error(_e, where);             \
     } while (0)
 
-static int g_pw[2] = {256, 256};   /* tuned CTA size: [fp32 mode, fp64 mode] */
+typedef struct { int nt, per_sm, interleave; } bcfg;
+static bcfg g_cfg[2] = {{256, 1, 0}, {256, 1, 0}};   /* tuned shape: [fp32 mode, fp64 mode] */
 
 static int batched_run(int count, const int *n, const int *nrhs, const int64_t *a_off, const int64_t *b_off,
                        const double *dA, const double *dB, double *dX, int mode, int max_iter, int *info,
-                       int *iters, cudaStream_t s, int pw)
+                       int *iters, cudaStream_t s, bcfg cf)
 {
     if (count < 0) return lnb_set_error(LNB_EINVAL, "count = %d < 0", count);
     if (count == 0) return 0;
@@ -43,7 +49,7 @@ static int batched_run(int count, const int *n, const int *nrhs, const int64_t *
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
     const int fp64 = mode == LNB_FACTOR_FP64;
-    const int grid = c->sms;
+    const int grid = c->sms * cf.per_sm;
     const size_t sb = lnb_batched_scratch_bytes(grid, fp64);
     void *ws = lnb_ws(c, lnb_align256(sb) + lnb_align256((size_t)count * 4) + 512);
     if (!ws) return LNB_ENOMEM;
@@ -52,9 +58,9 @@ static int batched_run(int count, const int *n, const int *nrhs, const int64_t *
     int *order = lnb_arena_take(&ar, (size_t)count * 4);
     int *ticket = lnb_arena_take(&ar, 64);
     if (!ticket) return lnb_set_error(LNB_ENOMEM, "batched workspace");
-    CK(lnb_k_batch_order(count, n, order, s), "order");
+    CK(lnb_k_batch_order(count, n, order, cf.interleave, s), "order");
     CK(lnb_k_batched_posv(count, n, nrhs, a_off, b_off, dA, dB, dX, scratch, grid, order, ticket, info, iters,
-                          max_iter > 0 ? max_iter : 10, fp64, pw, s), "batched");
+                          max_iter > 0 ? max_iter : 10, fp64, cf.nt, s), "batched");
     return 0;
 }
 
@@ -63,7 +69,16 @@ int lnb_batched_posv_dev(int count, const int *n_dev, const int *nrhs_dev, const
                          int max_iter, int *info_dev, int *iters_dev, void *stream)
 {
     return batched_run(count, n_dev, nrhs_dev, a_off_dev, b_off_dev, dA, dB, dX, mode, max_iter, info_dev,
-                       iters_dev, (cudaStream_t)stream, g_pw[mode == LNB_FACTOR_FP64]);
+                       iters_dev, (cudaStream_t)stream, g_cfg[mode == LNB_FACTOR_FP64]);
+}
+
+int lnb_batched_config(int mode, int *cta_threads, int *ctas_per_sm, int *interleave)
+{
+    const bcfg cf = g_cfg[mode == LNB_FACTOR_FP64];
+    if (cta_threads) *cta_threads = cf.nt;
+    if (ctas_per_sm) *ctas_per_sm = cf.per_sm;
+    if (interleave) *interleave = cf.interleave;
+    return 0;
 }
 
 int lnb_batched_autotune(int count, const int *n_dev, const int *nrhs_dev, const int64_t *a_off_dev,
@@ -73,10 +88,12 @@ int lnb_batched_autotune(int count, const int *n_dev, const int *nrhs_dev, const
     cudaStream_t s = (cudaStream_t)stream;
     lnb_ctx *c = lnb_ctx_get();
     if (!c) return LNB_ENODEV;
-    const int cand[2] = {256, 512};
-    const int ncand = mode == LNB_FACTOR_FP64 ? 1 : 2;
+    static const bcfg cand32[] = {{256, 1, 0}, {256, 2, 0}, {256, 2, 1}, {512, 1, 0}, {512, 1, 1}};
+    static const bcfg cand64[] = {{256, 1, 0}, {256, 1, 1}};
+    const bcfg *cand = mode == LNB_FACTOR_FP64 ? cand64 : cand32;
+    const int ncand = mode == LNB_FACTOR_FP64 ? 2 : 5;
     float best = 1e30f;
-    int pick = 256;
+    bcfg pick = cand[0];
     for (int k = 0; k < ncand; ++k) {
         for (int rep = 0; rep < 2; ++rep) {   /* first run warms up */
             CK(cudaEventRecord(c->t0, s), "event");
@@ -93,8 +110,8 @@ int lnb_batched_autotune(int count, const int *n_dev, const int *nrhs_dev, const
             }
         }
     }
-    g_pw[mode == LNB_FACTOR_FP64] = pick;
-    return pick;
+    g_cfg[mode == LNB_FACTOR_FP64] = pick;
+    return pick.nt;
 }
 
 /* ---- multi-GPU split of a batch -------------------------------------------- */
