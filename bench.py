@@ -1202,8 +1202,20 @@ def case_bf16(n):
     assert rc == 0, (rc, res)
 
 
+def case_lu(n):
+    """the LU with partial pivoting on device memory (lnb_dgetrf_dev), n x n N(0,1), 2 calls"""
+    import torch
+    import linompss_b200 as lnb
+    A0 = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    A = torch.empty_like(A0)
+    piv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    for _ in range(2):
+        A.copy_(A0)
+        lnb.dgetrf_dev(A, n, n, piv)
+
+
 CASES = {"symv8": (case_symv8, 16384), "syrk": (case_syrk, 8192), "dag": (case_dag, 4096),
-         "bf16": (case_bf16, 16384)}
+         "bf16": (case_bf16, 16384), "lu": (case_lu, 1500)}
 
 
 def main():
