@@ -220,9 +220,13 @@ __device__ int bfactor(TF *F, int ldF, int n, TF *Dv, TF *P, TF *Li, TF *Rd, int
 }
 
 // z <- inv(L) z, then z <- inv(L^T) z, for nr columns of z in shared memory
-// (z[q * BMAXN + i]); L in F, the block inverses in Dv.
+// (z[q * BMAXN + i]); L in F, the block inverses in Dv.  env (may be NULL):
+// the factor's envelope per 32-row tile t -- env[t] = the first column with a
+// nonzero in rows 32t .. 32t+31, env[BMAXN/BP + t] = the last row with a
+// nonzero in columns 32t .. 32t+31 -- so the sums skip tiles that are zero.
 template <typename TF, int NT>
-__device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double *z, double *red)
+__device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double *z, double *red,
+                       const int *env = nullptr)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = NT / 32;
@@ -231,13 +235,14 @@ __device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double
     // forward
     for (int kb = 0; kb < nblk; ++kb) {
         const int k0 = kb * BP, kn = min(BP, n - k0);
-        if (k0 > 0) {
+        const int cs = env ? env[kb] : 0;                   // columns before cs are zero in these rows
+        if (k0 > cs) {
             double acc[BMAXR];
 #pragma unroll
             for (int q = 0; q < BMAXR; ++q) acc[q] = 0.0;
             if (lane < kn) {
 #pragma unroll 4
-                for (int c = warp; c < k0; c += NW) {
+                for (int c = cs + warp; c < k0; c += NW) {
                     const double f = (double)__ldcg(F + (k0 + lane) + (int64_t)c * ldF);
 #pragma unroll
                     for (int q = 0; q < BMAXR; ++q)
@@ -269,14 +274,15 @@ __device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double
     // backward
     for (int kb = nblk - 1; kb >= 0; --kb) {
         const int k0 = kb * BP, kn = min(BP, n - k0), r0 = k0 + kn;
-        if (r0 < n) {
+        const int re = env ? min(n, env[BMAXN / BP + kb] + 1) : n;    // rows from re on are zero here
+        if (r0 < re) {
             for (int jc = warp; jc < kn; jc += NW) {
                 double acc[BMAXR];
 #pragma unroll
                 for (int q = 0; q < BMAXR; ++q) acc[q] = 0.0;
                 const TF *col = F + (int64_t)(k0 + jc) * ldF;
 #pragma unroll 4
-                for (int r = r0 + lane; r < n; r += 32) {
+                for (int r = r0 + lane; r < re; r += 32) {
                     const double f = (double)__ldcg(col + r);
 #pragma unroll
                     for (int q = 0; q < BMAXR; ++q)

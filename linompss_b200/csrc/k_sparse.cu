@@ -12,6 +12,8 @@
 //             cs_schol(A, 0) + cs_chol compute) by one CTA with the batched
 //             solver's bfactor, and applied as z = L^-T L^-1 r
 //             (bsblas_dcholsolv2, bsblas_csrmm.h:498) with its bsolve.
+#include <climits>
+
 #include "k_bfactor.cuh"
 
 namespace lnb {
@@ -45,11 +47,20 @@ __host__ __device__ inline int64_t bj_stride(int bm)
     return bj_ldf(bm) * bm + (int64_t)((bm + BP - 1) / BP) * BP * BP;
 }
 
-// block k of the matrix, dense: F[(r - r0) + (c - r0) ldF] for r, c in [r0, r0 + bk)
+// the envelope of block k's factor, per 32-row tile (bsolve's env): with natural
+// ordering the Cholesky factor keeps every row's nonzeros at or right of the
+// row's first nonzero in A (L_ij = (0 - sum of zeros) / L_jj = 0 before it)
+constexpr int ENV = 2 * (lnb::BMAXN / lnb::BP);
+
+// block k of the matrix, dense: F[(r - r0) + (c - r0) ldF] for r, c in [r0, r0 + bk);
+// env[k * ENV ..] its factor's envelope
 __global__ void __launch_bounds__(NT) k_bj_densify(int64_t n, int bm, int base, const int *__restrict__ vptr,
                                                    const int *__restrict__ vpos, const double *__restrict__ vval,
-                                                   double *fac)
+                                                   double *fac, int *env)
 {
+    constexpr int NTL = lnb::BMAXN / lnb::BP;
+    __shared__ int first[NTL], last[NTL];
+    if (threadIdx.x < NTL) { first[threadIdx.x] = INT_MAX; last[threadIdx.x] = -1; }
     const int64_t k = blockIdx.x, r0 = k * bm;
     const int bk = (int)((n - r0) < bm ? (n - r0) : bm);
     const int64_t ldF = bj_ldf(bm);
@@ -59,10 +70,25 @@ __global__ void __launch_bounds__(NT) k_bj_densify(int64_t n, int bm, int base, 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int r = warp; r < bk; r += NT / 32) {
         const int p0 = vptr[r0 + r] - base, p1 = vptr[r0 + r + 1] - base;
+        int f = r;                                          // the diagonal at least
         for (int p = p0 + lane; p < p1; p += 32) {
             const int64_t c = (int64_t)vpos[p] - base;
-            if (c >= r0 && c < r0 + bk) atomicAdd(F + r + (c - r0) * ldF, vval[p]);
+            if (c >= r0 && c < r0 + bk) {
+                atomicAdd(F + r + (c - r0) * ldF, vval[p]);
+                if (c - r0 < f) f = (int)(c - r0);
+            }
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) f = min(f, __shfl_xor_sync(0xffffffffu, f, o));
+        if (lane == 0) {
+            atomicMin(&first[r / lnb::BP], f);
+            for (int t = f / lnb::BP; t <= r / lnb::BP; ++t) atomicMax(&last[t], r);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < NTL) {
+        env[k * ENV + threadIdx.x] = first[threadIdx.x] == INT_MAX ? 0 : first[threadIdx.x];
+        env[k * ENV + NTL + threadIdx.x] = last[threadIdx.x];
     }
 }
 
@@ -91,7 +117,8 @@ __global__ void __launch_bounds__(NT) k_bj_factor(int64_t n, int bm, double *fac
 }
 
 // z = M^-1 r, one CTA per block
-__global__ void __launch_bounds__(NT) k_bj_apply(int64_t n, int bm, const double *fac, const double *r, double *z)
+__global__ void __launch_bounds__(NT) k_bj_apply(int64_t n, int bm, const double *fac, const int *env,
+                                                 const double *r, double *z)
 {
     __shared__ double zs[BMAXN];
     __shared__ double red[(NT / 32) * BP * BMAXR];
@@ -101,7 +128,7 @@ __global__ void __launch_bounds__(NT) k_bj_apply(int64_t n, int bm, const double
     const double *F = fac + k * bj_stride(bm);
     for (int i = threadIdx.x; i < bk; i += NT) zs[i] = r[r0 + i];
     __syncthreads();
-    bsolve<double, NT>(F, (int)ldF, F + ldF * bm, bk, 1, zs, red);
+    bsolve<double, NT>(F, (int)ldF, F + ldF * bm, bk, 1, zs, red, env + k * ENV);
     for (int i = threadIdx.x; i < bk; i += NT) z[r0 + i] = zs[i];
 }
 
@@ -125,16 +152,17 @@ extern "C" int64_t lnb_bj_doubles(int64_t n, int bm)
 {
     return ((n + bm - 1) / bm) * lnb::sp::bj_stride(bm);
 }
+extern "C" int64_t lnb_bj_env_ints(int64_t n, int bm) { return ((n + bm - 1) / bm) * lnb::sp::ENV; }
 
 // densify and factor the diagonal blocks; info[nblk] receives each block's info
 extern "C" int lnb_k_bj_setup(int64_t n, int bm, int base, const int *vptr, const int *vpos, const double *vval,
-                              double *fac, int *info, lnb_stream_t s)
+                              double *fac, int *env, int *info, lnb_stream_t s)
 {
     using namespace lnb::sp;
     if (n <= 0) return 0;
     if (bm < 1 || bm > lnb::BMAXN) return (int)cudaErrorInvalidValue;
     const unsigned nblk = (unsigned)((n + bm - 1) / bm);
-    k_bj_densify<<<nblk, NT, 0, (cudaStream_t)s>>>(n, bm, base, vptr, vpos, vval, fac);
+    k_bj_densify<<<nblk, NT, 0, (cudaStream_t)s>>>(n, bm, base, vptr, vpos, vval, fac, env);
     cudaError_t e = cudaFuncSetAttribute(k_bj_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BjSmem::total);
     if (e != cudaSuccess) return (int)e;
     k_bj_factor<<<nblk, NT, BjSmem::total, (cudaStream_t)s>>>(n, bm, fac, info);
@@ -142,11 +170,12 @@ extern "C" int lnb_k_bj_setup(int64_t n, int bm, int base, const int *vptr, cons
     return (int)cudaGetLastError();
 }
 
-extern "C" int lnb_k_bj_apply(int64_t n, int bm, const double *fac, const double *r, double *z, lnb_stream_t s)
+extern "C" int lnb_k_bj_apply(int64_t n, int bm, const double *fac, const int *env, const double *r, double *z,
+                              lnb_stream_t s)
 {
     using namespace lnb::sp;
     if (n <= 0) return 0;
-    k_bj_apply<<<(unsigned)((n + bm - 1) / bm), NT, 0, (cudaStream_t)s>>>(n, bm, fac, r, z);
+    k_bj_apply<<<(unsigned)((n + bm - 1) / bm), NT, 0, (cudaStream_t)s>>>(n, bm, fac, env, r, z);
     lnb_prof_count(1);
     return (int)cudaGetLastError();
 }

@@ -31,9 +31,11 @@
 int lnb_k_csrmv_f64(int64_t n, int base, const int *vptr, const int *vpos, const double *vval, const double *x,
                     double alpha, double beta, const double *yin, double *y, lnb_stream_t s);
 int64_t lnb_bj_doubles(int64_t n, int bm);
+int64_t lnb_bj_env_ints(int64_t n, int bm);
 int lnb_k_bj_setup(int64_t n, int bm, int base, const int *vptr, const int *vpos, const double *vval, double *fac,
-                   int *info, lnb_stream_t s);
-int lnb_k_bj_apply(int64_t n, int bm, const double *fac, const double *r, double *z, lnb_stream_t s);
+                   int *env, int *info, lnb_stream_t s);
+int lnb_k_bj_apply(int64_t n, int bm, const double *fac, const int *env, const double *r, double *z,
+                   lnb_stream_t s);
 
 #define BJ_MAX 512
 
@@ -43,6 +45,7 @@ typedef struct {
     int *vptr, *vpos;
     double *vval;
     double *fac;               /* block-Jacobi factors, NULL without the preconditioner */
+    int *env;                  /* their envelopes per 32-row tile (the apply skips zero tiles) */
     double *r, *p, *tmp, *z;   /* n each */
     double *scal;              /* [0]=alpha1 [1]=alpha2 [2]=<b,b> [3]=<r,r> scratch */
     double *dpart;
@@ -69,7 +72,9 @@ static size_t sp_ws_bytes(int64_t n, int64_t nnz, int bm, int precond, int extra
     size_t s = lnb_align256((size_t)(n + 1) * 4) + lnb_align256((size_t)nnz * 4) + lnb_align256((size_t)nnz * 8) +
                (4 + (size_t)extra_vectors) * lnb_align256((size_t)n * 8) + lnb_align256(8 * 8) +
                lnb_align256((size_t)lnb_dot_part_doubles(n) * 8) + 4096;
-    if (precond) s += lnb_align256((size_t)lnb_bj_doubles(n, bm) * 8) + lnb_align256((size_t)((n + bm - 1) / bm) * 4);
+    if (precond)
+        s += lnb_align256((size_t)lnb_bj_doubles(n, bm) * 8) + lnb_align256((size_t)((n + bm - 1) / bm) * 4) +
+             lnb_align256((size_t)lnb_bj_env_ints(n, bm) * 4);
     return s;
 }
 
@@ -100,9 +105,11 @@ static int sp_setup(lnb_ctx *c, int n, int bm, const int *vptr, const int *vpos,
     if (precond) {
         const int nblk = (n + bm - 1) / bm;
         w->fac = lnb_arena_take(ar, (size_t)lnb_bj_doubles(n, bm) * 8);
+        w->env = lnb_arena_take(ar, (size_t)lnb_bj_env_ints(n, bm) * 4);
         int *info = lnb_arena_take(ar, (size_t)nblk * 4);
         if (!info) return lnb_set_error(LNB_ENOMEM, "block-Jacobi workspace");
-        CK(lnb_k_bj_setup(n, bm, w->base, w->vptr, w->vpos, w->vval, w->fac, info, s), "block-Jacobi factor");
+        CK(lnb_k_bj_setup(n, bm, w->base, w->vptr, w->vpos, w->vval, w->fac, w->env, info, s),
+           "block-Jacobi factor");
         int *hinfo = (int *)malloc((size_t)nblk * 4);
         if (!hinfo) return lnb_set_error(LNB_ENOMEM, "host buffer");
         cudaError_t e = cudaMemcpyAsync(hinfo, info, (size_t)nblk * 4, cudaMemcpyDeviceToHost, s);
@@ -123,7 +130,7 @@ static int sp_setup(lnb_ctx *c, int n, int bm, const int *vptr, const int *vpos,
 /* z = M^-1 r (or a copy) */
 static int sp_precond(const sp_ws *w, const double *r, double *z, cudaStream_t s)
 {
-    if (w->fac) CK(lnb_k_bj_apply(w->n, w->bm, w->fac, r, z, s), "block-Jacobi apply");
+    if (w->fac) CK(lnb_k_bj_apply(w->n, w->bm, w->fac, w->env, r, z, s), "block-Jacobi apply");
     else CK(cudaMemcpyAsync(z, r, (size_t)w->n * 8, cudaMemcpyDeviceToDevice, s), "copy");
     return 0;
 }
