@@ -111,7 +111,8 @@ __global__ void __launch_bounds__(64) k_trsm_rlt_f32(const float *__restrict__ L
     __shared__ __align__(16) float Lc[2][32 * ptrsm::LDB];  // staged L_{j,kc}, [k][c]
     __shared__ __align__(16) float Ds[2][32 * ptrsm::LDB];  // Dinv_j, [q][c]
     __shared__ __align__(16) float Bs[2][32 * 32];          // B_j, [k][r]
-    __shared__ __align__(16) float Ts[32 * ptrsm::LDB];     // acc transposed, [q][r]
+    // finish(j) transposes acc ([q][r]) into the L buffer the finishing chunk
+    // has just consumed (34.8 KB per CTA: six CTAs per SM)
     using ptrsm::LDB;
     using ptrsm::NT;
     const int nj = (bs + 31) / 32;
@@ -121,7 +122,8 @@ __global__ void __launch_bounds__(64) k_trsm_rlt_f32(const float *__restrict__ L
 
     float acc[4][4];
     // X_j = acc Dinv_j^T, written to B and (optionally) as TF32 operands
-    auto finish = [&](int j) {
+    auto finish = [&](int j, float *Ts) {
+        __syncthreads();                  // every warp is done with the buffer Ts borrows
 #pragma unroll
         for (int c = 0; c < 4; ++c)
             *reinterpret_cast<float4 *>(Ts + (4 * cg + c) * LDB + 4 * rq) =
@@ -182,7 +184,7 @@ __global__ void __launch_bounds__(64) k_trsm_rlt_f32(const float *__restrict__ L
     cp_async_wait<0>();
     __syncthreads();
     load_b(0);
-    finish(0);
+    finish(0, Lc[0]);                     // nothing is staged in Lc yet
     __syncthreads();                      // X_0 is in B before chunk (1, 0) reads it back
     const int S = nj * (nj - 1) / 2;      // chunks (j, kc), kc < j, in j-major order
     if (S > 0) stage_chunk(0, 1, 0);
@@ -204,7 +206,7 @@ __global__ void __launch_bounds__(64) k_trsm_rlt_f32(const float *__restrict__ L
         for (int k = 0; k < 32; ++k)
             fma4x4(acc, *reinterpret_cast<const float4 *>(Xk + k * 32 + 4 * rq),
                    *reinterpret_cast<const float4 *>(Lb + k * LDB + 4 * cg), -1.f);
-        if (kc == j - 1) finish(j);
+        if (kc == j - 1) finish(j, Lc[s & 1]);   // this chunk's L buffer; the next chunk's is the other
         __syncthreads();
         j = jn; kc = kn;
     }
