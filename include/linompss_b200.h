@@ -279,7 +279,8 @@ LNB_EXPORT int ompss_sgetrf_ll(int m, int n, int b, float *A, int lda, int *IPIV
 LNB_EXPORT int dgensolv_main(int m, int n, int b, double *A, double *B);
 LNB_EXPORT int sgensolv_main(int m, int n, int b, float *A, float *B);
 /* device forms: dipiv receives LAPACK pivots (1-based, global rows);
- * info_dev (may be NULL) the info value; asynchronous on `stream` */
+ * info_dev (may be NULL) the info value; asynchronous on `stream`.  Every LU
+ * entry point takes at most 32768 rows (LNB_ETOOBIG beyond). */
 LNB_EXPORT int lnb_dgetrf_dev(int m, int n, double *dA, int lda, int *dipiv, int *info_dev, void *stream);
 LNB_EXPORT int lnb_dgetrs_dev(int n, int nrhs, const double *dLU, int lda, const int *dipiv, double *dB, int ldb,
                               void *stream);
