@@ -125,3 +125,17 @@ def test_getrf_errors(lnb):
     A = np.asfortranarray(np.eye(4))
     with pytest.raises(lnb.LinompssError):
         lnb.ompss_getrf(A, 0)
+
+
+def test_getrf_rows_limit(lnb):
+    """more rows than a panel cluster holds: LNB_ETOOBIG before any device work"""
+    A = np.asfortranarray(np.ones((32769, 2)))
+    with pytest.raises(lnb.LinompssError) as e:
+        lnb.ompss_getrf(A, 2)
+    assert e.value.code == lnb.LNB_ETOOBIG
+    A = np.asfortranarray(np.random.default_rng(3).standard_normal((32768, 4)))
+    lu, piv, _ = la.dgetrf(A)
+    info, ipiv = lnb.ompss_getrf(A, 4)
+    assert info == 0
+    np.testing.assert_array_equal(np.arange(4) + ipiv, piv + 1)
+    np.testing.assert_allclose(A, lu, rtol=0, atol=1e-12)
