@@ -4,7 +4,8 @@ C ABI:
     ompss_dgetrf and dgensolv_main on its GENMAT_IP matrix distribution);
   * against LAPACK (scipy) on matrices where pivoting happens: the same pivot
     sequence and factor for every panel width, ragged last panels, tall,
-    wide, and tall enough that a panel spans a cluster of several CTAs;
+    wide, and tall enough that a panel spans a cluster of several CTAs (each
+    panel shape: 32 columns to 4096 rows, 16 to 8192, 8 to 16384, 4 to 32768);
   * exactly singular columns: LAPACK's info, the factorization completed;
   * FP32 twins, the _ll drivers, and the device entry points.
 Tolerances: blocked FP64 sums in another order agree to ~1e-12 relative."""
