@@ -1214,8 +1214,20 @@ def case_lu(n):
         lnb.dgetrf_dev(A, n, n, piv)
 
 
+def case_batched(count):
+    """the batched solver (configuration 5's distribution, `count` systems), autotuned, then 2 calls"""
+    import torch
+    import linompss_b200 as lnb
+    ns, rs = batch_shape(count, 4321)
+    ns, rs, a_off, b_off, nd, rd, ao, bo, dA, dB = make_batch(ns, rs, 4321, torch.device("cuda", 0))
+    dX = torch.zeros_like(dB)
+    lnb.batched_autotune(nd, rd, ao, bo, dA, dB, dX, lnb.FACTOR_FP32, 10)
+    for _ in range(2):
+        lnb.batched_posv_dev(nd, rd, ao, bo, dA, dB, dX, lnb.FACTOR_FP32, 10)
+
+
 CASES = {"symv8": (case_symv8, 16384), "syrk": (case_syrk, 8192), "dag": (case_dag, 4096),
-         "bf16": (case_bf16, 16384), "lu": (case_lu, 1500)}
+         "bf16": (case_bf16, 16384), "lu": (case_lu, 1500), "batched": (case_batched, 2000)}
 
 
 def main():
