@@ -266,12 +266,20 @@ def measure_peaks(device):
 # ----------------------------------------------------------------------------
 # CPU: the reference build (oracle/_ref) or the oracle port, bounded sample
 # ----------------------------------------------------------------------------
+# The reference's external BLAS (the OpenBLAS 0.3.15 build it links here) picks
+# its kernels by CPU; on the benchmark host its default choice ran dspdsolv_main
+# at n = 32768 in 53.4 s and the Haswell kernels in 32.9 s, with the same
+# backward error (1.9e-17 / 2.0e-17).  The baseline runs the faster one.
+OPENBLAS_CORETYPE = "Haswell"
+
+
 def cpu_run(n, b, nrhs, steps, warmup, A_host=None):
     """Times dspdsolv_main of the reference build (OpenBLAS, all host threads)
     on an n x n sample; returns (TFLOP/s, kind, cores, seconds per step)."""
     import numpy as np
     cores = os.cpu_count() or 1
     os.environ["OPENBLAS_NUM_THREADS"] = str(cores)
+    os.environ.setdefault("OPENBLAS_CORETYPE", OPENBLAS_CORETYPE)
     from oracle import oracle as O
     kind = "reference" if O.ref_available() else "port"
     if A_host is None:
@@ -332,6 +340,7 @@ def reference_arm(args, world, rank):
     n, b, nrhs = w["n"], w["b"], w["nrhs"]
     cores = os.cpu_count() or 1
     os.environ["OPENBLAS_NUM_THREADS"] = str(cores)
+    os.environ.setdefault("OPENBLAS_CORETYPE", OPENBLAS_CORETYPE)
     from oracle import oracle as O
     kind = "reference" if O.ref_available() else "port"
     import torch
@@ -342,8 +351,10 @@ def reference_arm(args, world, rank):
     solve = O.ref_spdsolv if kind == "reference" else O.spdsolv
     nw = min(n, 4096)
     for _ in range(args.warmup):
-        A = np.asfortranarray(A0[:nw, :nw])
-        B = np.asfortranarray(B0[:nw])
+        # copies: asfortranarray of B0[:nw] (n x 1, already Fortran-ordered) would be a view,
+        # and the warm-up solve would overwrite the timed call's right-hand side
+        A = np.array(A0[:nw, :nw], order="F")
+        B = np.array(B0[:nw], order="F")
         solve(A, B, min(b, nw))
     times = []
     A = np.empty_like(A0, order="F")
@@ -372,8 +383,9 @@ def reference_arm(args, world, rank):
             "result": {"backward_error": be},
             "cpu_baseline": {"value": round(v, 6), "unit": UNIT, "cores": cores, "kind": kind,
                              "sample": f"the full workload: dspdsolv_main n={n} b={b} nrhs={nrhs} on the same "
-                                       f"seeded inputs, OpenBLAS threads={cores}, mean of {len(times)} call(s); "
-                                       f"warm-up on the leading {nw} x {nw} block"},
+                                       f"seeded inputs, OpenBLAS threads={cores} "
+                                       f"({os.environ.get('OPENBLAS_CORETYPE')} kernels), mean of {len(times)} "
+                                       f"call(s); warm-up on the leading {nw} x {nw} block"},
             "e2e": {"value": round(v, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -774,6 +786,7 @@ def blas_records(args, world, rank, dev, peaks):
     import linompss_b200 as lnb
     cores = os.cpu_count() or 1
     os.environ["OPENBLAS_NUM_THREADS"] = str(cores)
+    os.environ.setdefault("OPENBLAS_CORETYPE", OPENBLAS_CORETYPE)
     s = torch.cuda.current_stream()
     reps = max(1, min(args.steps, 3))
     out = {}
