@@ -350,28 +350,145 @@ __global__ void k_equil_scale(const double *A, int64_t lda, int64_t n, int on, d
     }
 }
 
-// lower triangle of S A S in FP32 (column-major, ld32); column j per blockIdx.y
-__global__ void k_lower_to_f32(const double *__restrict__ A, int64_t lda, int64_t n, const double *__restrict__ s,
-                               float *A32, int64_t ld32)
+// lower(S A S) in FP32 for columns [c0, c1), rows >= column (column-major,
+// ld32), in tiles of 128 rows x 64 columns.  With rsum != NULL the absolute
+// values of the FP64 A are summed as well: rsum[i] += |a_ij| for i >= j and
+// rsum[j] += |a_ij| for i > j, so that once every column has passed, rsum
+// holds the row sums of |A| for the symmetric matrix whose lower triangle A
+// stores (its infinity norm is their maximum).  Tile sums are added with FP64
+// atomics, so the last bits of rsum depend on their order.
+//
+// Persistent blocks walk the tiles column tile by column tile (a cursor that
+// only moves forward).  Warp w takes columns 8w..8w+7 of a tile and lane l
+// rows 2l, 2l+1, 64+2l, 65+2l: all 16 loads of a thread are issued before the
+// first use.  vec: A 16-byte aligned with lda even, A32 8-byte aligned with
+// ld32 even (pairs of rows move as double2 / float2).
+namespace cvt {
+constexpr int TR = 128, TC = 64, NT = 256;
+}
+
+__global__ void __launch_bounds__(cvt::NT, 2) k_lower_to_f32_t(const double *__restrict__ A, int64_t lda, int64_t n,
+                                                           int64_t c0, int64_t c1, const double *__restrict__ s,
+                                                           float *__restrict__ A32, int64_t ld32,
+                                                           double *__restrict__ rsum, int vec)
 {
-    for (int64_t j = blockIdx.y; j < n; j += gridDim.y) {
-        const double sj = s[j];
-        for (int64_t i = j + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-             i += (int64_t)gridDim.x * blockDim.x)
-            A32[i + j * ld32] = (float)(A[i + j * lda] * s[i] * sj);
+    __shared__ double red[8][cvt::TR];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t r0 = c0 & ~(int64_t)(cvt::TR - 1);
+    const int64_t nrt = (n - r0 + cvt::TR - 1) / cvt::TR;
+    const int64_t nct = (c1 - c0 + cvt::TC - 1) / cvt::TC;
+    int64_t cj = 0, base = 0;
+    for (int64_t t = blockIdx.x;; t += gridDim.x) {
+        // the column tile holding tile t: column tile cj has the row tiles
+        // from the one holding its first column down to the last
+        int64_t first;
+        for (;;) {
+            if (cj >= nct) return;
+            first = (c0 + cj * cvt::TC - r0) / cvt::TR;
+            if (t < base + nrt - first) break;
+            base += nrt - first;
+            ++cj;
+        }
+        const int64_t j0 = c0 + cj * cvt::TC;
+        const int64_t i0 = r0 + (first + t - base) * cvt::TR;
+        // offsets within the tile: row r = i - i0 is in the triangle and the
+        // matrix when lo_c <= r < hi, lo_c = j - i0 for column j (clamped)
+        const int hi = n - i0 < cvt::TR ? (int)(n - i0) : cvt::TR;
+        const int64_t jw = j0 + warp * 8;
+        const int ncol = c1 - jw < 8 ? (int)(c1 - jw) : 8;    // columns of this warp (may be <= 0)
+        const int lo0 = jw - i0 < -8 ? -8 : (jw - i0 > cvt::TR ? cvt::TR : (int)(jw - i0));
+        const double *pa = A + i0 + jw * lda;
+        double v[8][4];
+#pragma unroll
+        for (int cc = 0; cc < 8; ++cc) {
+            const int lo = lo0 + cc;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = 64 * h + 2 * lane;
+                const bool in0 = cc < ncol && r >= lo && r < hi, in1 = cc < ncol && r + 1 >= lo && r + 1 < hi;
+                const double *p = pa + cc * lda + r;
+                if (vec && in0 && in1) {
+                    const double2 q = __ldcs(reinterpret_cast<const double2 *>(p));
+                    v[cc][2 * h] = q.x;
+                    v[cc][2 * h + 1] = q.y;
+                } else {
+                    v[cc][2 * h] = in0 ? __ldcs(p) : 0.0;
+                    v[cc][2 * h + 1] = in1 ? __ldcs(p + 1) : 0.0;
+                }
+            }
+        }
+        double si[4], rs[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int r = 64 * (u >> 1) + 2 * lane + (u & 1);
+            si[u] = r < hi ? s[i0 + r] : 0.0;
+        }
+        float *pq = A32 + i0 + jw * ld32;
+#pragma unroll
+        for (int cc = 0; cc < 8; ++cc) {
+            if (cc >= ncol) break;                      // warp-uniform
+            const int lo = lo0 + cc;
+            const double sj = s[jw + cc];
+            float o[4];
+            double cs = 0.0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int r = 64 * (u >> 1) + 2 * lane + (u & 1);
+                o[u] = (float)(v[cc][u] * si[u] * sj);
+                const double a = fabs(v[cc][u]);      // 0 outside the triangle
+                rs[u] += a;
+                if (r > lo) cs += a;
+            }
+            float *q = pq + cc * ld32;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = 64 * h + 2 * lane;
+                const bool in0 = r >= lo && r < hi, in1 = r + 1 >= lo && r + 1 < hi;
+                if (vec && in0 && in1) {
+                    *reinterpret_cast<float2 *>(q + r) = make_float2(o[2 * h], o[2 * h + 1]);
+                } else {
+                    if (in0) q[r] = o[2 * h];
+                    if (in1) q[r + 1] = o[2 * h + 1];
+                }
+            }
+            if (rsum) {
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, d);
+                if (lane == 0 && cs != 0.0) atomicAdd(rsum + jw + cc, cs);
+            }
+        }
+        if (rsum) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) red[warp][64 * (u >> 1) + 2 * lane + (u & 1)] = rs[u];
+            __syncthreads();
+            if (threadIdx.x < cvt::TR) {
+                double sum = 0.0;
+#pragma unroll
+                for (int w = 0; w < 8; ++w) sum += red[w][threadIdx.x];
+                if ((int)threadIdx.x < hi && sum != 0.0) atomicAdd(rsum + i0 + threadIdx.x, sum);
+            }
+            __syncthreads();
+        }
     }
 }
 
-// columns [c0, c1) of the lower triangle of S A S in FP32; column c0 + blockIdx.y
-__global__ void k_lower_to_f32_cols(const double *__restrict__ A, int64_t lda, int64_t n, int64_t c0, int64_t c1,
-                                    const double *__restrict__ s, float *A32, int64_t ld32)
+static int launch_lower_to_f32(const double *A, int64_t lda, int64_t n, int64_t c0, int64_t c1, const double *S,
+                               float *A32, int64_t ld32, double *rsum, cudaStream_t s)
 {
-    for (int64_t j = c0 + blockIdx.y; j < c1; j += gridDim.y) {
-        const double sj = s[j];
-        for (int64_t i = j + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-             i += (int64_t)gridDim.x * blockDim.x)
-            A32[i + j * ld32] = (float)(A[i + j * lda] * s[i] * sj);
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0, v = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        sms = v;
     }
+    const int vec = ((uintptr_t)A % 16 == 0) && (lda % 2 == 0) && ((uintptr_t)A32 % 8 == 0) && (ld32 % 2 == 0);
+    const int64_t r0 = c0 & ~(int64_t)(cvt::TR - 1);
+    const int64_t tiles = ((n - r0 + cvt::TR - 1) / cvt::TR) * ((c1 - c0 + cvt::TC - 1) / cvt::TC);
+    const int64_t grid = tiles < 4LL * sms ? tiles : 4LL * sms;
+    k_lower_to_f32_t<<<(unsigned)grid, cvt::NT, 0, s>>>(A, lda, n, c0, c1, S, A32, ld32, rsum, vec);
+    lnb_prof_count(1);
+    return (int)cudaGetLastError();
 }
 
 }  // namespace lnb
@@ -379,14 +496,10 @@ __global__ void k_lower_to_f32_cols(const double *__restrict__ A, int64_t lda, i
 using namespace lnb;
 
 extern "C" int lnb_k_lower_to_f32_cols(const double *A, int64_t lda, int64_t n, int64_t c0, int64_t c1,
-                                       const double *S, float *A32, int64_t ld32, lnb_stream_t s)
+                                       const double *S, float *A32, int64_t ld32, double *rsum, lnb_stream_t s)
 {
     if (c1 <= c0 || c0 >= n) return 0;
-    const int64_t rows = n - c0;
-    dim3 grid((unsigned)((rows + 255) / 256 < 32 ? (rows + 255) / 256 : 32), (unsigned)(c1 - c0 < 65535 ? c1 - c0 : 65535));
-    k_lower_to_f32_cols<<<grid, 256, 0, s>>>(A, lda, n, c0, c1, S, A32, ld32);
-    lnb_prof_count(1);
-    return (int)cudaGetLastError();
+    return launch_lower_to_f32(A, lda, n, c0, c1 < n ? c1 : n, S, A32, ld32, rsum, s);
 }
 
 extern "C" int lnb_k_equil_scale_vec(const double *a, int64_t n, int on, double *s_out, lnb_stream_t s)
@@ -459,16 +572,13 @@ extern "C" int lnb_k_prep_bf16(const float *X, int64_t ldx, int64_t m, int kb, i
 }
 
 extern "C" int lnb_k_lower_to_f32(const double *A, int64_t lda, int64_t n, int equilibrate, double *s_out,
-                                  float *A32, int64_t ld32, lnb_stream_t s)
+                                  float *A32, int64_t ld32, double *rsum, lnb_stream_t s)
 {
     if (n <= 0) return 0;
     k_equil_scale<<<(unsigned)((n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024), 256, 0, s>>>(A, lda, n, equilibrate,
                                                                                              s_out);
     lnb_prof_count(1);
-    dim3 grid((unsigned)((n + 255) / 256 < 32 ? (n + 255) / 256 : 32), (unsigned)(n < 65535 ? n : 65535));
-    k_lower_to_f32<<<grid, 256, 0, s>>>(A, lda, n, s_out, A32, ld32);
-    lnb_prof_count(1);
-    return (int)cudaGetLastError();
+    return launch_lower_to_f32(A, lda, n, 0, n, s_out, A32, ld32, rsum, s);
 }
 
 // ------------------------------------------------------------------------

@@ -310,7 +310,7 @@ static int join_cols(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode,
 {
     const int64_t c0 = (int64_t)j0 * b, c1 = ((int64_t)j1 + 1) * b < n ? ((int64_t)j1 + 1) * b : n;
     for (int j = j0; j <= j1; ++j) CK(cudaStreamWaitEvent(s, in->arr[j], 0), "arrival wait");
-    CK(lnb_k_lower_to_f32_cols(in->A, in->lda, n, c0, c1, in->S, dA, lda, s), "convert");
+    CK(lnb_k_lower_to_f32_cols(in->A, in->lda, n, c0, c1, in->S, dA, lda, in->rsum, s), "convert");
     if (kdone > 0)
         CK(upd_tc(mode, HA + c0 * ldk, LA ? LA + c0 * ldk : NULL, ldk, dA + c0 + c0 * lda, lda, n - c0, 0, c1 - c0,
                   kdone * b, c->st, s), "catch-up update");

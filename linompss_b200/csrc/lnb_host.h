@@ -99,12 +99,15 @@ int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode,
 int lnb_get_factor_mode(void);
 /* A matrix arriving block column by block column on another stream: block
  * column j (columns [j b, (j+1) b), rows >= j b) of the FP64 copy A is
- * complete once arr[j] has fired; S is the equilibration scale on the device. */
+ * complete once arr[j] has fired; S is the equilibration scale on the device;
+ * rsum (NULL, or n zeroed doubles) gains the row sums of |A| as the block
+ * columns are converted. */
 typedef struct {
     const double *A;
     int64_t lda;
     const double *S;
     cudaEvent_t *arr;
+    double *rsum;
 } lnb_stream_in;
 int lnb_chol_f32_stream_ok(int n, int b, int mode);
 size_t lnb_chol_f32_stream_ws_bytes(int n, int b, int mode);

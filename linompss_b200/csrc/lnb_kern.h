@@ -101,12 +101,15 @@ int lnb_k_syrk_lower_f32_simt(const float *P, int64_t ldp, float *C, int64_t ldc
  * per-128-row power-of-two scales (the TF32 copies come from the panel solve) */
 int lnb_k_prep_bf16(const float *X, int64_t ldx, int64_t m, int kb, int kpad, float *scale, void *out,
                     lnb_stream_t s);
-/* A32 = lower(S A S) in FP32 with S = diag(1/sqrt(a_ii)) (S = I if !equilibrate) */
+/* A32 = lower(S A S) in FP32 with S = diag(1/sqrt(a_ii)) (S = I if !equilibrate);
+ * rsum (may be NULL, else zeroed by the caller) gains the row sums of |A| of
+ * the symmetric A whose lower triangle is given, for its infinity norm */
 int lnb_k_lower_to_f32(const double *A, int64_t lda, int64_t n, int equilibrate, double *s_out,
-                       float *A32, int64_t ld32, lnb_stream_t s);
-/* A32 columns [c0, c1), rows >= column: lower(S A S) in FP32, S given */
+                       float *A32, int64_t ld32, double *rsum, lnb_stream_t s);
+/* A32 columns [c0, c1), rows >= column: lower(S A S) in FP32, S given; rsum as
+ * above, for the elements of these columns */
 int lnb_k_lower_to_f32_cols(const double *A, int64_t lda, int64_t n, int64_t c0, int64_t c1, const double *S,
-                            float *A32, int64_t ld32, lnb_stream_t s);
+                            float *A32, int64_t ld32, double *rsum, lnb_stream_t s);
 /* s[i] = 1/sqrt(a[i]) (1 when !on or a[i] <= 0) from a packed diagonal; s may alias a */
 int lnb_k_equil_scale_vec(const double *a, int64_t n, int on, double *s, lnb_stream_t st);
 /* tensor-core lower update (k_tc_update.cu); mode 0 TF32x3, 1 TF32, 2 BF16.

@@ -62,7 +62,8 @@ void lnb_ir_default_opts(lnb_ir_opts *o)
 typedef struct {
     int64_t n, nrhs, ld32;
     float *A32;
-    double *S, *dinv, *R, *Z, *Y, *P, *Q, *ones, *scal; /* scal: 8 * nrhs scalars */
+    double *S, *dinv, *R, *Z, *Y, *P, *Q, *scal; /* scal: 8 * nrhs scalars */
+    double *rsum;           /* row sums of |A|, accumulated by the FP32 conversion */
     int *sync;
     /* solves on the inverses of the large diagonal blocks (k_trsv_blk.cu), when they apply */
     float *binv;
@@ -187,7 +188,7 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
     const int64_t nb = ((int64_t)n + TRSV_H - 1) / TRSV_H;
     w.A32 = lnb_arena_take(&ar, (size_t)w.ld32 * n * 4);
     w.S = lnb_arena_take(&ar, (size_t)n * 8);
-    w.ones = lnb_arena_take(&ar, (size_t)n * 8);
+    w.rsum = lnb_arena_take(&ar, (size_t)n * 8);
     w.dinv = lnb_arena_take(&ar, (size_t)nb * TRSV_H * TRSV_H * 8);
     w.R = lnb_arena_take(&ar, (size_t)n * nrhs * 8);
     w.Z = lnb_arena_take(&ar, (size_t)n * nrhs * 8);
@@ -221,13 +222,16 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
     lnb_refactor_ctx rf = {dA, lda, w.S, 0, 0, mode == LNB_FACTOR_BF16};
     const lnb_arena ar_factor = ar;   /* a rerun carves the same workspace again */
     int e;
+    /* the conversion to FP32 reads every element of the lower triangle once;
+     * it also sums |A| by rows for ||A||_inf */
+    CK(cudaMemsetAsync(w.rsum, 0, (size_t)n * 8, s), "row sums");
     if (in) {
         /* the matrix is converted block column by block column as it arrives */
         CK(cudaMemcpyAsync(w.S, in->dS, (size_t)n * 8, cudaMemcpyDeviceToDevice, s), "scale");
-        const lnb_stream_in sin = {dA, lda, w.S, in->arr};
+        const lnb_stream_in sin = {dA, lda, w.S, in->arr, w.rsum};
         e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, &sin, &ar, s);
     } else {
-        CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, s), "convert");
+        CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, w.rsum, s), "convert");
         /* every panel's operands kept: columns beyond the look-ahead take their
          * panels two at a time, halving the passes over the trailing matrix */
         if (lnb_chol_f32_stream_ok(n, b, mode))
@@ -247,7 +251,8 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
             rf.check = 1;
             ar = ar_factor;
             CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
-            CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, s), "convert");
+            /* the row sums are complete from the first pass */
+            CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, NULL, s), "convert");
             if (lnb_chol_f32_stream_ok(n, b, mode))
                 e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, NULL, &ar, s);
             else
@@ -279,19 +284,13 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
     CK(cudaEventRecord(c->t0, s), "event");
     double anorm, bmax[64];
     {
-        /* ||A||_inf = max row sum of |A|, from the lower triangle (symv of |A| with ones) */
+        /* ||A||_inf = max row sum of |A|, summed by the conversion */
         double h = 0.0;
-        double *hones = (double *)malloc((size_t)n * 8);
-        if (!hones) return lnb_set_error(LNB_ENOMEM, "host ones");
-        for (int64_t i = 0; i < n; ++i) hones[i] = 1.0;
-        CK(cudaMemcpyAsync(w.ones, hones, (size_t)n * 8, cudaMemcpyHostToDevice, s), "ones");
-        CK(lnb_k_symv_lower_f64(n, 1, dA, lda, w.ones, w.Y, 1, s), "row sums");
-        CK(lnb_k_colmax_f64(n, 1, w.Y, n, w.scal, s), "max");
+        CK(lnb_k_colmax_f64(n, 1, w.rsum, n, w.scal, s), "max");
         CK(lnb_k_colmax_f64(n, nrhs, dB, ldb, w.scal + 1, s), "bmax");
         CK(cudaMemcpyAsync(&h, w.scal, 8, cudaMemcpyDeviceToHost, s), "read");
         CK(cudaMemcpyAsync(bmax, w.scal + 1, (size_t)nrhs * 8, cudaMemcpyDeviceToHost, s), "read");
         CK(cudaStreamSynchronize(s), "sync");
-        free(hones);
         anorm = h;
     }
 

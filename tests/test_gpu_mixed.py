@@ -193,3 +193,33 @@ def test_ir_device_path_panel_grouping(lnb, cuda, monkeypatch, depth):
     assert rc == 0, (res, lnb.last_error())
     assert O.backward_error_np(A0, Xt.cpu().numpy().T, B0) <= 10 * n * EPS
     assert res["iterations"] <= 4 and not res["used_pcg"]
+
+
+@pytest.mark.parametrize("api,n", [("host", 2048), ("host", 1999), ("device", 2048), ("device", 1999)])
+def test_ir_reported_backward_error(lnb, cuda, api, n):
+    """The backward error the solver reports after one refinement step equals
+    the oracle's on the returned X: ||A||_inf comes from the row sums of |A|
+    that the FP32 conversion accumulates (both triangles of the symmetric A
+    from its lower one), on the streamed host path and the device path, with
+    an even and an odd leading dimension.  After one step the residual is far
+    above its rounding noise, so the two agree to ~1e-8 relative."""
+    import torch
+    b = 256
+    rng = np.random.default_rng(n + 40)
+    d = 10.0 ** rng.uniform(-1, 1, n)
+    A0 = np.asfortranarray(O.spd_covariance(n, 1e-2, seed=n) * d[:, None] * d[None, :])
+    B0 = np.asfortranarray(rng.standard_normal((n, 1)))   # one column: the oracle's max is over all
+    opts = lnb.ir_opts(factor=lnb.FACTOR_TF32X3, max_iter=1, allow_pcg=0)
+    if api == "host":
+        rc, X, res = lnb.dsposv_ir(A0.copy(order="F"), B0, b, opts)
+    else:
+        At = torch.tensor(np.ascontiguousarray(A0.T), device=cuda)
+        Bt = torch.tensor(np.ascontiguousarray(B0.T), device=cuda)
+        Xt = torch.zeros_like(Bt)
+        rc, res = lnb.dsposv_ir_dev(At, Bt, Xt, n, 1, b, opts)
+        torch.cuda.synchronize()
+        X = Xt.cpu().numpy().T
+    assert rc in (0, lnb.LNB_ENOCONV), (rc, lnb.last_error())
+    be = O.backward_error_np(A0, X, B0)
+    assert be > 1e3 * n * EPS, be          # far from the rounding level of the residual
+    assert abs(res["backward_error"] - be) <= 1e-6 * be, (res["backward_error"], be)
