@@ -367,7 +367,7 @@ namespace cvt {
 constexpr int TR = 128, TC = 64, NT = 256;
 }
 
-__global__ void __launch_bounds__(cvt::NT, 2) k_lower_to_f32_t(const double *__restrict__ A, int64_t lda, int64_t n,
+__global__ void __launch_bounds__(cvt::NT, 3) k_lower_to_f32_t(const double *__restrict__ A, int64_t lda, int64_t n,
                                                            int64_t c0, int64_t c1, const double *__restrict__ s,
                                                            float *__restrict__ A32, int64_t ld32,
                                                            double *__restrict__ rsum, int vec)
@@ -398,25 +398,6 @@ __global__ void __launch_bounds__(cvt::NT, 2) k_lower_to_f32_t(const double *__r
         const int ncol = c1 - jw < 8 ? (int)(c1 - jw) : 8;    // columns of this warp (may be <= 0)
         const int lo0 = jw - i0 < -8 ? -8 : (jw - i0 > cvt::TR ? cvt::TR : (int)(jw - i0));
         const double *pa = A + i0 + jw * lda;
-        double v[8][4];
-#pragma unroll
-        for (int cc = 0; cc < 8; ++cc) {
-            const int lo = lo0 + cc;
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = 64 * h + 2 * lane;
-                const bool in0 = cc < ncol && r >= lo && r < hi, in1 = cc < ncol && r + 1 >= lo && r + 1 < hi;
-                const double *p = pa + cc * lda + r;
-                if (vec && in0 && in1) {
-                    const double2 q = __ldcs(reinterpret_cast<const double2 *>(p));
-                    v[cc][2 * h] = q.x;
-                    v[cc][2 * h + 1] = q.y;
-                } else {
-                    v[cc][2 * h] = in0 ? __ldcs(p) : 0.0;
-                    v[cc][2 * h + 1] = in1 ? __ldcs(p + 1) : 0.0;
-                }
-            }
-        }
         double si[4], rs[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -424,37 +405,66 @@ __global__ void __launch_bounds__(cvt::NT, 2) k_lower_to_f32_t(const double *__r
             si[u] = r < hi ? s[i0 + r] : 0.0;
         }
         float *pq = A32 + i0 + jw * ld32;
+        // two passes of 4 columns: the loads of a pass are all issued before
+        // their first use, and the registers leave room for 3 blocks per SM
 #pragma unroll
-        for (int cc = 0; cc < 8; ++cc) {
-            if (cc >= ncol) break;                      // warp-uniform
-            const int lo = lo0 + cc;
-            const double sj = s[jw + cc];
-            float o[4];
-            double cs = 0.0;
+        for (int p = 0; p < 2; ++p) {
+            double v[4][4], sj[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                const int r = 64 * (u >> 1) + 2 * lane + (u & 1);
-                o[u] = (float)(v[cc][u] * si[u] * sj);
-                const double a = fabs(v[cc][u]);      // 0 outside the triangle
-                rs[u] += a;
-                if (r > lo) cs += a;
+            for (int c4 = 0; c4 < 4; ++c4) {
+                const int cc = 4 * p + c4, lo = lo0 + cc;
+                sj[c4] = cc < ncol ? s[jw + cc] : 0.0;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int r = 64 * h + 2 * lane;
+                    const bool in0 = cc < ncol && r >= lo && r < hi, in1 = cc < ncol && r + 1 >= lo && r + 1 < hi;
+                    const double *q = pa + cc * lda + r;
+                    if (vec && in0 && in1) {
+                        const double2 w = __ldcs(reinterpret_cast<const double2 *>(q));
+                        v[c4][2 * h] = w.x;
+                        v[c4][2 * h + 1] = w.y;
+                    } else {
+                        v[c4][2 * h] = in0 ? __ldcs(q) : 0.0;
+                        v[c4][2 * h + 1] = in1 ? __ldcs(q + 1) : 0.0;
+                    }
+                }
             }
-            float *q = pq + cc * ld32;
+            double cs[4];
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = 64 * h + 2 * lane;
-                const bool in0 = r >= lo && r < hi, in1 = r + 1 >= lo && r + 1 < hi;
-                if (vec && in0 && in1) {
-                    *reinterpret_cast<float2 *>(q + r) = make_float2(o[2 * h], o[2 * h + 1]);
-                } else {
-                    if (in0) q[r] = o[2 * h];
-                    if (in1) q[r + 1] = o[2 * h + 1];
+            for (int c4 = 0; c4 < 4; ++c4) {
+                const int cc = 4 * p + c4, lo = lo0 + cc;
+                cs[c4] = 0.0;
+                if (cc >= ncol) continue;                   // warp-uniform
+                float o[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int r = 64 * (u >> 1) + 2 * lane + (u & 1);
+                    o[u] = (float)(v[c4][u] * si[u] * sj[c4]);
+                    const double a = fabs(v[c4][u]);      // 0 outside the triangle
+                    rs[u] += a;
+                    if (r > lo) cs[c4] += a;
+                }
+                float *q = pq + cc * ld32;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int r = 64 * h + 2 * lane;
+                    const bool in0 = r >= lo && r < hi, in1 = r + 1 >= lo && r + 1 < hi;
+                    if (vec && in0 && in1) {
+                        *reinterpret_cast<float2 *>(q + r) = make_float2(o[2 * h], o[2 * h + 1]);
+                    } else {
+                        if (in0) q[r] = o[2 * h];
+                        if (in1) q[r + 1] = o[2 * h + 1];
+                    }
                 }
             }
             if (rsum) {
+                // the 4 column sums reduced over the warp side by side
 #pragma unroll
-                for (int d = 16; d > 0; d >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, d);
-                if (lane == 0 && cs != 0.0) atomicAdd(rsum + jw + cc, cs);
+                for (int d = 16; d > 0; d >>= 1)
+#pragma unroll
+                    for (int c4 = 0; c4 < 4; ++c4) cs[c4] += __shfl_xor_sync(0xffffffffu, cs[c4], d);
+                const double mine = lane == 0 ? cs[0] : lane == 1 ? cs[1] : lane == 2 ? cs[2] : cs[3];
+                if (lane < 4 && 4 * p + lane < ncol && mine != 0.0) atomicAdd(rsum + jw + 4 * p + lane, mine);
             }
         }
         if (rsum) {
@@ -475,17 +485,18 @@ __global__ void __launch_bounds__(cvt::NT, 2) k_lower_to_f32_t(const double *__r
 static int launch_lower_to_f32(const double *A, int64_t lda, int64_t n, int64_t c0, int64_t c1, const double *S,
                                float *A32, int64_t ld32, double *rsum, cudaStream_t s)
 {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0, v = 148;
+    static int slots = 0;      // resident blocks on the whole GPU
+    if (!slots) {
+        int dev = 0, sms = 148, per = 1;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
-        sms = v;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_lower_to_f32_t, cvt::NT, 0);
+        slots = sms * (per > 0 ? per : 1);
     }
     const int vec = ((uintptr_t)A % 16 == 0) && (lda % 2 == 0) && ((uintptr_t)A32 % 8 == 0) && (ld32 % 2 == 0);
     const int64_t r0 = c0 & ~(int64_t)(cvt::TR - 1);
     const int64_t tiles = ((n - r0 + cvt::TR - 1) / cvt::TR) * ((c1 - c0 + cvt::TC - 1) / cvt::TC);
-    const int64_t grid = tiles < 4LL * sms ? tiles : 4LL * sms;
+    const int64_t grid = tiles < slots ? tiles : slots;
     k_lower_to_f32_t<<<(unsigned)grid, cvt::NT, 0, s>>>(A, lda, n, c0, c1, S, A32, ld32, rsum, vec);
     lnb_prof_count(1);
     return (int)cudaGetLastError();

@@ -26,6 +26,11 @@
         if (_e != 0) return lnb_cuda_error(_e, where);             \
     } while (0)
 
+/* the triangular solves' diagonal blocks: 64 x 64 inverses, and 512 x 512 ones
+ * built from them (k_trsv_blk.cu) */
+#define TRSV_H 64
+int lnb_k_trtri_hb_f32(const float *T, int64_t ldt, int64_t n, const float *dinv64, float *Binv, lnb_stream_t s);
+
 static int g_schol_mode = LNB_FACTOR_TF32X3;
 
 void lnb_set_factor_mode(int mode)
@@ -181,7 +186,8 @@ int lnb_chol_f32_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode,
 {
     /* TF32 update paths with whole 32-blocks: every panel's operands kept, far
      * columns updated several panels at a time */
-    if (lnb_chol_f32_stream_ok(n, b, mode)) return lnb_chol_f32_stream_run(c, n, b, dA, lda, mode, rf, NULL, ar, s);
+    if (lnb_chol_f32_stream_ok(n, b, mode))
+        return lnb_chol_f32_stream_run(c, n, b, dA, lda, mode, rf, NULL, NULL, ar, s);
     float *dinv = (float *)lnb_arena_take(ar, (size_t)((b + 31) / 32) * 1024 * sizeof(float));
     if (!dinv) return lnb_set_error(LNB_ENOMEM, "chol32 workspace");
     panelbuf pb;
@@ -340,8 +346,25 @@ static int apply_panels(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mo
     return 0;
 }
 
+/* inverses of the diagonal blocks of rows [r0, r1) of the factor dA, on the
+ * side stream once the critical stream has finished them; r0 and r1 whole
+ * 512-blocks (r1 may be n).  Sub-matrices give the same inverses as the whole:
+ * the blocks are independent. */
+static int blkinv_rows(lnb_ctx *c, const lnb_blkinv *inv, const float *dA, int64_t lda, int64_t n, int64_t r0,
+                       int64_t r1)
+{
+    CK(cudaEventRecord(c->ev[5], c->crit), "event");
+    CK(cudaStreamWaitEvent(c->aux, c->ev[5], 0), "event wait");
+    const float *T = dA + r0 + r0 * lda;
+    float *d64 = inv->dinv64 + (r0 / TRSV_H) * TRSV_H * TRSV_H;
+    CK(lnb_k_trtri_blocks_f32(T, lda, r1 - r0, TRSV_H, 'L', 0, d64, c->aux), "trtri");
+    if (inv->binv)
+        CK(lnb_k_trtri_hb_f32(T, lda, r1 - r0, d64, inv->binv + (r0 / 512) * 512 * 512, c->aux), "block inverses");
+    return 0;
+}
+
 int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_refactor_ctx *rf,
-                            const lnb_stream_in *in, lnb_arena *ar, cudaStream_t s)
+                            const lnb_stream_in *in, const lnb_blkinv *inv, lnb_arena *ar, cudaStream_t s)
 {
     if (!lnb_chol_f32_stream_ok(n, b, mode)) return lnb_set_error(LNB_EINVAL, "streamed factor: n %d, b %d", n, b);
     const int64_t ldk = ldk_of(n);
@@ -358,6 +381,7 @@ int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, in
     cudaEvent_t ev_start = c->ev[0], ev_trsm = c->ev[1], ev_next = c->ev[2], ev_done = c->ev[3];
     cudaEvent_t ev_pace = c->ev[4];
     int e = 0;
+    int64_t inv_rows = 0;     /* rows whose diagonal-block inverses are queued on the side stream */
 #define RUN(x)                   \
     do {                         \
         if ((e = (x)) != 0) goto out; \
@@ -387,6 +411,15 @@ int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, in
              * the previous step's diagonal factor, then queue this step */
             if (k > 0) RUN(ck_cuda(cudaEventSynchronize(ev_pace), "pace"));
             RUN(ck_cuda(cudaEventRecord(ev_pace, crit), "event"));
+        }
+        if (inv) {
+            /* the 512-blocks finished by this step: 8 + 8 small CTAs beside
+             * the update, so only the last block's inverse follows the factor */
+            const int64_t done = k0 + bs == n ? n : (k0 + bs) / 512 * 512;
+            if (done > inv_rows) {
+                RUN(blkinv_rows(c, inv, dA, lda, n, inv_rows, done));
+                inv_rows = done;
+            }
         }
         if (mrem <= 0) break;
         float *hk = HA + (k0 + bs) * ldk + k0, *lk = LA ? LA + (k0 + bs) * ldk + k0 : NULL;
@@ -443,6 +476,12 @@ int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, in
     RUN(ck_cuda(cudaStreamWaitEvent(s, ev_done, 0), "event wait"));
 out:
 #undef RUN
+    if (inv_rows > 0) {
+        /* s (and so whatever reuses this workspace next) follows the side stream */
+        int e2 = ck_cuda(cudaEventRecord(c->ev[6], c->aux), "event");
+        if (!e2) e2 = ck_cuda(cudaStreamWaitEvent(s, c->ev[6], 0), "event wait");
+        if (!e) e = e2;
+    }
     free(u);
     return e;
 }
@@ -544,14 +583,12 @@ int ompss_schol_hll(int mt, int b, int t, float **Ah) { (void)t; return schol_hy
  * The triangular solves with an FP32 factor compute in FP64 (k_trsv.cu reads
  * the FP32 tiles and accumulates in double); FP32 right-hand sides are
  * widened on the way in and rounded on the way out. */
-#define TRSV_H 64
 int lnb_k_f64_to_f32(const double *D, int64_t ldd, int64_t m, int64_t k, float *X, int64_t ldx, cudaStream_t st);
 
 int64_t lnb_trsm_blk_ints(int64_t n);
 int64_t lnb_trsm_blk_inv_floats(int64_t n);
 int64_t lnb_trsm_blk_vec_doubles(int64_t n, int64_t nrhs);
 int lnb_trsm_blk_ok(const float *T, int64_t ldt, int64_t n, int64_t nrhs);
-int lnb_k_trtri_hb_f32(const float *T, int64_t ldt, int64_t n, const float *dinv64, float *Binv, lnb_stream_t s);
 int lnb_k_trsm_blk_f32(char trans, int64_t n, int64_t nrhs, const float *T, int64_t ldt, const float *Binv, double *B,
                        int64_t ldb, double *vec, int *sync, lnb_status_t *st, long long wait_ns, int sms,
                        lnb_stream_t s);

@@ -23,6 +23,7 @@ typedef struct {
     cudaStream_t  main;        /* stream of the host-pointer entry points */
     cudaStream_t  crit;        /* high-priority stream: panel factorization */
     cudaStream_t  copy;        /* device->host panel copies */
+    cudaStream_t  aux;         /* low-priority stream: work beside the critical path */
     cudaEvent_t   ev[8];
     void         *ws;          /* grow-only device workspace */
     size_t        ws_size;
@@ -111,11 +112,20 @@ typedef struct {
 } lnb_stream_in;
 int lnb_chol_f32_stream_ok(int n, int b, int mode);
 size_t lnb_chol_f32_stream_ws_bytes(int n, int b, int mode);
+/* Inverses of the factor's diagonal blocks for the triangular solves that
+ * follow: the 64 x 64 ones into dinv64 (lnb_k_trtri_blocks_f32) and, when binv
+ * is not NULL, the 512 x 512 ones (lnb_k_trtri_hb_f32). */
+typedef struct {
+    float *dinv64;
+    float *binv;
+} lnb_blkinv;
 /* The FP32 factorization of lower(S A S) into dA, keeping every panel's
  * operand copies: while A arrives (in != NULL, dA filled block column by block
- * column), or with dA already complete (in == NULL). */
+ * column), or with dA already complete (in == NULL).  With inv != NULL the
+ * diagonal-block inverses are formed on the side stream as the diagonal tiles
+ * are finished, and are complete on s when the call's work is. */
 int lnb_chol_f32_stream_run(lnb_ctx *c, int n, int b, float *dA, int64_t lda, int mode, lnb_refactor_ctx *rf,
-                            const lnb_stream_in *in, lnb_arena *ar, cudaStream_t s);
+                            const lnb_stream_in *in, const lnb_blkinv *inv, lnb_arena *ar, cudaStream_t s);
 
 /* ---- FP64 triangular solves on device memory (lnb_solve.c) --------------- */
 size_t lnb_trsm_f64_ws_bytes(int64_t n, int64_t nrhs);

@@ -225,17 +225,21 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
     /* the conversion to FP32 reads every element of the lower triangle once;
      * it also sums |A| by rows for ||A||_inf */
     CK(cudaMemsetAsync(w.rsum, 0, (size_t)n * 8, s), "row sums");
+    /* on the streamed schedule the solves' diagonal-block inverses are formed
+     * beside the factorization, as its diagonal tiles are finished */
+    const lnb_blkinv inv = {(float *)w.dinv, w.binv};
+    const int streamed = in || lnb_chol_f32_stream_ok(n, b, mode);
     if (in) {
         /* the matrix is converted block column by block column as it arrives */
         CK(cudaMemcpyAsync(w.S, in->dS, (size_t)n * 8, cudaMemcpyDeviceToDevice, s), "scale");
         const lnb_stream_in sin = {dA, lda, w.S, in->arr, w.rsum};
-        e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, &sin, &ar, s);
+        e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, &sin, &inv, &ar, s);
     } else {
         CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, w.rsum, s), "convert");
         /* every panel's operands kept: columns beyond the look-ahead take their
          * panels two at a time, halving the passes over the trailing matrix */
-        if (lnb_chol_f32_stream_ok(n, b, mode))
-            e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, NULL, &ar, s);
+        if (streamed)
+            e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, NULL, &inv, &ar, s);
         else
             e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &rf, &ar, s);
     }
@@ -253,8 +257,8 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
             CK(cudaMemsetAsync(c->st, 0, sizeof(lnb_status_t), s), "status reset");
             /* the row sums are complete from the first pass */
             CK(lnb_k_lower_to_f32(dA, lda, n, opts.equilibrate, w.S, w.A32, w.ld32, NULL, s), "convert");
-            if (lnb_chol_f32_stream_ok(n, b, mode))
-                e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, NULL, &ar, s);
+            if (streamed)
+                e = lnb_chol_f32_stream_run(c, n, b, w.A32, w.ld32, mode, &rf, NULL, &inv, &ar, s);
             else
                 e = lnb_chol_f32_run(c, n, b, w.A32, w.ld32, mode, &rf, &ar, s);
         }
@@ -264,8 +268,10 @@ static int ir_run(lnb_ctx *c, int n, int nrhs, int b, const double *dA, int lda,
         if (e > 0 && res) { rr.info = e; *res = rr; }
         return e > 0 ? lnb_set_error(e, "low-precision factor: tile at row %d could not be refactored", e) : e;
     }
-    CK(lnb_k_trtri_blocks_f32(w.A32, w.ld32, n, TRSV_H, 'L', 0, (float *)w.dinv, s), "trtri");
-    if (w.binv) CK(lnb_k_trtri_hb_f32(w.A32, w.ld32, n, (const float *)w.dinv, w.binv, s), "block inverses");
+    if (!streamed) {
+        CK(lnb_k_trtri_blocks_f32(w.A32, w.ld32, n, TRSV_H, 'L', 0, (float *)w.dinv, s), "trtri");
+        if (w.binv) CK(lnb_k_trtri_hb_f32(w.A32, w.ld32, n, (const float *)w.dinv, w.binv, s), "block inverses");
+    }
     CK(cudaEventRecord(c->t1, s), "event");
     int info = lnb_status_read(c, s);
     if (info < 0) return info;

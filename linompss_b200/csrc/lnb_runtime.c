@@ -66,7 +66,8 @@ lnb_ctx *lnb_ctx_get(void)
         cudaDeviceGetStreamPriorityRange(&lo, &hi);
         int ok = cudaStreamCreateWithPriority(&c->crit, cudaStreamNonBlocking, hi) == cudaSuccess &&
                  cudaStreamCreateWithFlags(&c->main, cudaStreamNonBlocking) == cudaSuccess &&
-                 cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) == cudaSuccess;
+                 cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking) == cudaSuccess &&
+                 cudaStreamCreateWithPriority(&c->aux, cudaStreamNonBlocking, lo) == cudaSuccess;
         for (int i = 0; ok && i < 8; ++i)
             ok = cudaEventCreateWithFlags(&c->ev[i], cudaEventDisableTiming) == cudaSuccess;
         ok = ok && cudaEventCreate(&c->t0) == cudaSuccess && cudaEventCreate(&c->t1) == cudaSuccess;
