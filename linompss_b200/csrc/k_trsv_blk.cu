@@ -293,7 +293,6 @@ __global__ void __launch_bounds__(256) k_trtri_hb(const float *__restrict__ T, i
     double (*Bs)[TLD] = reinterpret_cast<double (*)[TLD]>(tsm + 64 * TLD);      // Bs[k][c] = B[k][c]
     double (*Cs)[TLD] = reinterpret_cast<double (*)[TLD]>(tsm + 128 * TLD);     // the sum, row-major
     const int cb = blockIdx.x, s = blockIdx.y, tid = threadIdx.x;
-    const int ty = tid >> 4, tx = tid & 15;      // rows 4 ty.., columns 4 tx..
     const int64_t o = (int64_t)s * HB;           // first row / column of the block
     const int64_t nb64 = (n + 63) / 64;
     float *Xb = Binv + (int64_t)s * HB * HB;     // block s: element (r, c) at Xb[r + c * HB]
@@ -303,13 +302,28 @@ __global__ void __launch_bounds__(256) k_trtri_hb(const float *__restrict__ T, i
             const int c = i >> 6, r = i & 63;
             Xb[(64 * a + r) + (int64_t)(64 * cb + c) * HB] = 0.f;
         }
+    // DMMA tiling of a 64 x 64 product: warp w owns rows m0 .. m0+15 and
+    // columns n0 .. n0+31 (4 fragments of 8); with the row stride TLD = 68 (4
+    // mod 16 doubles) the fragment loads of each half-warp hit distinct banks
+    const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t4 = lane & 3;
+    const int m0 = 16 * (warp & 3), n0 = 32 * (warp >> 2);
     for (int a = cb; a < HB / 64; ++a) {
         const int64_t q64 = (o + 64 * a) / 64;      // global 64-block index of diagonal block a
+        if (a == cb) {
+            // X_cb = D_cb (the identity past the 64-blocks of the factor)
+            for (int i = tid; i < 64 * 64; i += 256) {
+                const int c = i >> 6, r = i & 63;
+                Xb[(64 * a + r) + (int64_t)(64 * cb + c) * HB] =
+                    q64 < nb64 ? dinv64[q64 * 4096 + r + 64 * c] : (r == c ? 1.f : 0.f);
+            }
+            __syncthreads();
+            continue;
+        }
         double acc[4][4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+            for (int v = 0; v < 4; ++v) acc[j][v] = 0.0;
         // sum_{c=cb}^{a-1} L_ac X_c
         for (int c = cb; c < a; ++c) {
             __syncthreads();
@@ -321,26 +335,23 @@ __global__ void __launch_bounds__(256) k_trtri_hb(const float *__restrict__ T, i
                 Bs[kk][cc] = (double)Xb[(64 * c + kk) + (int64_t)(64 * cb + cc) * HB];
             }
             __syncthreads();
-#pragma unroll 8
-            for (int k = 0; k < 64; ++k) {
-                const double2 a0 = *reinterpret_cast<const double2 *>(&As[k][4 * ty]);
-                const double2 a1 = *reinterpret_cast<const double2 *>(&As[k][4 * ty + 2]);
-                const double2 b0 = *reinterpret_cast<const double2 *>(&Bs[k][4 * tx]);
-                const double2 b1 = *reinterpret_cast<const double2 *>(&Bs[k][4 * tx + 2]);
-                const double ar[4] = {a0.x, a0.y, a1.x, a1.y}, bc[4] = {b0.x, b0.y, b1.x, b1.y};
+#pragma unroll 4
+            for (int k = 0; k < 64; k += 4) {
+                const double a0 = As[k + t4][m0 + g], a1 = As[k + t4][m0 + g + 8];
 #pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) acc[i][j] = fma(ar[i], bc[j], acc[i][j]);
+                for (int j = 0; j < 4; ++j) dmma16x8x4(acc[j], a0, a1, Bs[k + t4][n0 + 8 * j + g]);
             }
         }
-        // X_a = (a == cb) ? D_a : -D_a * acc   (D_a = identity past the 64-blocks of the factor)
+        // X_a = -D_a * acc   (D_a = identity past the 64-blocks of the factor)
         __syncthreads();
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                Cs[4 * ty + i][4 * tx + j] = (a == cb) ? ((4 * ty + i) == (4 * tx + j) ? 1.0 : 0.0) : acc[i][j];
+        for (int j = 0; j < 4; ++j) {
+            const int cc = n0 + 8 * j + 2 * t4;
+            Cs[m0 + g][cc] = acc[j][0];
+            Cs[m0 + g][cc + 1] = acc[j][1];
+            Cs[m0 + g + 8][cc] = acc[j][2];
+            Cs[m0 + g + 8][cc + 1] = acc[j][3];
+        }
         for (int i = tid; i < 64 * 64; i += 256) {
             const int k = i >> 6, r = i & 63;          // As[k][r] = D_a[r][k]
             As[k][r] = q64 < nb64 ? (double)dinv64[q64 * 4096 + r + 64 * k] : (r == k ? 1.0 : 0.0);
@@ -348,27 +359,26 @@ __global__ void __launch_bounds__(256) k_trtri_hb(const float *__restrict__ T, i
         __syncthreads();
         double out[4][4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) out[i][j] = 0.0;
-#pragma unroll 8
-        for (int k = 0; k < 64; ++k) {
-            const double2 d0 = *reinterpret_cast<const double2 *>(&As[k][4 * ty]);
-            const double2 d1 = *reinterpret_cast<const double2 *>(&As[k][4 * ty + 2]);
-            const double2 c0 = *reinterpret_cast<const double2 *>(&Cs[k][4 * tx]);
-            const double2 c1 = *reinterpret_cast<const double2 *>(&Cs[k][4 * tx + 2]);
-            const double dr[4] = {d0.x, d0.y, d1.x, d1.y}, cv[4] = {c0.x, c0.y, c1.x, c1.y};
+            for (int v = 0; v < 4; ++v) out[j][v] = 0.0;
+#pragma unroll 4
+        for (int k = 0; k < 64; k += 4) {
+            const double a0 = As[k + t4][m0 + g], a1 = As[k + t4][m0 + g + 8];
 #pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) out[i][j] = fma(dr[i], cv[j], out[i][j]);
+            for (int j = 0; j < 4; ++j) dmma16x8x4(out[j], a0, a1, Cs[k + t4][n0 + 8 * j + g]);
         }
-        const double sg = (a == cb) ? 1.0 : -1.0;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                Xb[(64 * a + 4 * ty + i) + (int64_t)(64 * cb + 4 * tx + j) * HB] = (float)(sg * out[i][j]);
+        for (int j = 0; j < 4; ++j) {
+            const int cc = n0 + 8 * j + 2 * t4;
+            float *x = Xb + 64 * a + m0 + g + (int64_t)(64 * cb + cc) * HB;
+            x[0] = (float)(-out[j][0]);
+            x[HB] = (float)(-out[j][1]);
+            x[8] = (float)(-out[j][2]);
+            x[HB + 8] = (float)(-out[j][3]);
+        }
+        // the stores of X_a are read back as B operands by the next rows
+        __syncthreads();
     }
 }
 
