@@ -52,7 +52,8 @@ struct BSmem {
     static constexpr size_t P = sizeof(TF) * BP * BLDP;              // panel, P[c][r] (factor phase)
     static constexpr size_t RS = sizeof(double) * BMAXR * BMAXN;      // r, z (solve phase, inside the panel)
     static constexpr size_t RED = sizeof(double) * (NT / 32) * BP * BMAXR;
-    static constexpr size_t PR = P > RS + RED ? P : RS + RED;
+    static constexpr size_t SD = (size_t)bsd_bytes<TF>();               // staged block inverse (solve phase)
+    static constexpr size_t PR = P > RS + RED + SD ? P : RS + RED + SD;
     static constexpr size_t LI = sizeof(TF) * BP * (BP + 1);         // block inverse, Li[p][j] = inv[j][p]
     static constexpr size_t RD = sizeof(TF) * BP;                     // 1 / diagonal
     static constexpr size_t CS = sizeof(float) * BMAXN;               // column sums of |A|
@@ -121,6 +122,7 @@ __global__ void __launch_bounds__(NT) k_batched_posv(BatchArgs a)
     TF *P = (TF *)smb;
     double *rs = (double *)smb;                                   // aliases P: solve phase only
     double *red = (double *)(smb + SM::RS);                       // aliases P: solve phase only
+    TF *sD = (TF *)(smb + SM::RS + SM::RED);                      // aliases P: solve phase only
     TF *Li = (TF *)(smb + SM::PR);
     TF *Rd = (TF *)(smb + SM::PR + SM::LI);
     float *colsum = (float *)(smb + SM::PR + SM::LI + SM::RD);
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(NT) k_batched_posv(BatchArgs a)
             const double tol = a.tol_eps * n;
             const int maxit = (sizeof(TF) == 8) ? 1 : a.max_iter;
             for (it = 1; it <= maxit; ++it) {
-                bsolve<TF, NT>(F, ldF, Dv, n, nr, rs, red);           // r <- M^-1 r
+                bsolve<TF, NT>(F, ldF, Dv, n, nr, rs, red, sD);       // r <- M^-1 r
                 for (int t = tid; t < n * nr; t += NT) {
                     const int i = t % n, q = t / n;
                     xs[q * BMAXN + i] += rs[q * BMAXN + i];

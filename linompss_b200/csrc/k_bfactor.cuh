@@ -219,13 +219,37 @@ __device__ int bfactor(TF *F, int ldF, int n, TF *Dv, TF *P, TF *Li, TF *Rd, int
     return *s_fail;
 }
 
+// column stride of a 32 x 32 block inverse staged in shared memory: a multiple
+// of 16 bytes (cp.async destinations) that spreads a row of the block over the
+// banks (at most 4-way conflicts when the lanes walk a row)
+template <typename TF>
+__host__ __device__ constexpr int bsd_ld() { return sizeof(TF) == 4 ? BP + 4 : BP + 2; }
+template <typename TF>
+__host__ __device__ constexpr int bsd_bytes() { return (int)sizeof(TF) * BP * bsd_ld<TF>(); }
+
+// start the copy of one block inverse (column-major, 32 x 32) into sD
+// (column stride bsd_ld); the caller waits with cp_async_wait<0> + a barrier
+template <typename TF, int NT>
+LNB_DEV void bstage_inv(TF *sD, const TF *Dk)
+{
+    constexpr int CPC = BP * (int)sizeof(TF) / 16;           // 16-byte chunks per column
+    for (int i = threadIdx.x; i < BP * CPC; i += NT) {
+        const int c = i / CPC, o = i - c * CPC;
+        bcp16(sD + c * bsd_ld<TF>() + o * (16 / (int)sizeof(TF)), Dk + c * BP + o * (16 / (int)sizeof(TF)), 16);
+    }
+    cp_async_commit();
+}
+
 // z <- inv(L) z, then z <- inv(L^T) z, for nr columns of z in shared memory
 // (z[q * BMAXN + i]); L in F, the block inverses in Dv.  env (may be NULL):
 // the factor's envelope per 32-row tile t -- env[t] = the first column with a
 // nonzero in rows 32t .. 32t+31, env[BMAXN/BP + t] = the last row with a
 // nonzero in columns 32t .. 32t+31 -- so the sums skip tiles that are zero.
+// sD: bsd_bytes<TF>() of shared memory.  Each block's inverse is copied there
+// by cp.async while the block's partial sums run, so the block step reads it
+// from shared memory instead of waiting on one L2 load per term.
 template <typename TF, int NT>
-__device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double *z, double *red,
+__device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double *z, double *red, TF *sD,
                        const int *env = nullptr)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -236,6 +260,8 @@ __device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double
     for (int kb = 0; kb < nblk; ++kb) {
         const int k0 = kb * BP, kn = min(BP, n - k0);
         const int cs = env ? env[kb] : 0;                   // columns before cs are zero in these rows
+        const TF *Dk = Dv + (int64_t)kb * BP * BP;
+        bstage_inv<TF, NT>(sD, Dk);
         if (k0 > cs) {
             double acc[BMAXR];
 #pragma unroll
@@ -251,6 +277,7 @@ __device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double
             }
 #pragma unroll
             for (int q = 0; q < BMAXR; ++q) red[(q * NW + warp) * BP + lane] = acc[q];   // lanes contiguous
+            cp_async_wait<0>();
             __syncthreads();
             for (int t = tid; t < kn * nr; t += NT) {
                 const int q = t / kn, i = t - q * kn;
@@ -259,14 +286,16 @@ __device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double
                 z[q * BMAXN + k0 + i] -= s;
             }
             __syncthreads();
+        } else {
+            cp_async_wait<0>();
+            __syncthreads();
         }
         // z_blk = inv(L_kk) z_blk: thread (j, q), j = row of the block, q = rhs
-        const TF *Dk = Dv + (int64_t)kb * BP * BP;
         const int j = tid & 31, q = tid >> 5;
         const bool act = j < kn && q < nr;
         double v = 0.0;
         if (act)
-            for (int p = 0; p <= j; ++p) v = fma((double)__ldcg(Dk + j + BP * p), z[q * BMAXN + k0 + p], v);
+            for (int p = 0; p <= j; ++p) v = fma((double)sD[j + bsd_ld<TF>() * p], z[q * BMAXN + k0 + p], v);
         __syncthreads();
         if (act) z[q * BMAXN + k0 + j] = v;
         __syncthreads();
@@ -275,6 +304,7 @@ __device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double
     for (int kb = nblk - 1; kb >= 0; --kb) {
         const int k0 = kb * BP, kn = min(BP, n - k0), r0 = k0 + kn;
         const int re = env ? min(n, env[BMAXN / BP + kb] + 1) : n;    // rows from re on are zero here
+        bstage_inv<TF, NT>(sD, Dv + (int64_t)kb * BP * BP);
         if (r0 < re) {
             for (int jc = warp; jc < kn; jc += NW) {
                 double acc[BMAXR];
@@ -296,20 +326,23 @@ __device__ void bsolve(const TF *F, int ldF, const TF *Dv, int n, int nr, double
                     if (lane == 0) red[q * BP + jc] = v;
                 }
             }
+            cp_async_wait<0>();
             __syncthreads();
             for (int t = tid; t < kn * nr; t += NT) {
                 const int q = t / kn, i = t - q * kn;
                 z[q * BMAXN + k0 + i] -= red[q * BP + i];
             }
             __syncthreads();
+        } else {
+            cp_async_wait<0>();
+            __syncthreads();
         }
         // z_blk = inv(L_kk)^T z_blk
-        const TF *Dk = Dv + (int64_t)kb * BP * BP;
         const int j = tid & 31, q = tid >> 5;
         const bool act = j < kn && q < nr;
         double v = 0.0;
         if (act)
-            for (int p = j; p < kn; ++p) v = fma((double)__ldcg(Dk + p + BP * j), z[q * BMAXN + k0 + p], v);
+            for (int p = j; p < kn; ++p) v = fma((double)sD[p + bsd_ld<TF>() * j], z[q * BMAXN + k0 + p], v);
         __syncthreads();
         if (act) z[q * BMAXN + k0 + j] = v;
         __syncthreads();

@@ -122,13 +122,14 @@ __global__ void __launch_bounds__(NT) k_bj_apply(int64_t n, int bm, const double
 {
     __shared__ double zs[BMAXN];
     __shared__ double red[(NT / 32) * BP * BMAXR];
+    __shared__ __align__(16) double sD[bsd_bytes<double>() / sizeof(double)];
     const int64_t k = blockIdx.x, r0 = k * bm;
     const int bk = (int)((n - r0) < bm ? (n - r0) : bm);
     const int64_t ldF = bj_ldf(bm);
     const double *F = fac + k * bj_stride(bm);
     for (int i = threadIdx.x; i < bk; i += NT) zs[i] = r[r0 + i];
     __syncthreads();
-    bsolve<double, NT>(F, (int)ldF, F + ldF * bm, bk, 1, zs, red, env + k * ENV);
+    bsolve<double, NT>(F, (int)ldF, F + ldF * bm, bk, 1, zs, red, sD, env + k * ENV);
     for (int i = threadIdx.x; i < bk; i += NT) z[r0 + i] = zs[i];
 }
 

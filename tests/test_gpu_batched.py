@@ -102,7 +102,8 @@ def test_batched_edge_sizes_and_capacity(lnb, cuda):
     assert got[1] == -7 and (np.delete(got, 1) == 0).all()
 
 
-def test_batched_not_spd_reports_info(lnb, cuda):
+@pytest.mark.parametrize("mode", ["FACTOR_FP32", "FACTOR_FP64"])
+def test_batched_not_spd_reports_info(lnb, cuda, mode):
     import torch
     ns, rs, As, Bs = make_batch(20, seed=3, nmax=200)
     As[7] = As[7].copy()
@@ -110,7 +111,7 @@ def test_batched_not_spd_reports_info(lnb, cuda):
     nd, rd, ao, bo, dA, dB, b_off = to_device(ns, rs, As, Bs, cuda)
     dX = torch.zeros_like(dB)
     info = torch.full((len(ns),), -99, dtype=torch.int32, device=cuda)
-    lnb.batched_posv_dev(nd, rd, ao, bo, dA, dB, dX, lnb.FACTOR_FP64, 10, info)
+    lnb.batched_posv_dev(nd, rd, ao, bo, dA, dB, dX, getattr(lnb, mode), 10, info)
     torch.cuda.synchronize()
     got = info.cpu().numpy()
     assert got[7] == 6 and (np.delete(got, 7) == 0).all()
