@@ -76,7 +76,7 @@ __device__ double bresidual(const double *A, int n, int nr, const double *B, con
 #pragma unroll
         for (int q = 0; q < BMAXR; ++q) acc[q] = 0.0;
         if (i < n) {
-#pragma unroll 4
+#pragma unroll 16
             for (int c = cg; c < n; c += CG) {
                 const double a = __ldg(A + i + (int64_t)c * n);
 #pragma unroll

@@ -1,10 +1,11 @@
 // k_bfactor.cuh -- single-CTA right-looking Cholesky of a matrix of order <= 512
 // held in global memory (L2-resident): 32-column panels staged in shared memory
-// by cp.async; one warp factors each diagonal block left-looking (potf2 order)
-// and inverts it; the rows below become dot products with that inverse; the
-// trailing update runs 4 x 4 tiles per thread with 16-byte loads.  Used per
-// system by the batched solver and, in one launch, for the large diagonal tiles
-// of the FP32 factorization.
+// by cp.async; warp 0 factors each diagonal block left-looking (potf2 order)
+// while warp 1 inverts it one row behind; the rows below become dot products
+// with that inverse; the trailing update runs 4 x 4 tiles per thread with
+// 16-byte loads.  Also the triangular solves with the stored block inverses.
+// Used per system by the batched solver (k_batched.cu) and per diagonal block
+// by the block-Jacobi preconditioner of the sparse refinement (k_sparse.cu).
 #pragma once
 #include "common.cuh"
 
@@ -100,28 +101,47 @@ __device__ int bfactor(TF *F, int ldF, int n, TF *Dv, TF *P, TF *Li, TF *Rd, int
         cp_async_commit();
         cp_async_wait<0>();
         __syncthreads();
+        // Diagonal block: warp 0 factors it column by column while warp 1 forms its
+        // inverse one row behind.  Row r of the inverse needs row r of L and
+        // 1/L[r][r], which factor step r completes, so the two warps meet at named
+        // barrier 1 once per column (bar.sync on both sides: exactly 32 + 32
+        // arrivals per generation).  A bad pivot at column c is recorded in
+        // *s_fail (= j0 + c + 1) before barrier c; warp 0 leaves after barrier c
+        // and warp 1 after the barrier at which it reads that value for its own
+        // row c, so each has passed c + 1 barriers.
         if (warp == 0) {
-            // diagonal block, left-looking (potf2 order); lane l owns row l
+            // left-looking (potf2 order); lane l owns row l
             const int rl = lane < jb ? lane : 0;
-            int bad = -1;
             for (int c = 0; c < jb; ++c) {
                 const TF sv = P[c * BLDP + rl] - bdot(P + rl, BLDP, P + c, BLDP, c);
                 const TF d = __shfl_sync(0xffffffffu, sv, c);
-                if (!(d > TF(0))) { bad = c; break; }
-                const TF inv = brsqrt(d);
-                if (lane == c) { P[c * BLDP + c] = d * inv; Rd[c] = inv; }
-                else if (lane > c && lane < jb) P[c * BLDP + lane] = sv * inv;
-                __syncwarp();
-            }
-            if (lane == 0 && bad >= 0) *s_fail = j0 + bad + 1;
-            if (bad < 0) {
-                // inverse of the block: lane c builds column c, Li[c][*] = inv[*][c]
-                TF *Xc = Li + lane * (BP + 1);
-                for (int r = 0; r < BP; ++r) {
-                    TF v = (r == lane) ? TF(1) : TF(0);
-                    if (r < jb) v = (v - bdot(P + r, BLDP, Xc, 1, r)) * Rd[r];
-                    Xc[r] = v;
+                const bool bad = !(d > TF(0));                  // warp-uniform: d is broadcast
+                if (bad) {
+                    if (lane == 0) *s_fail = j0 + c + 1;
+                } else {
+                    const TF inv = brsqrt(d);
+                    if (lane == c) { P[c * BLDP + c] = d * inv; Rd[c] = inv; }
+                    else if (lane > c && lane < jb) P[c * BLDP + lane] = sv * inv;
                 }
+                asm volatile("bar.sync 1, 64;" ::: "memory");   // column c published
+                if (bad) break;
+            }
+        } else if (warp == 1) {
+            // inverse of the block: lane c builds column c, Li[c][*] = inv[*][c]
+            TF *Xc = Li + lane * (BP + 1);
+            bool ok = true;
+            for (int r = 0; r < BP; ++r) {
+                TF v = (r == lane) ? TF(1) : TF(0);
+                if (r < jb) {
+                    asm volatile("bar.sync 1, 64;" ::: "memory");   // factor column r done
+                    // warp 0 may already be one column ahead (and may have recorded a
+                    // failure there), so only a failure AT column r ends this loop
+                    if (*(volatile int *)s_fail == j0 + r + 1) { ok = false; break; }
+                    v = (v - bdot(P + r, BLDP, Xc, 1, r)) * Rd[r];
+                }
+                Xc[r] = v;
+            }
+            if (ok) {
                 __syncwarp();
                 TF *Dk = Dv + (int64_t)(j0 / BP) * BP * BP;     // column-major: Dk[r + 32 c] = inv[r][c]
                 for (int c = 0; c < BP; ++c) Dk[lane + BP * c] = Li[c * (BP + 1) + lane];

@@ -154,3 +154,24 @@ def test_sspdsolv_and_spotrs(lnb, cuda):
     lnb.spotrs_dev(Lt, Bt, m, nrhs, "B")
     torch.cuda.synchronize()
     np.testing.assert_allclose(Bt.cpu().numpy().T, B, rtol=0, atol=1e-5 * np.abs(B).max())
+
+
+@pytest.mark.parametrize("mode", ["FACTOR_FP32", "FACTOR_FP64"])
+def test_batched_not_spd_at_every_panel_position(lnb, cuda, mode):
+    """A non-positive pivot at the first, last and a middle column of the first,
+    a middle and a ragged last 32-column panel: each system reports its own
+    column (LAPACK info) and the others are solved."""
+    import torch
+    bad_cols = [0, 5, 31, 32, 63, 80, 95, 99]
+    ns, rs, As, Bs = make_batch(len(bad_cols) + 3, seed=11, nmin=100, nmax=100)
+    for k, c in enumerate(bad_cols):
+        As[k] = As[k].copy()
+        As[k][c, c] = -1.0
+    nd, rd, ao, bo, dA, dB, b_off = to_device(ns, rs, As, Bs, cuda)
+    dX = torch.zeros_like(dB)
+    info = torch.full((len(ns),), -99, dtype=torch.int32, device=cuda)
+    lnb.batched_posv_dev(nd, rd, ao, bo, dA, dB, dX, getattr(lnb, mode), 10, info)
+    torch.cuda.synchronize()
+    got = info.cpu().numpy()
+    assert list(got[:len(bad_cols)]) == [c + 1 for c in bad_cols]
+    assert (got[len(bad_cols):] == 0).all()
