@@ -60,6 +60,11 @@ struct BSmem {
     static constexpr size_t XS = sizeof(double) * BMAXR * BMAXN;      // x
     static constexpr size_t total = PR + LI + RD + CS + XS;
 };
+// every shape fits one CTA's 227 KB; the autotuner's "two FP32 systems per SM"
+// needs two 256-thread CTAs (plus 1 KB reserved each) within the SM's 228 KB
+static_assert(BSmem<double, 256>::total <= 227 * 1024 && BSmem<float, 512>::total <= 227 * 1024,
+              "batched solver: shared memory per CTA");
+static_assert(2 * (BSmem<float, 256>::total + 1024) <= 228 * 1024, "batched solver: two FP32 systems per SM");
 
 // r = b - A x (A full symmetric n x n, FP64) for nr columns; returns the max
 // over columns of ||r||_inf / (anorm ||x||_inf + ||b||_inf), same in every thread
